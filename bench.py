@@ -1,0 +1,481 @@
+#!/usr/bin/env python
+"""bench.py — the fused-chain hot path on B200, measured against HBM roofline, with the reference's CPU path beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--quick]
+
+Headline (`value`): the fused GEMVER at n = 16384 in f32 (A is 1 GiB: inputs larger than L2), as achieved HBM GB/s of
+algorithmic traffic (read A, write Â, read Â again, the vectors: 12n² + 32n bytes per step), device-timed with CUDA
+events over K steps on the launching stream, max over ranks. Beside it in the same line: the roofline of the
+kernel, the CPU baseline (the reference's unfused component loops, f32, OpenMP on all host threads), the end-to-end
+number through the C ABI from pinned host buffers, SM clocks sampled during the measurement, and secondary
+workloads (BF16-storage GEMVER, both NS residuals at 4096², the gemver chain) with their errors against f64.
+
+With --impl reference, the same metric and configuration measured on the reference's CPU implementation of the path
+(the oracle's port of the unfused component loops; AdaptiveCpp is not available to build the reference itself).
+Under torchrun, each rank runs its own replica of the workload (independent units: no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "GEMVER/NS-residual HBM GB/s & %roofline; batched req/s + p50/p99 vs plain, ≤1e-3 rel err"
+N_HEAD = 16384
+FALLBACK_HBM = 6650.0
+
+
+def gemver_bytes(n: int, a_bytes: int = 4, store_B: bool = True, second_read_bytes: int | None = None) -> float:
+    """Algorithmic bytes of one GEMVER: A once, Â written (if stored), the matrix read once more, vectors."""
+    rb = a_bytes if second_read_bytes is None else second_read_bytes
+    return float(n) * n * (a_bytes + (4 if store_B else 0) + rb) + 32.0 * n
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": FALLBACK_HBM, "source": "fallback"}
+
+
+def profile_traffic(name: str):
+    """Per-launch DRAM bytes recorded from an ncu capture (a line `traffic_bytes_per_launch = N` in profiles/<name>)."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch"):
+            try:
+                return float(line.split("=")[1].split()[0])
+            except (IndexError, ValueError):
+                return None
+    return None
+
+
+# ---- distributed plumbing ----------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, torch):
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self, torch):
+        if self.pg:
+            self.pg.barrier()
+        torch.cuda.synchronize()
+
+    def max(self, torch, x: float) -> float:
+        if not self.pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks -----------------------------------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the measurement runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 10:
+                continue
+            try:
+                rows.append({"sm": float(f[1]), "max": float(f[2]), "util": float(f[4]), "hw": f[6], "hwt": f[7],
+                             "swt": f[8], "pcap": f[9]})
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r["util"] > 0] or rows
+        reasons = []
+        for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                          ("pcap", "sw_power_cap")):
+            if any(r[key].lower().startswith("active") for r in load):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load), "sm_max_mhz": load[0]["max"],
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(load)}
+
+
+# ---- timing -----------------------------------------------------------------------------------------------------
+def timed(torch, dist: Dist, step, K: int, W: int, soak_s: float = 0.0) -> float:
+    """W untimed steps (plus an untimed soak), then K steps between two CUDA events on the current stream, with a
+    barrier and a synchronize on both sides. Returns ms per step, max over ranks."""
+    for _ in range(W):
+        step()
+    if soak_s > 0:
+        t0 = time.time()
+        while time.time() - t0 < soak_s:
+            for _ in range(10):
+                step()
+            torch.cuda.synchronize()
+    dist.barrier(torch)
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(K):
+        step()
+    e1.record(s)
+    e1.synchronize()
+    dist.barrier(torch)
+    return dist.max(torch, e0.elapsed_time(e1) / K)
+
+
+def relerr(torch, got, want) -> float:
+    got = got.double()
+    want = want.double()
+    den = float(torch.linalg.vector_norm(want))
+    num = float(torch.linalg.vector_norm(got - want))
+    return num / den if den else (0.0 if num == 0 else float("inf"))
+
+
+# ---- workloads --------------------------------------------------------------------------------------------------
+def gemver_f64_reference(torch, d, alpha, beta, A=None):
+    """x, w of the GEMVER in f64 on the GPU (torch), from the f32 / bf16 operands: the error yardstick."""
+    A = (d["A"] if A is None else A).double()
+    B = A + torch.outer(d["u1"].double(), d["v1"].double()) + torch.outer(d["u2"].double(), d["v2"].double())
+    x = beta * (B.t() @ d["y"].double()) + d["z"].double()
+    w = alpha * (B @ x)
+    return B, x, w
+
+
+def bench_gemver(torch, cb, dist, args, peak):
+    from cospanmdao_b200 import workloads
+    n = args.n
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = workloads.gemver_inputs(n, 0, device=dev)
+    B = torch.empty((n, n), dtype=torch.float32, device=dev)
+    x = torch.empty(n, dtype=torch.float32, device=dev)
+    w = torch.empty(n, dtype=torch.float32, device=dev)
+    ws = cb.Workspace(dev)
+    alpha, beta = 1.5, 1.2
+
+    def step():
+        cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=alpha, beta=beta, B=B, x=x, w=w,
+                  workspace=ws)
+
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    ms = timed(torch, dist, step, args.steps, args.warmup, soak_s=args.soak)
+    clk = clocks.stop()
+    nbytes = gemver_bytes(n)
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    # errors per output against f64 (computed once, outside the timed region)
+    B64, x64, w64 = gemver_f64_reference(torch, d, alpha, beta)
+    err = {"B": relerr(torch, B, B64), "x": relerr(torch, x, x64), "w": relerr(torch, w, w64)}
+    del B64, x64, w64
+    torch.cuda.empty_cache()
+
+    # end to end through the C ABI: inputs from pinned host memory, x and w back to the host, every step
+    hA = torch.empty((n, n), dtype=torch.float32, pin_memory=True)
+    hA.copy_(d["A"])
+    hv = {k: d[k].cpu().pin_memory() for k in workloads.VECTORS}
+    hx = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    hw = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    dA = torch.empty_like(d["A"])
+    dv = {k: torch.empty_like(d[k]) for k in workloads.VECTORS}
+
+    def e2e_step():
+        dA.copy_(hA, non_blocking=True)
+        for k in workloads.VECTORS:
+            dv[k].copy_(hv[k], non_blocking=True)
+        cb.gemver(dA, dv["u1"], dv["v1"], dv["u2"], dv["v2"], dv["y"], dv["z"], alpha=alpha, beta=beta, B=B, x=x,
+                  w=w, workspace=ws)
+        hx.copy_(x, non_blocking=True)
+        hw.copy_(w, non_blocking=True)
+
+    ke = max(3, min(args.steps, 10))
+    ms_e2e = timed(torch, dist, e2e_step, ke, 2)
+    h2d = n * n * 4 + 6 * n * 4
+    d2h = 2 * n * 4
+    del hA, dA
+    out = {
+        "ms": ms, "gbs": gbs, "bytes": nbytes, "err": err, "clocks": clk,
+        "e2e": {"value": dist.world * nbytes / (ms_e2e * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+    }
+    del d, B
+    torch.cuda.empty_cache()
+    return out
+
+
+def bench_gemver_bf16(torch, cb, dist, args):
+    from cospanmdao_b200 import workloads
+    n = args.n
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = workloads.gemver_inputs(n, 0, device=dev)
+    A16 = d["A"].to(torch.bfloat16)
+    x = torch.empty(n, dtype=torch.float32, device=dev)
+    w = torch.empty(n, dtype=torch.float32, device=dev)
+    B = torch.empty((n, n), dtype=torch.float32, device=dev)
+    ws = cb.Workspace(dev)
+    res = {}
+    for store in (True, False):
+        def step():
+            cb.gemver(A16, d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2,
+                      B=B if store else None, want_B=store, x=x, w=w, workspace=ws)
+        ms = timed(torch, dist, step, args.steps, args.warmup)
+        nbytes = gemver_bytes(n, a_bytes=2, store_B=store, second_read_bytes=2)
+        res["store_B" if store else "no_B"] = {"ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "bytes": nbytes}
+    cb.gemver(A16, d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2, B=B, x=x, w=w,
+              workspace=ws)
+    B64, x64, w64 = gemver_f64_reference(torch, d, 1.5, 1.2)  # the f32 matrix: storage error included
+    res["err_vs_f64_of_f32_A"] = {"B": relerr(torch, B, B64), "x": relerr(torch, x, x64), "w": relerr(torch, w, w64)}
+    del B64, x64, w64, B, A16, d
+    torch.cuda.empty_cache()
+    return res
+
+
+def bench_chain(torch, cb, dist, args):
+    from cospanmdao_b200 import workloads
+    n = args.n
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = workloads.gemver_inputs(n, 0, device=dev, dist="reference")
+    a = {k: d[k] for k in workloads.VECTORS}
+    b = {k: d[k] for k in ("u1", "v1", "u2", "v2")}
+    out = {k: torch.empty((n, n) if k.startswith("B") else (n,), dtype=torch.float32, device=dev)
+           for k in ("B1", "x1", "w1", "q", "s", "B2", "x2", "w2")}
+    ws = cb.Workspace(dev)
+    ab = 1.0 / math.sqrt(n)
+
+    def step():
+        cb.gemver_chain(d["A"], a, b, alpha=ab, beta=ab, out=out, workspace=ws)
+
+    ms = timed(torch, dist, step, max(3, args.steps // 2), args.warmup)
+    alg = 24.0 * n * n + 80.0 * n
+    nominal = 8.0 * n * n * 4  # the reference's quoted traffic (examples/gemver-chain/README.md:136)
+    del out, d
+    torch.cuda.empty_cache()
+    return {"ms": ms, "gbs_algorithmic": alg / (ms * 1e-3) / 1e9, "gbs_nominal_reference_formula": nominal / (ms * 1e-3) / 1e9,
+            "reference_rtx4090_crafted_ms": 8.359}
+
+
+def bench_ns(torch, cb, dist, args):
+    from cospanmdao_b200 import workloads
+    N = args.grid
+    dev = torch.device("cuda", torch.cuda.current_device())
+    res = {}
+    u, v, p, h = workloads.ns_fields(N, seed=0, device=dev)
+    out = tuple(torch.empty((N, N), dtype=torch.float32, device=dev) for _ in range(3))
+    norms = torch.empty(3, dtype=torch.float64, device=dev)
+    ws = cb.Workspace(dev)
+
+    def step():
+        cb.ns_incompressible(u, v, p, h=h, nu=1e-3, out=out, norms=norms, workspace=ws)
+
+    ms = timed(torch, dist, step, args.steps, args.warmup)
+    nbytes = 24.0 * N * N
+    # f64 yardstick of the formula (torch on the GPU)
+    U, V, P = u.double(), v.double(), p.double()
+
+    def ddx(f):
+        return (torch.roll(f, -1, 1) - torch.roll(f, 1, 1)) / (2 * h)
+
+    def ddy(f):
+        return (torch.roll(f, -1, 0) - torch.roll(f, 1, 0)) / (2 * h)
+
+    def lap(f):
+        return ((torch.roll(f, -1, 1) - f) + (torch.roll(f, 1, 1) - f) + (torch.roll(f, -1, 0) - f)
+                + (torch.roll(f, 1, 0) - f)) / (h * h)
+    ru64 = U * ddx(U) + V * ddy(U) + ddx(P) - 1e-3 * lap(U)
+    rv64 = U * ddx(V) + V * ddy(V) + ddy(P) - 1e-3 * lap(V)
+    rc64 = ddx(U) + ddy(V)
+    n64 = torch.stack([torch.linalg.vector_norm(t) for t in (ru64, rv64, rc64)])
+    res["incompressible_f32"] = {
+        "grid": N, "ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "bytes": nbytes,
+        "err": {"r_u": relerr(torch, out[0], ru64), "r_v": relerr(torch, out[1], rv64), "r_c": relerr(torch, out[2], rc64),
+                "norms": float(((norms - n64).abs() / n64).max())}}
+    ub, vb, pb = (t.to(torch.bfloat16) for t in (u, v, p))
+
+    def step16():
+        cb.ns_incompressible(ub, vb, pb, h=h, nu=1e-3, out=out, norms=norms, workspace=ws)
+
+    ms16 = timed(torch, dist, step16, args.steps, args.warmup)
+    b16 = 18.0 * N * N
+    res["incompressible_bf16"] = {"ms": ms16, "gbs": b16 / (ms16 * 1e-3) / 1e9, "bytes": b16,
+                                  "err_vs_f64_of_f32_fields": {"r_u": relerr(torch, out[0], ru64),
+                                                               "r_v": relerr(torch, out[1], rv64),
+                                                               "r_c": relerr(torch, out[2], rc64)}}
+    del U, V, P, ru64, rv64, rc64, u, v, p, ub, vb, pb, out
+    torch.cuda.empty_cache()
+
+    Uc = cb.ns_init_cons(N, N, 1.0, device=dev)
+    R = torch.empty_like(Uc)
+    diag = torch.empty(18, dtype=torch.float32, device=dev)
+    sq = torch.empty(4, dtype=torch.float64, device=dev)
+    for bc in ("walls", "periodic"):
+        def stepc():
+            cb.ns_compressible(Uc, limiter="minmod", bc=bc, R=R, diag=diag, det_sq64=sq, workspace=ws)
+        msc = timed(torch, dist, stepc, args.steps, args.warmup)
+        res[f"compressible_{bc}_minmod"] = {"grid": N, "ms": msc, "gbs_nominal": 32.0 * N * N / (msc * 1e-3) / 1e9,
+                                            "reference_rtx4090_handwritten_ms": 3.550 if bc == "walls" else None}
+    del Uc, R
+    torch.cuda.empty_cache()
+    return res
+
+
+# ---- the CPU path ---------------------------------------------------------------------------------------------
+def cpu_gemver(n: int, target_s: float = 3.0, reps: int = 3) -> dict:
+    """The reference's unfused GEMVER component loops in f32 (oracle port, OpenMP, every host thread) on a bounded
+    sample of the n = 16384 workload: a band of rows sized to ~target_s per run, up to the whole matrix. Returns GB/s
+    of the same algorithmic traffic per row."""
+    import numpy as np
+    import oracle
+    lib = oracle.restatement()
+    A = np.empty(n * n, dtype=np.float32)
+    lib.orc_fill_hash(A.ctypes.data_as(__import__("ctypes").c_void_p), n * n, 0, 1, 0)
+    vecs = [oracle.hash_fill(n, s, 1) for s in range(2, 8)]
+    B = np.empty(n * n, dtype=np.float32)
+    x = np.empty(n, dtype=np.float32)
+    w = np.empty(n, dtype=np.float32)
+    P = lambda a: a.ctypes.data_as(__import__("ctypes").c_void_p)  # noqa: E731
+
+    def run(rows):
+        t0 = time.perf_counter()
+        lib.orc_gemver_f32_unfused(n, 64, P(A), *[P(v) for v in vecs], 1.5, 1.2, P(B), P(x), P(w), 0, rows)
+        return time.perf_counter() - t0
+
+    rows = 256
+    t = run(rows)
+    while t < target_s / 4 and rows < n:
+        rows = min(n, rows * 4)
+        t = run(rows)
+    if t < target_s and rows < n:
+        rows = min(n, int(rows * target_s / max(t, 1e-3)) // 64 * 64 or 64)
+    times = [run(rows) for _ in range(reps)]
+    tmed = statistics.median(times)
+    bytes_ = 12.0 * rows * n + 32.0 * n
+    return {"value": bytes_ / tmed / 1e9, "unit": "GB/s", "cores": oracle.threads(), "kind": "port",
+            "sample": f"rows 0..{rows} of the n={n} f32 GEMVER (A, Â, Â re-read of those rows), median of {reps}",
+            "seconds_per_sample": tmed}
+
+
+# ---- main -------------------------------------------------------------------------------------------------------
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_HEAD)
+    ap.add_argument("--grid", type=int, default=4096)
+    ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed steps before the timed region")
+    ap.add_argument("--quick", action="store_true", help="headline only (no secondary workloads, no CPU baseline)")
+    args = ap.parse_args(argv)
+    args.warmup = max(3, args.warmup)
+    dist = Dist()
+
+    config = {"workload": f"fused GEMVER n={args.n} f32 (A {args.n * args.n * 4 / 2**30:.2f} GiB), one launch",
+              "n": args.n, "alpha": 1.5, "beta": 1.2, "seed": 0,
+              "l2": "inputs larger than L2 (A and Â are 1 GiB each vs 126 MB)",
+              "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"}
+
+    if args.impl == "reference":
+        if dist.rank != 0:
+            return 0
+        cpu = cpu_gemver(args.n, target_s=2.0, reps=max(1, min(args.steps, 3)))
+        line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "GB/s", "n_gpus": dist.world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["seconds_per_sample"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded hash generator of the reference example)", "config": config,
+                "cpu_baseline": cpu,
+                "e2e": {"value": cpu["value"], "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference's unfused GEMVER component loops (examples/gemver-chain/components.hpp:85-265) "
+                        "restated in C++ with OpenMP; AdaptiveCpp is not available to build the reference itself"}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import cospanmdao_b200 as cb
+    dist.init(torch)
+    cb.lib()
+    pk = peaks()
+    g = bench_gemver(torch, cb, dist, args, pk)
+    total_bytes = g["bytes"] * dist.world
+    value = total_bytes / (g["ms"] * 1e-3) / 1e9
+    kernel_gbs = g["bytes"] / (g["ms"] * 1e-3) / 1e9  # per launch on one GPU
+    traffic = profile_traffic("gemver_f32_n16384.md")
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": g["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded hash generator: A ~ U[-1,1), vectors ~ U[0,1), seed 0)",
+        "config": config,
+        "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": kernel_gbs / pk["hbm_gbs"], "peak_source": pk["source"],
+                     "traffic": traffic, "algorithmic_bytes_per_launch": g["bytes"],
+                     "kernel": "cspb::k_gemver<float, true>"},
+        "e2e": g["e2e"],
+        "gpu_launches": args.steps,
+        "clocks": g["clocks"],
+        "err_vs_f64": g["err"],
+    }
+    if not args.quick:
+        sec = {}
+        sec["gemver_bf16_storage"] = bench_gemver_bf16(torch, cb, dist, args)
+        sec["gemver_chain"] = bench_chain(torch, cb, dist, args)
+        sec["ns_residual"] = bench_ns(torch, cb, dist, args)
+        line["secondary"] = sec
+    if dist.rank == 0 and not args.quick:
+        line["cpu_baseline"] = cpu_gemver(args.n)
+    if dist.rank == 0:
+        print(json.dumps(line))
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

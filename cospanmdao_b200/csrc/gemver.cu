@@ -1,0 +1,355 @@
+// gemver.cu — GEMVER, BiCGK and the gemver chain as persistent cooperative kernels built from rowpass.cuh.
+//
+// GEMVER (one launch, 3 passes over n² elements — the minimum, since w needs all of x):
+//   pass 1   read A, write Â, f64 column partials of Â·y      (Rank2Update + GemvTPartial, fused)
+//   barrier, x = z + β·Σ partials (fixed order), barrier       (ColReduce<true>)
+//   pass 2   read Â (or A again, re-applying the update), row dots with x, last chunk of a strip writes w = α·dot
+//            (Gemv); walked from the last strip back, so the Â rows still in L2 are read first.
+// BiCGK (one pass): q = B·p row dots and s = Bᵀ·r column partials from the same loads; one barrier; s.
+// Chain (G1 → BiCGK → G2, six passes — the reference's nominal traffic counts eight):
+//   1: A0 → B1 + x1 partials | 2: B1 → w1 = α·(B1·x1), q = B1·x1 (p = x1, so one dot gives both)
+//   3: B1 → s partials (with w1) + B2 + x2 partials (with q) | 4: B2 → w2.
+#include <cstdio>
+
+#include "rowpass.cuh"
+
+namespace cspb {
+
+constexpr int kWX = 2;  // warps across columns in every GEMVER-family pass
+
+struct GemverK {
+    PassArgs p1, p2;
+    uint32_t* ctrl;
+    int64_t units;
+    const float* z;
+    float beta;
+    float* x;
+};
+
+template <typename T, bool P2_FROM_B>
+__global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0);
+        if (u >= g.units) break;
+        pass_unit<T, kWX, true, true, false, true, false>(g.p1, u, vec_ok != 0, smem);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
+    if (!grid_barrier(g.ctrl)) return;
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0 + 1);
+        if (u >= g.units) break;
+        const int64_t unit = g.units - 1 - int64_t(u);
+        if constexpr (P2_FROM_B)
+            pass_unit<float, kWX, false, false, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+        else
+            pass_unit<T, kWX, true, true, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+    }
+}
+
+struct BicgkK {
+    PassArgs p;
+    uint32_t* ctrl;
+    int64_t units;
+    float* s;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kPassThreads, 2) k_bicgk(BicgkK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0);
+        if (u >= g.units) break;
+        pass_unit<T, kWX, true, false, false, true, true>(g.p, u, vec_ok != 0, smem);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish(g.p.PB, g.p.strips, g.p.n, nullptr, 1.0f, g.s);
+}
+
+struct ChainK {
+    PassArgs p1, p2, p3, p4;
+    uint32_t* ctrl;
+    int64_t units;
+    const float* za;
+    float beta;
+    float *x1, *s, *x2;
+};
+
+__global__ void __launch_bounds__(kPassThreads, 2) k_chain(ChainK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<float, kWX>()];
+    const bool vo = vec_ok != 0;
+    // 1: A0 -> B1, partials of B1ᵀ·ya
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0);
+        if (u >= g.units) break;
+        pass_unit<float, kWX, true, true, false, true, false>(g.p1, u, vo, smem);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.za, g.beta, g.x1);
+    if (!grid_barrier(g.ctrl)) return;
+    // 2: B1 · x1 -> w1 (α) and q (1), from the last strip back
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0 + 1);
+        if (u >= g.units) break;
+        pass_unit<float, kWX, false, false, false, false, true>(g.p2, g.units - 1 - int64_t(u), vo, smem);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    // 3: B1 -> partials of B1ᵀ·w1 (s); B2 = B1 + update; partials of B2ᵀ·q (x2)
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0 + 2);
+        if (u >= g.units) break;
+        pass_unit<float, kWX, false, true, true, true, false>(g.p3, u, vo, smem);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish(g.p3.PA, g.p3.strips, g.p3.n, nullptr, 1.0f, g.s);    // s = B1ᵀ·w1
+    colsum_finish(g.p3.PB, g.p3.strips, g.p3.n, g.s, g.beta, g.x2);     // x2 = s + β·B2ᵀ·q (same thread owns s[j])
+    if (!grid_barrier(g.ctrl)) return;
+    // 4: B2 · x2 -> w2
+    for (;;) {
+        const uint32_t u = grab_work(g.ctrl, kWork0 + 3);
+        if (u >= g.units) break;
+        pass_unit<float, kWX, false, false, false, false, true>(g.p4, g.units - 1 - int64_t(u), vo, smem);
+    }
+}
+
+}  // namespace cspb
+
+// =====================================================================================================================
+// host side
+// =====================================================================================================================
+using namespace cspb;
+using cspb_host::align_up;
+using cspb_host::aligned;
+
+namespace {
+
+struct PassLayout {
+    int64_t strips = 0, chunks = 0, units = 0;
+    size_t off_done = 0, off_PA = 0, off_PB = 0, off_Wp = 0, total = 0;
+};
+
+// Workspace: [ctrl 256][strip_done: strips u32 × nsets][PA: strips×n f64][PB: strips×n f64][Wp: chunks×n f32]
+PassLayout pass_layout(int64_t n, int S, int CW, int done_sets, bool want_PA) {
+    PassLayout L;
+    L.strips = (n + S - 1) / S;
+    L.chunks = (n + CW - 1) / CW;
+    L.units = L.strips * L.chunks;
+    size_t o = kCtrlBytes;
+    L.off_done = o;
+    o = align_up(o + size_t(L.strips) * sizeof(uint32_t) * size_t(done_sets), 256);
+    L.off_PA = o;
+    if (want_PA) o = align_up(o + size_t(L.strips) * size_t(n) * sizeof(double), 256);
+    L.off_PB = o;
+    o = align_up(o + size_t(L.strips) * size_t(n) * sizeof(double), 256);
+    L.off_Wp = o;
+    o = align_up(o + size_t(L.chunks) * size_t(n) * sizeof(float), 256);
+    L.total = o;
+    return L;
+}
+
+constexpr int kS = PassGeo<float, kWX>::S;
+constexpr int kCW32 = PassGeo<float, kWX>::CW;
+constexpr int kCW16 = PassGeo<__nv_bfloat16, kWX>::CW;
+
+template <typename K>
+int launch_coop(K kernel, void** args, int64_t units, size_t zero_bytes, void* ws, cudaStream_t st) {
+    const cspb_host::DeviceInfo di = cspb_host::device_info();
+    if (di.device < 0) return CSPB_ERR_CUDA;
+    if (!di.coop) return CSPB_ERR_UNSUPPORTED;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPassThreads, 0);
+    if (e != cudaSuccess || per_sm < 1) return e != cudaSuccess ? cspb_host::map_cuda_error(e) : CSPB_ERR_LAUNCH;
+    int64_t grid = int64_t(per_sm) * di.sms;
+    if (grid > units) grid = units;
+    if (grid < 1) grid = 1;
+    e = cudaMemsetAsync(ws, 0, zero_bytes, st);
+    if (e != cudaSuccess) return cspb_host::map_cuda_error(e);
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(unsigned(grid)), dim3(kPassThreads),
+                                    args, 0, st);
+    if (e != cudaSuccess) return CSPB_ERR_LAUNCH;
+    return CSPB_OK;
+}
+
+bool vec_aligned(const void* p, int64_t ld, int elem_bytes) {
+    return p == nullptr || (aligned(p, 16) && (ld * elem_bytes) % 16 == 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cspb_gemver_workspace_bytes(int64_t n) {
+    if (n < 1) return 0;
+    return pass_layout(n, kS, kCW32, 1, false).total;  // the f32 layout has the most chunks
+}
+
+int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    const int64_t n = d->n;
+    if (n < 1 || d->lda < n || (d->B && d->ldb < n)) return CSPB_ERR_ARGUMENT;
+    if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
+    if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
+    if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    const bool bf16 = d->a_dtype == CSPB_BF16;
+    const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    char* ws = static_cast<char*>(d->workspace);
+
+    GemverK g{};
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    g.units = L.units;
+    g.z = d->z;
+    g.beta = d->beta;
+    g.x = d->x;
+    PassArgs& p1 = g.p1;
+    p1.n = n;
+    p1.src = d->A;
+    p1.lds = d->lda;
+    p1.dst = d->B;
+    p1.ldd = d->ldb;
+    p1.u1 = d->u1; p1.v1 = d->v1; p1.u2 = d->u2; p1.v2 = d->v2;
+    p1.cyB = d->y;
+    p1.PB = reinterpret_cast<double*>(ws + L.off_PB);
+    p1.strips = L.strips;
+    p1.chunks = L.chunks;
+    PassArgs& p2 = g.p2;
+    p2 = p1;
+    p2.dst = nullptr;
+    p2.cyB = nullptr;
+    p2.PB = nullptr;
+    p2.xv = d->x;
+    p2.Wp = reinterpret_cast<float*>(ws + L.off_Wp);
+    p2.strip_done = reinterpret_cast<uint32_t*>(ws + L.off_done);
+    p2.rout1 = d->w;
+    p2.rscale1 = d->alpha;
+    const bool from_B = !bf16 && d->B != nullptr;
+    if (from_B) {
+        p2.src = d->B;
+        p2.lds = d->ldb;
+    }
+    const int eb = bf16 ? 2 : 4;
+    const int vec_ok = vec_aligned(d->A, d->lda, eb) && vec_aligned(d->B, d->ldb, 4) ? 1 : 0;
+    void* args[] = {&g, const_cast<int*>(&vec_ok)};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t zero = L.off_PA;  // ctrl + strip_done
+    if (bf16) return launch_coop(k_gemver<__nv_bfloat16, false>, args, L.units, zero, ws, st);
+    if (from_B) return launch_coop(k_gemver<float, true>, args, L.units, zero, ws, st);
+    return launch_coop(k_gemver<float, false>, args, L.units, zero, ws, st);
+}
+
+size_t cspb_bicgk_workspace_bytes(int64_t n) {
+    if (n < 1) return 0;
+    return pass_layout(n, kS, kCW32, 1, false).total;
+}
+
+int cspb_bicgk_fused(const cspb_bicgk_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    const int64_t n = d->n;
+    if (n < 1 || d->ldb < n || n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
+    if (!d->B || !d->p || !d->r || !d->q || !d->s) return CSPB_ERR_ARGUMENT;
+    if (d->b_dtype != CSPB_F32 && d->b_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    const bool bf16 = d->b_dtype == CSPB_BF16;
+    const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    char* ws = static_cast<char*>(d->workspace);
+    BicgkK g{};
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    g.units = L.units;
+    g.s = d->s;
+    PassArgs& p = g.p;
+    p.n = n;
+    p.src = d->B;
+    p.lds = d->ldb;
+    p.cyB = d->r;
+    p.PB = reinterpret_cast<double*>(ws + L.off_PB);
+    p.xv = d->p;
+    p.Wp = reinterpret_cast<float*>(ws + L.off_Wp);
+    p.strip_done = reinterpret_cast<uint32_t*>(ws + L.off_done);
+    p.rout1 = d->q;
+    p.rscale1 = 1.0f;
+    p.strips = L.strips;
+    p.chunks = L.chunks;
+    const int vec_ok = vec_aligned(d->B, d->ldb, bf16 ? 2 : 4) ? 1 : 0;
+    void* args[] = {&g, const_cast<int*>(&vec_ok)};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (bf16) return launch_coop(k_bicgk<__nv_bfloat16>, args, L.units, L.off_PA, ws, st);
+    return launch_coop(k_bicgk<float>, args, L.units, L.off_PA, ws, st);
+}
+
+size_t cspb_chain_workspace_bytes(int64_t n) {
+    if (n < 1) return 0;
+    return pass_layout(n, kS, kCW32, 2, true).total;
+}
+
+int cspb_gemver_chain(const cspb_chain_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    const int64_t n = d->n;
+    if (n < 1 || n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
+    const void* need[] = {d->A0, d->u1a, d->v1a, d->u2a, d->v2a, d->ya, d->u1b, d->v1b, d->u2b, d->v2b,
+                          d->B1, d->x1, d->w1, d->q, d->s, d->B2, d->x2, d->w2};
+    for (const void* p : need)
+        if (!p) return CSPB_ERR_ARGUMENT;
+    const PassLayout L = pass_layout(n, kS, kCW32, 2, true);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    char* ws = static_cast<char*>(d->workspace);
+    ChainK g{};
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    g.units = L.units;
+    g.za = d->za;
+    g.beta = d->beta;
+    g.x1 = d->x1;
+    g.s = d->s;
+    g.x2 = d->x2;
+    uint32_t* done = reinterpret_cast<uint32_t*>(ws + L.off_done);
+    double* PA = reinterpret_cast<double*>(ws + L.off_PA);
+    double* PB = reinterpret_cast<double*>(ws + L.off_PB);
+    float* Wp = reinterpret_cast<float*>(ws + L.off_Wp);
+    PassArgs base{};
+    base.n = n;
+    base.lds = n;
+    base.ldd = n;
+    base.strips = L.strips;
+    base.chunks = L.chunks;
+    // 1
+    g.p1 = base;
+    g.p1.src = d->A0;
+    g.p1.dst = d->B1;
+    g.p1.u1 = d->u1a; g.p1.v1 = d->v1a; g.p1.u2 = d->u2a; g.p1.v2 = d->v2a;
+    g.p1.cyB = d->ya;
+    g.p1.PB = PB;
+    // 2
+    g.p2 = base;
+    g.p2.src = d->B1;
+    g.p2.xv = d->x1;
+    g.p2.Wp = Wp;
+    g.p2.strip_done = done;
+    g.p2.rout1 = d->w1;
+    g.p2.rscale1 = d->alpha;
+    g.p2.rout2 = d->q;
+    g.p2.rscale2 = 1.0f;
+    // 3
+    g.p3 = base;
+    g.p3.src = d->B1;
+    g.p3.dst = d->B2;
+    g.p3.u1 = d->u1b; g.p3.v1 = d->v1b; g.p3.u2 = d->u2b; g.p3.v2 = d->v2b;
+    g.p3.cyA = d->w1;
+    g.p3.PA = PA;
+    g.p3.cyB = d->q;
+    g.p3.PB = PB;
+    // 4
+    g.p4 = base;
+    g.p4.src = d->B2;
+    g.p4.xv = d->x2;
+    g.p4.Wp = Wp;
+    g.p4.strip_done = done + L.strips;
+    g.p4.rout1 = d->w2;
+    g.p4.rscale1 = d->alpha;
+    const int vec_ok = (vec_aligned(d->A0, n, 4) && vec_aligned(d->B1, n, 4) && vec_aligned(d->B2, n, 4)) ? 1 : 0;
+    void* args[] = {&g, const_cast<int*>(&vec_ok)};
+    return launch_coop(k_chain, args, L.units, L.off_PA, ws, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

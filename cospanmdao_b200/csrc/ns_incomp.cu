@@ -1,0 +1,285 @@
+// ns_incomp.cu — the incompressible Navier-Stokes residual on a 2D periodic collocated grid, one streaming kernel.
+//
+//   r_u = u·∂u/∂x + v·∂u/∂y + ∂p/∂x − ν∇²u
+//   r_v = u·∂v/∂x + v·∂v/∂y + ∂p/∂y − ν∇²v
+//   r_c = ∂u/∂x + ∂v/∂y
+// with ∂f/∂x ≈ (f[i+1] − f[i−1]) / 2h and ∇²f ≈ ((f[i+1]−f) + (f[i−1]−f) + (f[j+1]−f) + (f[j−1]−f)) / h². The
+// neighbour differences are formed first: fields whose neighbours lie within a factor 2 of each other subtract exactly
+// in f32 (Sterbenz), so the only roundings are the few that follow.
+//
+// No reference code computes this residual (the reference's ns-residual is the compressible one, ns_comp.cu); the
+// formula is the workload's definition, and the oracle is an f64 restatement of it.
+//
+// Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. Work item = one warp on a strip of 32·VEC columns × H rows:
+// each lane owns VEC consecutive cells of a row (one 16-byte load per field per row), x-neighbours come from the
+// adjacent lanes by shuffle (the warp's edge lanes load one wrapped scalar), and the warp marches down its rows
+// keeping the rows above and below in registers, two rows of loads in flight. Each input is read from HBM once (the
+// 2 halo rows of a strip are L2 hits of the neighbouring strip); 24 B/cell in f32 storage, 18 B/cell in bf16.
+//
+// The three squared norms are accumulated per thread in f64, reduced per warp by a fixed xor tree, per block in warp
+// order, and across blocks in block order by the last block to finish: bit-identical on every run.
+#include "common.cuh"
+
+namespace cspb {
+
+constexpr int kNsiThreads = 256;
+constexpr int kNsiWarps = kNsiThreads / 32;
+
+struct NsiK {
+    int nx, ny, H;
+    int segs;          // column segments of 32·VEC cells
+    int64_t items;     // segs × row strips
+    float inv2h, invh2, nu;
+    const void *u, *v, *p;
+    float *ru, *rv, *rc;
+    double* norms;
+    double* part;      // [blocks][3]
+    uint32_t* ctrl;
+};
+
+template <typename T, int VEC>
+struct NsiRow {
+    float c[VEC];  // this lane's cells
+    float l, r;    // the wrapped neighbours outside the lane's cells when this lane needs them from memory
+};
+
+template <typename T>
+__device__ __forceinline__ float ld1(const T* p, int64_t i) {
+    if constexpr (sizeof(T) == 4) return __ldg(reinterpret_cast<const float*>(p) + i);
+    else return __bfloat162float(p[i]);
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void load_cells(const T* f, int64_t rowoff, int c0, int ncols, float (&out)[VEC]) {
+    if constexpr (VEC == 4 && sizeof(T) == 4) {
+        if (ncols == 4) {
+            const float4 q = ld_stream_f4(reinterpret_cast<const float*>(f) + rowoff + c0);
+            out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
+            return;
+        }
+    } else if constexpr (VEC == 8 && sizeof(T) == 2) {
+        if (ncols == 8) {
+            const uint4 q = ld_stream_u4(f + rowoff + c0);
+            out[0] = bf16_lo(q.x); out[1] = bf16_hi(q.x); out[2] = bf16_lo(q.y); out[3] = bf16_hi(q.y);
+            out[4] = bf16_lo(q.z); out[5] = bf16_hi(q.z); out[6] = bf16_lo(q.w); out[7] = bf16_hi(q.w);
+            return;
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) out[e] = e < ncols ? ld1(f, rowoff + c0 + e) : 0.f;
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void load_row(const T* f, int nx, int64_t rowoff, int c0, int ncols, bool need_l, bool need_r,
+                                         NsiRow<T, VEC>& row) {
+    load_cells<T, VEC>(f, rowoff, c0, ncols, row.c);
+    row.l = need_l ? ld1(f, rowoff + (c0 == 0 ? nx - 1 : c0 - 1)) : 0.f;
+    row.r = need_r ? ld1(f, rowoff + ((c0 + ncols) % nx)) : 0.f;
+}
+
+// x-neighbours of the lane's cells: left of cell 0 and right of cell VEC-1, from the adjacent lanes or memory.
+template <typename T, int VEC>
+__device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool need_l, bool need_r, float& left, float& right) {
+    const float from_left = __shfl_up_sync(0xffffffffu, row.c[VEC - 1], 1);
+    const float from_right = __shfl_down_sync(0xffffffffu, row.c[0], 1);
+    left = need_l ? row.l : from_left;
+    right = need_r ? row.r : from_right;
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t item = int64_t(blockIdx.x) * kNsiWarps + warp;
+    double su = 0.0, sv = 0.0, sc = 0.0;
+    if (item < g.items) {  // warp-uniform
+        const int seg = int(item % g.segs);
+        const int strip = int(item / g.segs);
+        const int c0 = seg * 32 * VEC + lane * VEC;
+        const int ncols = c0 >= g.nx ? 0 : (g.nx - c0 >= VEC ? VEC : g.nx - c0);
+        const bool active = ncols > 0;
+        // the lane needs its left neighbour from memory when it is the first lane; its right one when it is the
+        // last lane of the warp or the last lane holding cells
+        const bool need_l = lane == 0;
+        const bool need_r = active && (lane == 31 || c0 + VEC >= g.nx);
+        const int j0 = strip * g.H;
+        const int j1 = min(g.ny, j0 + g.H);
+        const T* U = static_cast<const T*>(g.u);
+        const T* V = static_cast<const T*>(g.v);
+        const T* P = static_cast<const T*>(g.p);
+        const int64_t nx = g.nx;
+        auto wrapj = [&](int j) { return j < 0 ? j + g.ny : (j >= g.ny ? j - g.ny : j); };
+
+        NsiRow<T, VEC> u0, u1, u2, v0, v1, v2, p0, p1, p2;  // rows j-1, j, j+1
+        NsiRow<T, VEC> u3, v3, p3;                          // row j+2 (in flight)
+        {
+            const int64_t ra = int64_t(wrapj(j0 - 1)) * nx, rb = int64_t(j0) * nx, rc = int64_t(wrapj(j0 + 1)) * nx;
+            load_row<T, VEC>(U, g.nx, ra, c0, ncols, need_l, need_r, u0);
+            load_row<T, VEC>(V, g.nx, ra, c0, ncols, need_l, need_r, v0);
+            load_row<T, VEC>(P, g.nx, ra, c0, ncols, need_l, need_r, p0);
+            load_row<T, VEC>(U, g.nx, rb, c0, ncols, need_l, need_r, u1);
+            load_row<T, VEC>(V, g.nx, rb, c0, ncols, need_l, need_r, v1);
+            load_row<T, VEC>(P, g.nx, rb, c0, ncols, need_l, need_r, p1);
+            load_row<T, VEC>(U, g.nx, rc, c0, ncols, need_l, need_r, u2);
+            load_row<T, VEC>(V, g.nx, rc, c0, ncols, need_l, need_r, v2);
+            load_row<T, VEC>(P, g.nx, rc, c0, ncols, need_l, need_r, p2);
+        }
+        const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
+        for (int j = j0; j < j1; ++j) {
+            if (j + 1 < j1) {  // prefetch row j+2 while row j is computed
+                const int64_t rd = int64_t(wrapj(j + 2)) * nx;
+                load_row<T, VEC>(U, g.nx, rd, c0, ncols, need_l, need_r, u3);
+                load_row<T, VEC>(V, g.nx, rd, c0, ncols, need_l, need_r, v3);
+                load_row<T, VEC>(P, g.nx, rd, c0, ncols, need_l, need_r, p3);
+            }
+            float ul, ur, vl, vr, pl, pr;
+            x_neighbours<T, VEC>(u1, need_l, need_r, ul, ur);
+            x_neighbours<T, VEC>(v1, need_l, need_r, vl, vr);
+            x_neighbours<T, VEC>(p1, need_l, need_r, pl, pr);
+            float oru[VEC], orv[VEC], orc[VEC];
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+                const float uc = u1.c[e], vc = v1.c[e];
+                const float uW = e == 0 ? ul : u1.c[e - 1], uE = e == VEC - 1 ? ur : u1.c[e + 1];
+                const float vW = e == 0 ? vl : v1.c[e - 1], vE = e == VEC - 1 ? vr : v1.c[e + 1];
+                const float pW = e == 0 ? pl : p1.c[e - 1], pE = e == VEC - 1 ? pr : p1.c[e + 1];
+                const float uS = u0.c[e], uN = u2.c[e], vS = v0.c[e], vN = v2.c[e], pS = p0.c[e], pN = p2.c[e];
+                const float dudx = (uE - uW) * inv2h, dudy = (uN - uS) * inv2h;
+                const float dvdx = (vE - vW) * inv2h, dvdy = (vN - vS) * inv2h;
+                const float dpdx = (pE - pW) * inv2h, dpdy = (pN - pS) * inv2h;
+                const float lapu = (((uE - uc) + (uW - uc)) + ((uN - uc) + (uS - uc))) * invh2;
+                const float lapv = (((vE - vc) + (vW - vc)) + ((vN - vc) + (vS - vc))) * invh2;
+                const float ru = ((uc * dudx + vc * dudy) + dpdx) - nu * lapu;
+                const float rv = ((uc * dvdx + vc * dvdy) + dpdy) - nu * lapv;
+                const float rc = dudx + dvdy;
+                oru[e] = ru; orv[e] = rv; orc[e] = rc;
+                if (e < ncols) {
+                    su = __fma_rn(double(ru), double(ru), su);
+                    sv = __fma_rn(double(rv), double(rv), sv);
+                    sc = __fma_rn(double(rc), double(rc), sc);
+                }
+            }
+            const int64_t ro = int64_t(j) * nx + c0;
+            if (ncols == VEC && (VEC % 4) == 0) {
+#pragma unroll
+                for (int q = 0; q < VEC / 4; ++q) {
+                    st_f4(g.ru + ro + 4 * q, make_float4(oru[4 * q], oru[4 * q + 1], oru[4 * q + 2], oru[4 * q + 3]));
+                    st_f4(g.rv + ro + 4 * q, make_float4(orv[4 * q], orv[4 * q + 1], orv[4 * q + 2], orv[4 * q + 3]));
+                    st_f4(g.rc + ro + 4 * q, make_float4(orc[4 * q], orc[4 * q + 1], orc[4 * q + 2], orc[4 * q + 3]));
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < VEC; ++e)
+                    if (e < ncols) { g.ru[ro + e] = oru[e]; g.rv[ro + e] = orv[e]; g.rc[ro + e] = orc[e]; }
+            }
+            u0 = u1; u1 = u2; u2 = u3;
+            v0 = v1; v1 = v2; v2 = v3;
+            p0 = p1; p1 = p2; p2 = p3;
+        }
+    }
+    // ---- the norms: warp xor tree, block in warp order, grid in block order by the last block ----
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        su += __shfl_xor_sync(0xffffffffu, su, off);
+        sv += __shfl_xor_sync(0xffffffffu, sv, off);
+        sc += __shfl_xor_sync(0xffffffffu, sc, off);
+    }
+    __shared__ double s_red[kNsiWarps][3];
+    __shared__ int s_last;
+    if (lane == 0) { s_red[warp][0] = su; s_red[warp][1] = sv; s_red[warp][2] = sc; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double s = s_red[0][threadIdx.x];
+        for (int w = 1; w < kNsiWarps; ++w) s += s_red[w][threadIdx.x];
+        g.part[int64_t(blockIdx.x) * 3 + threadIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(g.ctrl + kDone0, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last && threadIdx.x < 3) {
+        __threadfence();
+        double s = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(g.part + int64_t(b) * 3 + threadIdx.x);
+        if (g.norms) g.norms[threadIdx.x] = sqrt(s);
+    }
+}
+
+}  // namespace cspb
+
+using namespace cspb;
+using cspb_host::align_up;
+using cspb_host::aligned;
+
+namespace {
+
+struct NsiPlan {
+    int vec = 4, H = 32, segs = 0;
+    int64_t items = 0, blocks = 0;
+    size_t ws = 0;
+};
+
+// The row-strip height depends on the grid alone (never on the device), so the sums run in the same order anywhere.
+NsiPlan nsi_plan(int nx, int ny, int vec) {
+    NsiPlan p;
+    p.vec = vec;
+    p.segs = (nx + 32 * vec - 1) / (32 * vec);
+    p.H = 32;
+    while (p.H > 4 && int64_t(p.segs) * ((ny + p.H - 1) / p.H) < 4096) p.H /= 2;
+    p.items = int64_t(p.segs) * ((ny + p.H - 1) / p.H);
+    p.blocks = (p.items + kNsiWarps - 1) / kNsiWarps;
+    p.ws = align_up(kCtrlBytes + size_t(p.blocks) * 3 * sizeof(double), 256);
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny) {
+    if (nx < 3 || ny < 3) return 0;
+    // the scalar plan (vec 1) has the most blocks
+    return nsi_plan(nx, ny, 1).ws;
+}
+
+int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    if (d->nx < 3 || d->ny < 3) return CSPB_ERR_ARGUMENT;
+    if (!d->u || !d->v || !d->p || !d->ru || !d->rv || !d->rc) return CSPB_ERR_ARGUMENT;
+    if (!(d->h > 0.0) || !(d->nu >= 0.0)) return CSPB_ERR_ARGUMENT;
+    if (d->dtype != CSPB_F32 && d->dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    const bool bf16 = d->dtype == CSPB_BF16;
+    const int vfast = bf16 ? 8 : 4;
+    const bool in_al = aligned(d->u, 16) && aligned(d->v, 16) && aligned(d->p, 16);
+    const bool out_al = aligned(d->ru, 16) && aligned(d->rv, 16) && aligned(d->rc, 16);
+    const bool fast = in_al && out_al && d->nx % vfast == 0;
+    const NsiPlan P = nsi_plan(d->nx, d->ny, fast ? vfast : 1);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < P.ws) return CSPB_ERR_WORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
+    NsiK g{};
+    g.nx = d->nx;
+    g.ny = d->ny;
+    g.H = P.H;
+    g.segs = P.segs;
+    g.items = P.items;
+    g.inv2h = float(1.0 / (2.0 * d->h));
+    g.invh2 = float(1.0 / (d->h * d->h));
+    g.nu = float(d->nu);
+    g.u = d->u; g.v = d->v; g.p = d->p;
+    g.ru = d->ru; g.rv = d->rv; g.rc = d->rc;
+    g.norms = d->norms;
+    g.ctrl = static_cast<uint32_t*>(d->workspace);
+    g.part = reinterpret_cast<double*>(static_cast<char*>(d->workspace) + kCtrlBytes);
+    const dim3 grid(unsigned(P.blocks)), block(kNsiThreads);
+    if (bf16) {
+        if (fast) k_ns_incomp<__nv_bfloat16, 8><<<grid, block, 0, st>>>(g);
+        else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
+    } else {
+        if (fast) k_ns_incomp<float, 4><<<grid, block, 0, st>>>(g);
+        else k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
+    }
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+}  // extern "C"

@@ -1,0 +1,307 @@
+// rowpass.cuh — the streaming matrix pass every GEMVER-family kernel of libcspb is built from.
+//
+// A pass walks an n×n row-major matrix in UNITS of S rows × CW columns (a strip × a column chunk). A 256-thread block
+// owns one unit at a time: its 8 warps form a WX × WY grid, each warp covers 32 rows × (32 · VEC) columns, each lane
+// VEC consecutive columns (one 16-byte load per row: 4 f32 or 8 bf16). Per loaded row a lane can
+//   - add the rank-2 update (a + u1[i]·v1[j]) + u2[i]·v2[j]   (Rank2Update, examples/gemver-chain/components.hpp:85-97)
+//   - store the updated row                                    (the B / Â output)
+//   - accumulate column sums Σ_i a[i][j]·cyA[i] and Σ_i b[i][j]·cyB[i] in f64 (GemvTPartial + ColReduce,
+//     components.hpp:142-219, and BicgkOnePass's Ps, components.hpp:306-320)
+//   - form row dots Σ_j b[i][j]·xv[j]                           (Gemv, components.hpp:237-265; BicgkOnePass's Pq)
+// Column sums leave the unit as one f64 partial per (strip, column); row dots as one f32 partial per (chunk, row),
+// and the block that completes the last chunk of a strip combines them into the row results. Every sum runs in an
+// order fixed by (n, S, CW) alone — never by the grid size, the scheduling or other work on the GPU — so a result is
+// bit-identical however it was launched.
+#pragma once
+
+#include "common.cuh"
+
+namespace cspb {
+
+template <typename T> struct VecOf;
+template <> struct VecOf<float> { static constexpr int N = 4; static constexpr int RB = 8; };
+template <> struct VecOf<__nv_bfloat16> { static constexpr int N = 8; static constexpr int RB = 4; };
+
+constexpr int kPassThreads = 256;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Geometry of a pass (WX warps across columns).
+template <typename T, int WX>
+struct PassGeo {
+    static constexpr int VEC = VecOf<T>::N;
+    static constexpr int WY = 8 / WX;
+    static constexpr int S = WY * 32;        // rows per strip
+    static constexpr int CW = WX * 32 * VEC; // columns per chunk
+};
+
+struct PassArgs {
+    int64_t n;
+    const void* src;   // the matrix read (T, or f32 when the pass reads B)
+    int64_t lds;
+    float* dst;        // STORE target (f32); NULL: no store
+    int64_t ldd;
+    const float *u1, *v1, *u2, *v2;  // rank-2 update
+    const float* cyA;  // column sums of the loaded values, weighted per row
+    double* PA;        // [strips][n]
+    const float* cyB;  // column sums of the updated values
+    double* PB;        // [strips][n]
+    const float* xv;   // row dots with this column vector
+    float* Wp;         // [chunks][n]
+    uint32_t* strip_done;  // [strips]
+    float* rout1;      // row results: rout1[i] = rscale1 · Σ_j b[i][j] xv[j]
+    float rscale1;
+    float* rout2;      // optional second copy with its own scale
+    float rscale2;
+    int64_t strips, chunks;
+};
+
+// 32 values per lane -> lane L holds the warp-wide sum of value L (31 shuffles, a fixed tree).
+__device__ __forceinline__ float transpose_reduce32(float (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < off; ++k) {
+            const float send = upper ? v[k] : v[k + off];
+            const float keep = upper ? v[k + off] : v[k];
+            v[k] = keep + __shfl_xor_sync(kFull, send, off);
+        }
+    }
+    return v[0];
+}
+
+// One lane's VEC elements of a row. NC: the matrix is read-only for the whole kernel (an input), so the
+// non-coherent path with evict-first is allowed; otherwise (a matrix written earlier in the same kernel) the load
+// goes through L2 coherently.
+template <typename T, bool NC>
+__device__ __forceinline__ void load_vec(const T* row, int64_t c0, int ncols, bool vec_ok, float (&out)[VecOf<T>::N]);
+
+template <>
+__device__ __forceinline__ void load_vec<float, true>(const float* row, int64_t c0, int ncols, bool vec_ok, float (&out)[4]) {
+    if (vec_ok && ncols == 4) {
+        const float4 v = ld_stream_f4(row + c0);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) out[e] = e < ncols ? __ldg(row + c0 + e) : 0.0f;
+    }
+}
+template <>
+__device__ __forceinline__ void load_vec<float, false>(const float* row, int64_t c0, int ncols, bool vec_ok, float (&out)[4]) {
+    if (vec_ok && ncols == 4) {
+        const float4 v = ld_cg_f4(row + c0);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) out[e] = e < ncols ? __ldcg(row + c0 + e) : 0.0f;
+    }
+}
+
+template <>
+__device__ __forceinline__ void load_vec<__nv_bfloat16, true>(const __nv_bfloat16* row, int64_t c0, int ncols, bool vec_ok,
+                                                              float (&out)[8]) {
+    if (vec_ok && ncols == 8) {
+        const uint4 v = ld_stream_u4(row + c0);
+        out[0] = bf16_lo(v.x); out[1] = bf16_hi(v.x);
+        out[2] = bf16_lo(v.y); out[3] = bf16_hi(v.y);
+        out[4] = bf16_lo(v.z); out[5] = bf16_hi(v.z);
+        out[6] = bf16_lo(v.w); out[7] = bf16_hi(v.w);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) out[e] = e < ncols ? __bfloat162float(row[c0 + e]) : 0.0f;
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void store_vec(float* row, int64_t c0, int ncols, bool vec_ok, const float (&b)[VEC]) {
+    if (vec_ok && ncols == VEC) {
+#pragma unroll
+        for (int q = 0; q < VEC / 4; ++q) st_f4(row + c0 + 4 * q, make_float4(b[4 * q], b[4 * q + 1], b[4 * q + 2], b[4 * q + 3]));
+    } else {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e)
+            if (e < ncols) row[c0 + e] = b[e];
+    }
+}
+
+// Shared memory a pass needs (bytes).
+template <typename T, int WX>
+__host__ __device__ constexpr size_t pass_smem_bytes() {
+    using G = PassGeo<T, WX>;
+    const size_t cs = size_t(G::WY) * G::CW * sizeof(double);
+    const size_t rd = size_t(WX) * G::S * sizeof(float);
+    return cs > rd ? cs : rd;
+}
+
+// One unit of a pass. LT: the loaded element type; NC: see load_vec. Flags: RANK2 add the update; CSA / CSB column sums of the loaded /
+// updated values; RDOT row dots of the updated values. Stores happen when a.dst != NULL.
+template <typename LT, int WX, bool NC, bool RANK2, bool CSA, bool CSB, bool RDOT>
+__device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
+    using G = PassGeo<LT, WX>;
+    constexpr int VEC = G::VEC, WY = G::WY, S = G::S, CW = G::CW, RB = VecOf<LT>::RB;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wx = warp % WX, wy = warp / WX;
+    const int64_t n = a.n;
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    const int64_t r0 = strip * S + wy * 32;
+    const int64_t c0 = chunk * CW + int64_t(wx * 32 + lane) * VEC;
+    const int64_t rem_r = n - r0, rem_c = n - c0;
+    const int nrows = rem_r <= 0 ? 0 : (rem_r >= 32 ? 32 : int(rem_r));
+    const int ncols = rem_c <= 0 ? 0 : (rem_c >= VEC ? VEC : int(rem_c));
+
+    float u1r = 0.f, u2r = 0.f, cyar = 0.f, cybr = 0.f;
+    if (lane < nrows) {
+        const int64_t row = r0 + lane;
+        if (RANK2) { u1r = __ldcg(a.u1 + row); u2r = __ldcg(a.u2 + row); }
+        if (CSA) cyar = __ldcg(a.cyA + row);
+        if (CSB) cybr = __ldcg(a.cyB + row);
+    }
+    float v1c[VEC], v2c[VEC], xc[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) {
+        const bool ok = e < ncols;
+        v1c[e] = (RANK2 && ok) ? __ldcg(a.v1 + c0 + e) : 0.f;
+        v2c[e] = (RANK2 && ok) ? __ldcg(a.v2 + c0 + e) : 0.f;
+        xc[e] = (RDOT && ok) ? __ldcg(a.xv + c0 + e) : 0.f;
+    }
+    double accA[VEC], accB[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) { accA[e] = 0.0; accB[e] = 0.0; }
+    float racc[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) racc[k] = 0.f;
+
+    const LT* src = static_cast<const LT*>(a.src);
+    const bool store = a.dst != nullptr;
+
+#pragma unroll
+    for (int kb = 0; kb < 32; kb += RB) {
+        if (kb < nrows) {  // warp-uniform
+            float val[RB][VEC];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                if (kb + k < nrows && ncols > 0) load_vec<LT, NC>(src + (r0 + kb + k) * a.lds, c0, ncols, vec_ok, val[k]);
+                else {
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) val[k][e] = 0.f;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const int kk = kb + k;
+                const float u1k = __shfl_sync(kFull, u1r, kk);
+                const float u2k = __shfl_sync(kFull, u2r, kk);
+                const float cyak = __shfl_sync(kFull, cyar, kk);
+                const float cybk = __shfl_sync(kFull, cybr, kk);
+                if (kk < nrows) {
+                    float b[VEC];
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e)
+                        b[e] = RANK2 ? __fadd_rn(__fadd_rn(val[k][e], __fmul_rn(u1k, v1c[e])), __fmul_rn(u2k, v2c[e]))
+                                     : val[k][e];
+                    if (store && ncols > 0) store_vec<VEC>(a.dst + (r0 + kk) * a.ldd, c0, ncols, vec_ok, b);
+                    if (CSA) {
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) accA[e] = __fma_rn(double(val[k][e]), double(cyak), accA[e]);
+                    }
+                    if (CSB) {
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) accB[e] = __fma_rn(double(b[e]), double(cybk), accB[e]);
+                    }
+                    if (RDOT) {
+                        float d = 0.f;
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) d = fmaf(b[e], xc[e], d);
+                        racc[kk] = d;
+                    }
+                }
+            }
+        }
+    }
+
+    // ---- column sums: combine the WY warps of a column in a fixed order, one f64 partial per (strip, column) ----
+    if (CSA || CSB) {
+        double* red = reinterpret_cast<double*>(smem);
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            if ((which == 0 && !CSA) || (which == 1 && !CSB)) continue;
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) red[wy * CW + (wx * 32 + lane) * VEC + e] = which == 0 ? accA[e] : accB[e];
+            __syncthreads();
+            double* P = which == 0 ? a.PA : a.PB;
+            for (int t = threadIdx.x; t < CW; t += kPassThreads) {
+                const int64_t col = chunk * CW + t;
+                if (col < n) {
+                    double s = red[t];
+#pragma unroll
+                    for (int y = 1; y < WY; ++y) s += red[y * CW + t];
+                    P[strip * n + col] = s;
+                }
+            }
+        }
+    }
+
+    // ---- row dots: warp tree, then the WX warps of a row in order; the last chunk of a strip finishes its rows ----
+    if (RDOT) {
+        const float v = transpose_reduce32(racc);
+        float* red2 = reinterpret_cast<float*>(smem);
+        __syncthreads();
+        red2[wx * S + wy * 32 + lane] = v;
+        __syncthreads();
+        for (int t = threadIdx.x; t < S; t += kPassThreads) {
+            const int64_t row = strip * S + t;
+            if (row < n) {
+                float s = red2[t];
+#pragma unroll
+                for (int x = 1; x < WX; ++x) s += red2[x * S + t];
+                a.Wp[chunk * n + row] = s;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        __shared__ int s_last;
+        if (threadIdx.x == 0) s_last = atomicAdd(a.strip_done + strip, 1u) == uint32_t(a.chunks - 1);
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            for (int t = threadIdx.x; t < S; t += kPassThreads) {
+                const int64_t row = strip * S + t;
+                if (row < n) {
+                    float s = 0.f;
+                    for (int64_t c = 0; c < a.chunks; ++c) s += __ldcg(a.Wp + c * n + row);
+                    a.rout1[row] = a.rscale1 * s;
+                    if (a.rout2) a.rout2[row] = a.rscale2 * s;
+                }
+            }
+        }
+    }
+}
+
+// out[j] = (z ? z[j] : 0) + scale · Σ_s P[s][j] over all strips in index order (f64), rounded once to f32.
+// Four lanes share a column: lane q sums strips q, q+4, ...; the four partials combine as ((p0+p1)+(p2+p3)).
+// Called by every thread of the grid; no barrier inside.
+__device__ __forceinline__ void colsum_finish(const double* P, int64_t strips, int64_t n, const float* z, float scale,
+                                              float* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t base = gtid - lane; base < 4 * n; base += gthreads) {
+        const int64_t item = base + lane;
+        const bool valid = item < 4 * n;
+        const int64_t j = item >> 2;
+        const int q = int(item & 3);
+        double s = 0.0;
+        if (valid)
+            for (int64_t st = q; st < strips; st += 4) s += __ldcg(P + st * n + j);
+        s += __shfl_xor_sync(kFull, s, 1);
+        s += __shfl_xor_sync(kFull, s, 2);
+        if (valid && q == 0) {
+            const double zz = z ? double(__ldcg(z + j)) : 0.0;
+            out[j] = float(zz + double(scale) * s);
+        }
+    }
+}
+
+}  // namespace cspb

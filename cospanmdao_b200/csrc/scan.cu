@@ -1,0 +1,407 @@
+// scan.cu — single-pass exclusive scan (decoupled lookback) of u32 / u64, and the fused ragged-column builder.
+//
+// Replaces cs::detail::exclusive_scan_u32 (cospanmdao/include/naga/cospan/device_scan.hpp:46-110), a recursive
+// reduce-then-scan of 3 kernels per level with temporary allocations, by ONE launch over tiles of 256 threads × ITEMS:
+//   1. a tile takes a dynamic tile index (so every tile it waits on has started), loads its items coalesced through
+//      shared memory, and scans them in the block;
+//   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 32 at a time, adding
+//      aggregates until it meets a published inclusive prefix (flag 2), and publishes its own inclusive prefix;
+//   3. it writes its outputs coalesced; the last tile writes out[n], the total.
+// Integer addition mod 2^32 / 2^64 is associative, so the result is bit-identical to std::exclusive_scan whatever the
+// order of the lookback. Every wait is bounded (common.cuh).
+//
+// cspb_build_column fuses the three other launches of cs::detail::build_column (shape_hook.hpp:265-338) into the same
+// kernel: the narrowing of the source values (negative -> flag 1, past 32 bits -> flag 2) happens as the tile loads,
+// the running sum is carried in 64 bits so that a total past 2^32 - 1 is known exactly (the reference detects the same
+// thing as a decrease of the wrapped u32 offsets), and the last tile writes [total, flag].
+#include "common.cuh"
+
+namespace cspb {
+
+constexpr int kScanThreads = 256;
+
+template <typename T> struct ScanItems;
+template <> struct ScanItems<uint32_t> { static constexpr int N = 16; };
+template <> struct ScanItems<uint64_t> { static constexpr int N = 8; };
+
+// Where the items come from. Plain: in[i]. Column: narrowed count values of src[i * k] of an integer dtype.
+struct ScanSrc {
+    const void* in;
+    int32_t dtype;  // CSPB_U32 / CSPB_U64 for a plain scan; CSPB_I32/U32/I64/U64 for a column
+    int64_t k;      // column stride (build_column), 1 for a plain scan
+    bool column;    // narrow + flags
+    uint32_t* extents;  // column: the narrowed values are written here
+};
+
+// The value of item i (always < n), and the flag bits it raises.
+template <typename T>
+__device__ __forceinline__ T scan_item(const ScanSrc& s, int64_t i, uint32_t& flag) {
+    if (!s.column) return static_cast<const T*>(s.in)[i];
+    uint32_t x = 0;
+    switch (s.dtype) {
+        case CSPB_I32: {
+            const int32_t v = static_cast<const int32_t*>(s.in)[i * s.k];
+            if (v < 0) flag |= 1u; else x = uint32_t(v);
+            break;
+        }
+        case CSPB_U32: x = static_cast<const uint32_t*>(s.in)[i * s.k]; break;
+        case CSPB_I64: {
+            const int64_t v = static_cast<const int64_t*>(s.in)[i * s.k];
+            if (v < 0) flag |= 1u;
+            else if (v > int64_t(0xffffffffll)) flag |= 2u;
+            else x = uint32_t(v);
+            break;
+        }
+        default: {
+            const uint64_t v = static_cast<const uint64_t*>(s.in)[i * s.k];
+            if (v > 0xffffffffull) flag |= 2u; else x = uint32_t(v);
+            break;
+        }
+    }
+    s.extents[i] = x;
+    return T(x);
+}
+
+template <typename T>
+struct ScanK {
+    ScanSrc src;
+    T* out;             // n + 1 (column: u32 offsets, T = u64 carries the exact running sum)
+    uint32_t* out32;    // column mode: the u32 offsets are written here instead of out
+    int64_t n;
+    int64_t tiles;
+    uint32_t* ctrl;
+    uint32_t* tflag;    // per tile: 0 nothing, 1 aggregate, 2 inclusive prefix
+    T* tagg;
+    T* tinc;
+    uint32_t* total_flag;  // column mode: [total, flag]
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const T o = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += o;
+    }
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
+    constexpr int IT = ScanItems<T>::N;
+    constexpr int TILE = kScanThreads * IT;
+    constexpr int PAD = TILE + TILE / 32;
+    __shared__ T sm[PAD];
+    __shared__ T s_warp[kScanThreads / 32];
+    __shared__ T s_prefix;
+    __shared__ uint32_t s_flag;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+
+    const uint32_t tile = grab_work(g.ctrl, kWork0);
+    if (tile >= g.tiles) return;
+    if (t == 0) s_flag = 0;
+    const int64_t base = int64_t(tile) * TILE;
+
+    // 1. striped coalesced load -> shared (padded) -> blocked items
+    uint32_t flag = 0;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int idx = k * kScanThreads + t;
+        const int64_t i = base + idx;
+        sm[idx + idx / 32] = i < g.n ? scan_item<T>(g.src, i, flag) : T(0);
+    }
+    __syncthreads();
+    if (flag) atomicOr(&s_flag, flag);
+    T v[IT];
+    T run = 0;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int idx = t * IT + k;
+        v[k] = run;  // exclusive within the thread
+        run += sm[idx + idx / 32];
+    }
+    // block scan of the thread totals
+    const T incl = warp_incl_scan(run);
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T wv = lane < kScanThreads / 32 ? s_warp[lane] : T(0);
+        const T wi = warp_incl_scan(wv);
+        if (lane < kScanThreads / 32) s_warp[lane] = wi - wv;  // exclusive warp offsets
+    }
+    __syncthreads();
+    const T thread_excl = s_warp[warp] + incl - run;
+    __shared__ T s_agg;
+    if (t == kScanThreads - 1) s_agg = thread_excl + run;
+    __syncthreads();
+    const T agg = s_agg;
+
+    // 2. publish the aggregate, look back, publish the inclusive prefix
+    if (warp == 0) {
+        T prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) {
+                g.tinc[0] = agg;
+                __threadfence();
+                st_release(g.tflag, 2u);
+            }
+        } else {
+            if (lane == 0) {
+                g.tagg[tile] = agg;
+                __threadfence();
+                st_release(g.tflag + tile, 1u);
+            }
+            int64_t look = int64_t(tile) - 1;  // the nearest predecessor this window starts at
+            bool done = false;
+            const unsigned long long t0 = globaltimer_ns();
+            while (!done) {
+                const int64_t p = look - lane;  // lane 0 is the nearest
+                uint32_t f = p >= 0 ? ld_acquire(g.tflag + p) : 2u;
+                // wait until every lane of the window has something published (lane 0 decides to give up)
+                for (;;) {
+                    if (__all_sync(0xffffffffu, f != 0u)) break;
+                    int give_up = 0;
+                    if (lane == 0) {
+                        if (status_bad(g.ctrl)) give_up = 1;
+                        else if (globaltimer_ns() - t0 > kWaitBudgetNs) {
+                            set_status(g.ctrl, CSPB_DEV_TIMEOUT);
+                            give_up = 1;
+                        }
+                    }
+                    if (__shfl_sync(0xffffffffu, give_up, 0)) {
+                        done = true;
+                        break;
+                    }
+                    __nanosleep(64);
+                    if (f == 0u) f = ld_acquire(g.tflag + p);
+                }
+                if (done) break;
+                const unsigned incl_mask = __ballot_sync(0xffffffffu, f == 2u);
+                // the nearest lane holding an inclusive prefix: lanes before it contribute aggregates
+                const int stop = incl_mask ? __ffs(incl_mask) - 1 : 32;
+                T c = 0;
+                if (lane < stop) c = p >= 0 ? __ldcg(g.tagg + p) : T(0);
+                else if (lane == stop) c = p >= 0 ? __ldcg(g.tinc + p) : T(0);
+#pragma unroll
+                for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+                prefix += c;
+                if (incl_mask) done = true;
+                else look -= 32;
+            }
+            if (lane == 0) {
+                g.tinc[tile] = prefix + agg;
+                __threadfence();
+                st_release(g.tflag + tile, 2u);
+                s_prefix = prefix;
+            }
+        }
+        if (tile == 0 && lane == 0) s_prefix = 0;
+    }
+    __syncthreads();
+    const T prefix = s_prefix;
+
+    // 3. blocked exclusive values -> shared -> striped coalesced stores
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int idx = t * IT + k;
+        sm[idx + idx / 32] = prefix + thread_excl + v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int idx = k * kScanThreads + t;
+        const int64_t i = base + idx;
+        if (i < g.n) {
+            const T o = sm[idx + idx / 32];
+            if (g.out32) g.out32[i] = uint32_t(o);
+            else g.out[i] = o;
+        }
+    }
+    if (s_flag && t == 0) {
+        if (g.total_flag) atomicOr(g.total_flag + 1, s_flag);
+        set_status(g.ctrl, ((s_flag & 1u) ? CSPB_DEV_NEGATIVE : 0u) | ((s_flag & 2u) ? CSPB_DEV_EXCEEDS32 : 0u));
+    }
+    if (tile == g.tiles - 1 && t == 0) {
+        const T total = prefix + agg;
+        if (g.out32) {
+            g.out32[g.n] = uint32_t(total);
+            if (g.total_flag) {
+                const bool over = uint64_t(total) > 0xffffffffull;
+                g.total_flag[0] = uint32_t(total);
+                if (over) {
+                    atomicOr(g.total_flag + 1, 2u);
+                    set_status(g.ctrl, CSPB_DEV_EXCEEDS32);
+                }
+            }
+        } else {
+            g.out[g.n] = total;
+        }
+    }
+}
+
+// Offsets mode of build_column: offs[i] = narrowed value (bad: negative, offs[0] != 0), extents from differences.
+__global__ void k_column_offsets(ScanSrc s, int64_t m, uint32_t* offs, uint32_t* ctrl, uint32_t* total_flag) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride) {
+        uint32_t flag = 0, x = 0;
+        switch (s.dtype) {
+            case CSPB_I32: { const int32_t v = static_cast<const int32_t*>(s.in)[i]; if (v < 0) flag |= 1u; else x = uint32_t(v); break; }
+            case CSPB_U32: x = static_cast<const uint32_t*>(s.in)[i]; break;
+            case CSPB_I64: {
+                const int64_t v = static_cast<const int64_t*>(s.in)[i];
+                if (v < 0) flag |= 1u; else if (v > int64_t(0xffffffffll)) flag |= 2u; else x = uint32_t(v);
+                break;
+            }
+            default: { const uint64_t v = static_cast<const uint64_t*>(s.in)[i]; if (v > 0xffffffffull) flag |= 2u; else x = uint32_t(v); break; }
+        }
+        if (i == 0 && x != 0) flag |= 1u;
+        offs[i] = x;
+        if (flag) {
+            atomicOr(total_flag + 1, flag);
+            set_status(ctrl, ((flag & 1u) ? CSPB_DEV_NEGATIVE : 0u) | ((flag & 2u) ? CSPB_DEV_EXCEEDS32 : 0u));
+        }
+    }
+}
+__global__ void k_column_extents(const uint32_t* offs, int64_t n, uint32_t* extents, uint32_t* ctrl, uint32_t* total_flag) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t a = offs[i], b = offs[i + 1];
+        if (b < a) {
+            extents[i] = 0;
+            atomicOr(total_flag + 1, 1u);
+            set_status(ctrl, CSPB_DEV_NEGATIVE);
+        } else {
+            extents[i] = b - a;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) total_flag[0] = offs[n];
+}
+
+__global__ void k_scan_empty32(uint32_t* out) { out[0] = 0; }
+__global__ void k_scan_empty64(uint64_t* out) { out[0] = 0; }
+
+}  // namespace cspb
+
+using namespace cspb;
+using cspb_host::align_up;
+using cspb_host::aligned;
+
+namespace {
+
+template <typename T>
+struct ScanLayout {
+    int64_t tiles = 0;
+    size_t off_flag = 0, off_agg = 0, off_inc = 0, total = 0;
+};
+
+template <typename T>
+ScanLayout<T> scan_layout(int64_t n) {
+    ScanLayout<T> L;
+    const int64_t TILE = int64_t(kScanThreads) * ScanItems<T>::N;
+    L.tiles = n <= 0 ? 0 : (n + TILE - 1) / TILE;
+    size_t o = kCtrlBytes;
+    L.off_flag = o;
+    o = align_up(o + size_t(L.tiles) * 4, 256);
+    L.off_agg = o;
+    o = align_up(o + size_t(L.tiles) * sizeof(T), 256);
+    L.off_inc = o;
+    o = align_up(o + size_t(L.tiles) * sizeof(T), 256);
+    L.total = o;
+    return L;
+}
+
+template <typename T>
+int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, size_t ws_bytes, uint32_t* total_flag,
+             cudaStream_t st) {
+    const ScanLayout<T> L = scan_layout<T>(n);
+    if (!ws || !aligned(ws, 256) || ws_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    char* w = static_cast<char*>(ws);
+    cudaError_t e = cudaMemsetAsync(w, 0, L.off_agg, st);  // ctrl + tile flags
+    if (e != cudaSuccess) return CSPB_ERR_CUDA;
+    ScanK<T> g{};
+    g.src = src;
+    g.out = out;
+    g.out32 = out32;
+    g.n = n;
+    g.tiles = L.tiles;
+    g.ctrl = reinterpret_cast<uint32_t*>(w);
+    g.tflag = reinterpret_cast<uint32_t*>(w + L.off_flag);
+    g.tagg = reinterpret_cast<T*>(w + L.off_agg);
+    g.tinc = reinterpret_cast<T*>(w + L.off_inc);
+    g.total_flag = total_flag;
+    k_scan<T><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cspb_scan_workspace_bytes(int64_t n) {
+    if (n < 0) return 0;
+    const size_t a = scan_layout<uint32_t>(n).total, b = scan_layout<uint64_t>(n).total;
+    return a > b ? a : b;
+}
+
+int cspb_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    if (n < 0 || !out || (n > 0 && !in)) return CSPB_ERR_ARGUMENT;
+    if (n > (int64_t(1) << 40)) return CSPB_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        k_scan_empty32<<<1, 1, 0, st>>>(out);
+        return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+    }
+    ScanSrc s{in, CSPB_U32, 1, false, nullptr};
+    return run_scan<uint32_t>(s, out, nullptr, n, workspace, workspace_bytes, nullptr, st);
+}
+
+int cspb_exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    if (n < 0 || !out || (n > 0 && !in)) return CSPB_ERR_ARGUMENT;
+    if (n > (int64_t(1) << 40)) return CSPB_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        k_scan_empty64<<<1, 1, 0, st>>>(out);
+        return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+    }
+    ScanSrc s{in, CSPB_U64, 1, false, nullptr};
+    return run_scan<uint64_t>(s, out, nullptr, n, workspace, workspace_bytes, nullptr, st);
+}
+
+int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
+                      uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* workspace, size_t workspace_bytes,
+                      void* stream) {
+    if (src_dtype < CSPB_I32 || src_dtype > CSPB_U64) return CSPB_ERR_UNSUPPORTED;
+    if (count < 0 || !offs || !total_flag || (count > 0 && !src)) return CSPB_ERR_ARGUMENT;
+    if (offsets_mode && count == 0) return CSPB_ERR_ARGUMENT;  // N + 1 >= 1 offsets are needed
+    if (!offsets_mode && k < 1) return CSPB_ERR_ARGUMENT;
+    if (count > (int64_t(1) << 40)) return CSPB_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = offsets_mode ? count - 1 : count;
+    if (n > 0 && !extents) return CSPB_ERR_ARGUMENT;
+    if (!workspace || !aligned(workspace, 256) || workspace_bytes < cspb_scan_workspace_bytes(n)) return CSPB_ERR_WORKSPACE;
+    cudaError_t e = cudaMemsetAsync(total_flag, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return CSPB_ERR_CUDA;
+    ScanSrc s{src, src_dtype, offsets_mode ? 1 : k, true, extents};
+    if (!offsets_mode) {
+        if (n == 0) {
+            e = cudaMemsetAsync(workspace, 0, kCtrlBytes, st);
+            if (e != cudaSuccess) return CSPB_ERR_CUDA;
+            k_scan_empty32<<<1, 1, 0, st>>>(offs);
+            return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+        }
+        // the running sum in 64 bits, the offsets stored as u32
+        return run_scan<uint64_t>(s, nullptr, offs, n, workspace, workspace_bytes, total_flag, st);
+    }
+    e = cudaMemsetAsync(workspace, 0, kCtrlBytes, st);
+    if (e != cudaSuccess) return CSPB_ERR_CUDA;
+    uint32_t* ctrl = static_cast<uint32_t*>(workspace);
+    const int64_t blocks = count / 256 + 1 > 1024 ? 1024 : count / 256 + 1;
+    k_column_offsets<<<unsigned(blocks), 256, 0, st>>>(s, count, offs, ctrl, total_flag);
+    k_column_extents<<<unsigned(blocks), 256, 0, st>>>(offs, n, extents, ctrl, total_flag);
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+}  // extern "C"

@@ -1,0 +1,245 @@
+/*
+ * cspb.h — the C ABI of libcspb.so, the B200 (sm_100a) kernels behind CoSpan's fused component chains.
+ *
+ * Every entry point is asynchronous on the given CUDA stream (passed as void*; NULL is the legacy default stream),
+ * takes caller-owned device buffers and a caller-owned workspace, and never allocates. A call returns a host status
+ * (CSPB_OK or a CSPB_ERR_* code) for what can be checked before the launch; what only the device can see (a bounded
+ * wait that gave up, a ragged count that is negative or too large) is written to the status word at the start of the
+ * workspace and read back by cspb_read_status() after the work has run.
+ *
+ * The reference (NAGAGroup/CospanMDAO) has no C ABI: its kernels are SYCL bodies that AdaptiveCpp JIT-compiles and
+ * launches from GroupLauncher::launch (cospanmdao/include/naga/cospan/component.hpp:779-970) through launch_group
+ * (cospanmdao/include/naga/cospan/kernel.hpp:1015-1067). Each entry point below names the reference code whose
+ * results it reproduces; a host runtime calls it where the reference submits the corresponding fused group.
+ *
+ * Thread safety: calls on distinct (stream, workspace) pairs may run concurrently. Two calls that share a workspace
+ * must be ordered on one stream.
+ */
+#ifndef CSPB_H
+#define CSPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------------------------- */
+enum {
+    CSPB_OK = 0,
+    CSPB_ERR_ARGUMENT = 1,    /* a size, pointer, stride or alignment the entry point rejects */
+    CSPB_ERR_WORKSPACE = 2,   /* workspace NULL, misaligned or smaller than cspb_*_workspace_bytes() */
+    CSPB_ERR_LAUNCH = 3,      /* a kernel launch failed (cudaGetLastError after the launch) */
+    CSPB_ERR_TIMEOUT = 4,     /* device status: a bounded device-side wait gave up; outputs are not valid */
+    CSPB_ERR_NEGATIVE = 5,    /* device status: a ragged count is negative, or offsets decrease or do not start at 0 */
+    CSPB_ERR_EXCEEDS32 = 6,   /* device status: a ragged value or total is past 2^32 - 1 */
+    CSPB_ERR_UNSUPPORTED = 7, /* a dtype / option combination this build does not provide */
+    CSPB_ERR_CUDA = 8         /* another CUDA runtime error (cudaMemsetAsync, cudaMemcpyAsync, ...) */
+};
+
+/* bits of the device status word (the first 4 bytes of every workspace) */
+#define CSPB_DEV_TIMEOUT 1u
+#define CSPB_DEV_NEGATIVE 2u
+#define CSPB_DEV_EXCEEDS32 4u
+
+/* storage dtypes of the big operands (the matrix of a GEMVER, the fields of a stencil) */
+enum { CSPB_F32 = 0, CSPB_BF16 = 1 };
+
+/* integer dtypes of a ragged count source (build_column) */
+enum { CSPB_I32 = 0, CSPB_U32 = 1, CSPB_I64 = 2, CSPB_U64 = 3 };
+
+/* A human-readable name of a status code. */
+const char* cspb_status_string(int status);
+
+/* The library's version string and the sm architecture it was built for (e.g. "cspb 0.1 sm_100a"). */
+const char* cspb_version(void);
+
+/* Synchronizes `stream`, reads the device status word of `workspace` and returns the CSPB_ERR_* code it holds
+ * (CSPB_OK when clear). The raw word goes to *raw when raw is not NULL. */
+int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
+
+/* ==================================================================================================================
+ * GEMVER:  Â = A + u1·v1ᵀ + u2·v2ᵀ ;  x = β·Âᵀy + z ;  w = α·Â·x
+ *
+ * Reproduces the gemver stages of examples/gemver-chain: Rank2Update (components.hpp:85-97), GemvTPartial
+ * (components.hpp:142-167), ColReduce<true> (components.hpp:192-219) and Gemv (components.hpp:237-265), as wired by
+ * the Gemver System (systems.hpp:71-133), in ONE persistent launch. The host double-precision reference is
+ * gemver_chain::reference_chain's gemver lambda (common/chain_data.hpp:104-117).
+ *
+ * A is row-major n×n with row stride lda elements, stored as f32 or bf16 (a_dtype). Â is computed in f32 as
+ * (a + u1[i]·v1[j]) + u2[i]·v2[j] with each operation rounded separately (no fused multiply-add), and written to B
+ * (row stride ldb) when B is not NULL. Âᵀy is accumulated in f64 and combined in a fixed order; Â·x in f32 with a
+ * fixed reduction tree: results do not depend on the launch shape or on other work on the GPU. z may be NULL (zero).
+ * ================================================================================================================== */
+typedef struct cspb_gemver_desc {
+    int64_t n;         /* rows = columns, >= 1 */
+    int64_t lda;       /* row stride of A in elements, >= n */
+    int64_t ldb;       /* row stride of B in elements, >= n (ignored when B is NULL) */
+    int32_t a_dtype;   /* CSPB_F32 or CSPB_BF16 */
+    int32_t flags;     /* reserved, 0 */
+    const void* A;
+    const float* u1;
+    const float* v1;
+    const float* u2;
+    const float* v2;
+    const float* y;
+    const float* z;    /* may be NULL */
+    float alpha;
+    float beta;
+    float* B;          /* may be NULL: Â is not materialized */
+    float* x;          /* n */
+    float* w;          /* n */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_gemver_desc;
+
+size_t cspb_gemver_workspace_bytes(int64_t n);
+int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream);
+
+/* ==================================================================================================================
+ * BiCGK:  q = B·p ;  s = Bᵀ·r   (one pass over B)
+ *
+ * Reproduces Bicgk (examples/gemver-chain/systems.hpp:138-212): BicgkOnePass + RowReduce + ColReduce<false>
+ * (components.hpp:277-358), and the q / s loops of reference_chain (common/chain_data.hpp:122-134). Bᵀr is
+ * accumulated in f64, B·p in f32 with a fixed tree.
+ * ================================================================================================================== */
+typedef struct cspb_bicgk_desc {
+    int64_t n;
+    int64_t ldb;
+    int32_t b_dtype;   /* CSPB_F32 or CSPB_BF16 */
+    int32_t flags;     /* reserved, 0 */
+    const void* B;
+    const float* p;
+    const float* r;
+    float* q;
+    float* s;
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_bicgk_desc;
+
+size_t cspb_bicgk_workspace_bytes(int64_t n);
+int cspb_bicgk_fused(const cspb_bicgk_desc* d, void* stream);
+
+/* ==================================================================================================================
+ * The gemver chain G1 → BiCGK → G2 in one persistent launch (examples/gemver-chain, Chain System systems.hpp:214-266;
+ * host reference reference_chain common/chain_data.hpp:93-144):
+ *   G1:    B1 = A0 + u1a·v1aᵀ + u2a·v2aᵀ,  x1 = β·B1ᵀ·ya + za,  w1 = α·B1·x1
+ *   BiCGK: q = B1·x1,  s = B1ᵀ·w1
+ *   G2:    B2 = B1 + u1b·v1bᵀ + u2b·v2bᵀ,  x2 = β·B2ᵀ·q + s,   w2 = α·B2·x2
+ * Six passes over n² elements (the reference's nominal traffic counts eight). B1 and B2 may not be NULL.
+ * ================================================================================================================== */
+typedef struct cspb_chain_desc {
+    int64_t n;
+    const float* A0;                               /* n×n, row stride n */
+    const float *u1a, *v1a, *u2a, *v2a, *ya, *za;  /* G1's vectors */
+    const float *u1b, *v1b, *u2b, *v2b;            /* G2's rank-2 update */
+    float alpha;                                   /* both GEMVERs (the reference ties one scale: 1/sqrt(n)) */
+    float beta;
+    float *B1, *x1, *w1, *q, *s, *B2, *x2, *w2;
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_chain_desc;
+
+size_t cspb_chain_workspace_bytes(int64_t n);
+int cspb_gemver_chain(const cspb_chain_desc* d, void* stream);
+
+/* ==================================================================================================================
+ * NS residual, compressible (the reference's examples/ns-residual): one evaluation of R = -div F_conv + div F_visc
+ * per cell plus the diagnostics, in ONE kernel whose face fluxes stay on chip.
+ *
+ * Reproduces NsFused (examples/ns-residual/systems.hpp:88-140) and hw_forward (handwritten.hpp:51-191): physics.hpp
+ * (to_prim, grad_cell, hllc, visc_flux, cell_diag, MinMod / VanLeer), tile.hpp:39-229 (tile stages, face ownership),
+ * components.hpp:393-628 (atomic diagnostics, deterministic reductions, error stage). The host double-precision
+ * reference is reference_residual (reference.hpp:30-130).
+ *
+ * U and R are (4, ny, nx) f32, row-major. diag (device, 18 floats) receives, in this order:
+ *   [0] Dt  [1] Ws  [2..5] Sq0..3           the atomic diagnostics (float atomics; Sq is order dependent)
+ *   [6..9] detn.Det  [10] detd.Det  [11] detw.Det   the deterministic ones (f64 sums in a fixed order, rounded)
+ *   [12..17] err.Err = atomic - deterministic: [dt, ws, sq0..sq3]
+ * det_sq64 (device, 4 doubles, may be NULL) receives the f64 sums of R² before rounding.
+ * ================================================================================================================== */
+typedef struct cspb_ns_comp_desc {
+    int32_t nx, ny;      /* >= 4 each */
+    int32_t limiter;     /* 0 minmod, 1 van Leer */
+    int32_t walls;       /* 1: no-slip adiabatic walls in y; 0: periodic in y. x is always periodic. */
+    const float* U;
+    float* R;
+    float* diag;         /* 18 floats */
+    double* det_sq64;    /* 4 doubles, may be NULL */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_ns_comp_desc;
+
+size_t cspb_ns_comp_workspace_bytes(int32_t nx, int32_t ny);
+int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream);
+
+/* The reference's initial field (examples/ns-residual/physics.hpp:203-215, make_init main.cpp:100-112) on the
+ * device: U(v, j, i) for amplitude amp. */
+int cspb_ns_init_cons(float* U, int32_t nx, int32_t ny, float amp, void* stream);
+
+/* ==================================================================================================================
+ * NS residual, incompressible, 2D periodic collocated grid (no reference code computes it; the formula is
+ *   r_u = u·∂u/∂x + v·∂u/∂y + ∂p/∂x − ν∇²u,   r_v = u·∂v/∂x + v·∂v/∂y + ∂p/∂y − ν∇²v,   r_c = ∂u/∂x + ∂v/∂y
+ * with 2nd-order central differences on spacing h). u, v, p are (ny, nx) in f32 or bf16 storage; r_u, r_v, r_c are
+ * f32. norms (device, 3 doubles, may be NULL) receives ||r_u||₂, ||r_v||₂, ||r_c||₂ from f64 sums in a fixed order.
+ * ================================================================================================================== */
+typedef struct cspb_ns_incomp_desc {
+    int32_t nx, ny;      /* >= 3 each */
+    int32_t dtype;       /* storage of u, v, p: CSPB_F32 or CSPB_BF16 */
+    int32_t flags;       /* reserved, 0 */
+    double h;
+    double nu;
+    const void* u;
+    const void* v;
+    const void* p;
+    float* ru;
+    float* rv;
+    float* rc;
+    double* norms;       /* 3 doubles, may be NULL */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_ns_incomp_desc;
+
+size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny);
+int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream);
+
+/* ==================================================================================================================
+ * Device scan: out[0..n] = the exclusive scan of in[0..n), out[n] = the total, in ONE single-pass launch
+ * (decoupled lookback). The u32 variant wraps mod 2^32 like cs::detail::exclusive_scan_u32
+ * (cospanmdao/include/naga/cospan/device_scan.hpp:46-110), which it replaces bit for bit; the u64 variant wraps
+ * mod 2^64. in and out must not overlap. n == 0 writes out[0] = 0.
+ * ================================================================================================================== */
+size_t cspb_scan_workspace_bytes(int64_t n);
+int cspb_exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, void* workspace, size_t workspace_bytes,
+                            void* stream);
+int cspb_exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* ==================================================================================================================
+ * A ragged column from an integer variable (cs::detail::build_column, cospanmdao/include/naga/cospan/
+ * shape_hook.hpp:215-348): counts mode (offsets_mode = 0) reads count values src[i * k] (column 0 of a rank-2 [N, k]
+ * source, k = 1 for rank 1), writes extents[i] = max(value, 0) narrowed to u32 and offs = their exclusive scan
+ * (count + 1 entries); offsets mode (offsets_mode = 1) reads count = N + 1 offsets, writes offs = the values and
+ * extents[i] = offs[i+1] - offs[i]. The flag bits follow the reference: 1 = a negative value, offs[0] != 0 or a
+ * decrease; 2 = a value or a total past 2^32 - 1. total_flag (device or mapped host memory, 2 words) receives
+ * [offs[N], flag]. Single pass: narrow + scan + wrap check in one launch.
+ * ================================================================================================================== */
+int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
+                      uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* ==================================================================================================================
+ * Seeded inputs on the device: the reference's generator gemver_chain::hash_unit (common/chain_data.hpp:34-49).
+ * dist 0: hash_unit(seed, i) in [-1, 1); dist 1: (hash_unit(seed, i) + 1) / 2 in [0, 1), exactly (h >> 8) · 2^-24.
+ * out_dtype CSPB_F32 or CSPB_BF16 (round to nearest even). Element i of the output is at out + i (index_base added to
+ * i for the hash).
+ * ================================================================================================================== */
+int cspb_fill_hash(void* out, int32_t out_dtype, int64_t count, uint64_t index_base, uint32_t seed, int32_t dist,
+                   void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSPB_H */

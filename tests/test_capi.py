@@ -1,0 +1,95 @@
+"""The C ABI without a GPU: the library loads, exports every function include/cspb.h declares, sizes workspaces
+sanely, and rejects bad arguments before touching CUDA."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+import cospanmdao_b200 as cb
+from cospanmdao_b200 import _capi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "cspb.h"
+
+
+def declared():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cspb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = cb.lib()
+    names = declared()
+    assert len(names) >= 19
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python view knows every one of them
+    assert set(names) <= set(_capi.PROTOTYPES), set(names) - set(_capi.PROTOTYPES)
+
+
+def test_version_and_status_strings():
+    assert "sm_100a" in cb.version()
+    lib = cb.lib()
+    for code in range(9):
+        assert lib.cspb_status_string(code)
+    assert lib.cspb_status_string(99) == b"unknown status"
+
+
+def test_workspace_sizes():
+    lib = cb.lib()
+    for f in (lib.cspb_gemver_workspace_bytes, lib.cspb_bicgk_workspace_bytes, lib.cspb_chain_workspace_bytes):
+        assert f(0) == 0
+        prev = 0
+        for n in (1, 7, 256, 1000, 4096, 16384):
+            b = f(n)
+            assert b % 256 == 0 and b >= prev
+            prev = b
+    # GEMVER at n = 16384: the f64 column partials (n/128 strips) dominate, well under 1% of the matrix
+    assert lib.cspb_gemver_workspace_bytes(16384) < 24 * 2 ** 20
+    assert lib.cspb_scan_workspace_bytes(0) >= 256
+    assert lib.cspb_ns_incomp_workspace_bytes(2, 2) == 0
+    assert lib.cspb_ns_incomp_workspace_bytes(4096, 4096) > 256
+
+
+def test_arguments_are_rejected_before_cuda():
+    lib = cb.lib()
+    assert lib.cspb_gemver_fused(None, None) == _capi.ERR_ARGUMENT
+    d = _capi.GemverDesc()
+    d.n = 0
+    assert lib.cspb_gemver_fused(C.byref(d), None) == _capi.ERR_ARGUMENT
+    d.n, d.lda, d.ldb = 8, 8, 8
+    fake = 0x1000
+    for f in ("A", "u1", "v1", "u2", "v2", "y", "x", "w"):
+        setattr(d, f, fake)
+    d.a_dtype = 7
+    assert lib.cspb_gemver_fused(C.byref(d), None) == _capi.ERR_UNSUPPORTED
+    d.a_dtype = _capi.F32
+    d.lda = 4
+    assert lib.cspb_gemver_fused(C.byref(d), None) == _capi.ERR_ARGUMENT
+    d.lda = 8
+    d.workspace, d.workspace_bytes = 0x100, 16
+    assert lib.cspb_gemver_fused(C.byref(d), None) == _capi.ERR_WORKSPACE
+    d.workspace = 0x101  # misaligned
+    d.workspace_bytes = 1 << 30
+    assert lib.cspb_gemver_fused(C.byref(d), None) == _capi.ERR_WORKSPACE
+    assert lib.cspb_bicgk_fused(None, None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_gemver_chain(None, None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_exclusive_scan_u32(None, None, -1, None, 0, None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_exclusive_scan_u64(fake, None, 4, None, 0, None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_build_column(fake, 9, 4, 1, 0, fake, fake, fake, None, 0, None) == _capi.ERR_UNSUPPORTED
+    assert lib.cspb_build_column(fake, 0, 0, 1, 1, fake, fake, fake, None, 0, None) == _capi.ERR_ARGUMENT
+    nd = _capi.NsIncompDesc()
+    nd.nx, nd.ny = 2, 8
+    assert lib.cspb_ns_incompressible(C.byref(nd), None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_fill_hash(fake, 0, 10, 0, 1, 5, None) == _capi.ERR_ARGUMENT
+
+
+def test_python_view_raises_value_errors_like_the_reference():
+    # port checks happen before any device work
+    with pytest.raises(ValueError):
+        cb.gemver(None, None, None, None, None, None, alpha=1.0, beta=1.0)
+    with pytest.raises(ValueError, match="limiter"):
+        cb.ns_compressible(None, limiter="superbee")
+    with pytest.raises(ValueError, match="bc"):
+        cb.ns_compressible(None, bc="open")

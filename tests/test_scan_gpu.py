@@ -1,0 +1,93 @@
+"""The single-pass device scan and the ragged column against tests/test_device_scan.cpp's cases (bit-exact)."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _u32(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+def test_scan_known_answers(cuda, golden):
+    import torch
+    import cospanmdao_b200 as cb
+    g = golden("scan_known.npz")
+    for k in g:
+        if not k.startswith("in_"):
+            continue
+        v = g[k]
+        t = torch.from_numpy(v.view(np.int32)).to(cuda)
+        out = cb.exclusive_scan(t)
+        assert np.array_equal(_u32(out), g["out_" + k[3:]]), k
+
+
+@pytest.mark.parametrize("n", [4095, 4096, 4097, 1 << 20, (1 << 24) + 5])
+def test_scan_u32_large_wrapping(cuda, n):
+    import torch
+    import cospanmdao_b200 as cb
+    rng = np.random.default_rng(n)
+    v = rng.integers(0, 2 ** 32, size=n, dtype=np.uint64).astype(np.uint32)
+    out = cb.exclusive_scan(torch.from_numpy(v.view(np.int32)).to(cuda))
+    assert np.array_equal(_u32(out), oracle.exclusive_scan(v))
+
+
+@pytest.mark.parametrize("n", [0, 1, 2047, 2048, 2049, 300001])
+def test_scan_u64(cuda, n):
+    import torch
+    import cospanmdao_b200 as cb
+    rng = np.random.default_rng(7 + n)
+    v = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64) * np.uint64(3)  # wraps mod 2^64
+    out = cb.exclusive_scan(torch.from_numpy(v.view(np.int64)).to(cuda))
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), oracle.exclusive_scan(v))
+
+
+def test_scan_repeat_is_identical(cuda):
+    import torch
+    import cospanmdao_b200 as cb
+    v = torch.randint(0, 1000, (3_000_000,), dtype=torch.int32, device=cuda)
+    a = cb.exclusive_scan(v)
+    b = cb.exclusive_scan(v)
+    assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("dtype", ["int32", "uint32", "int64", "uint64"])
+def test_build_column_counts(cuda, dtype):
+    import torch
+    import cospanmdao_b200 as cb
+    rng = np.random.default_rng(3)
+    src = rng.integers(0, 5000, size=10007).astype(dtype)
+    t = torch.from_numpy(src).to(cuda)
+    ext, offs, total, flag = cb.build_column(t)
+    e2, o2, tot2, f2 = oracle.build_column(src)
+    assert np.array_equal(_u32(ext), e2) and np.array_equal(_u32(offs), o2) and total == tot2 and flag == 0
+
+
+def test_build_column_rank2_and_offsets_mode(cuda):
+    import torch
+    import cospanmdao_b200 as cb
+    src = np.array([[4, 9], [1, 9], [2, 9], [0, 1]], dtype=np.int32)
+    ext, offs, total, _ = cb.build_column(torch.from_numpy(src).to(cuda))
+    assert _u32(ext).tolist() == [4, 1, 2, 0] and _u32(offs).tolist() == [0, 4, 5, 7, 7] and total == 7
+    o = np.array([0, 2, 2, 7, 11], dtype=np.int64)
+    ext, offs, total, _ = cb.build_column(torch.from_numpy(o).to(cuda), offsets_mode=True)
+    assert _u32(ext).tolist() == [2, 0, 5, 4] and total == 11
+    ext, offs, total, _ = cb.build_column(torch.zeros(0, dtype=torch.int32, device=cuda))
+    assert _u32(offs).tolist() == [0] and total == 0
+
+
+def test_build_column_flags_raise_like_the_reference(cuda):
+    import torch
+    import cospanmdao_b200 as cb
+    with pytest.raises(ValueError, match="negative"):
+        cb.build_column(torch.tensor([3, -1, 5], dtype=torch.int64, device=cuda))
+    with pytest.raises(ValueError, match="2\\^32"):
+        cb.build_column(torch.tensor([2 ** 33], dtype=torch.int64, device=cuda))
+    with pytest.raises(ValueError, match="2\\^32"):
+        cb.build_column(torch.tensor([2 ** 31, 2 ** 31, 1], dtype=torch.int64, device=cuda))
+    with pytest.raises(ValueError, match="negative"):
+        cb.build_column(torch.tensor([1, 2], dtype=torch.int32, device=cuda), offsets_mode=True)
+    with pytest.raises(ValueError, match="negative"):
+        cb.build_column(torch.tensor([0, 5, 3], dtype=torch.int32, device=cuda), offsets_mode=True)
