@@ -205,7 +205,7 @@ def bench_gemver(torch, cb, dist, args, peak):
 
     def step():
         cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=alpha, beta=beta, B=B, x=x, w=w,
-                  workspace=ws)
+                  schedule=args.schedule, workspace=ws)
 
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
@@ -237,6 +237,8 @@ def bench_gemver(torch, cb, dist, args, peak):
         hx.copy_(x, non_blocking=True)
         hw.copy_(w, non_blocking=True)
 
+    if args.no_e2e:
+        return {"ms": ms, "gbs": gbs, "bytes": nbytes, "err": err, "clocks": clk, "e2e": None}
     ke = max(3, min(args.steps, 10))
     ms_e2e = timed(torch, dist, e2e_step, ke, 2)
     h2d = n * n * 4 + 6 * n * 4
@@ -414,6 +416,8 @@ def main(argv=None) -> int:
     ap.add_argument("--grid", type=int, default=4096)
     ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed steps before the timed region")
     ap.add_argument("--quick", action="store_true", help="headline only (no secondary workloads, no CPU baseline)")
+    ap.add_argument("--schedule", default="panel", choices=["panel", "barrier"], help="GEMVER schedule")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     dist = Dist()
@@ -457,7 +461,8 @@ def main(argv=None) -> int:
         "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": kernel_gbs / pk["hbm_gbs"], "peak_source": pk["source"],
                      "traffic": traffic, "algorithmic_bytes_per_launch": g["bytes"],
-                     "kernel": "cspb::k_gemver<float, true>"},
+                     "kernel": "cspb::k_gemver_panel<float, true>" if args.schedule == "panel"
+                     else "cspb::k_gemver<float, true>"},
         "e2e": g["e2e"],
         "gpu_launches": args.steps,
         "clocks": g["clocks"],

@@ -142,9 +142,12 @@ def _mat_dtype(t):
 
 # ---- GEMVER family ------------------------------------------------------------------------------------------------
 def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: bool = True, B=None, x=None, w=None,
-           workspace: Workspace | None = None, stream=None):
+           schedule: str = "panel", workspace: Workspace | None = None, stream=None):
     """Â = A + u1·v1ᵀ + u2·v2ᵀ, x = β·Âᵀy + z, w = α·Â·x in one launch. A: (n, n) float32 or bfloat16 (a row
-    stride from A.stride(0) is honoured). Returns (B or None, x, w)."""
+    stride from A.stride(0) is honoured). schedule 'panel' (column panels pipelined through L2, the default) or
+    'barrier' (three streaming passes); both give the same bits. Returns (B or None, x, w)."""
+    if schedule not in ("panel", "barrier"):
+        raise ValueError("schedule must be 'panel' or 'barrier'")
     torch = _torch()
     if A is None or A.dim() != 2 or A.shape[0] != A.shape[1]:
         raise ValueError("'A' must be a square matrix")
@@ -168,7 +171,8 @@ def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: b
     ws = workspace or default_workspace(dev, stream)
     need = lib().cspb_gemver_workspace_bytes(n)
     wp, wb = ws.ptr(need)
-    d = _capi.GemverDesc(n, A.stride(0), B.stride(0) if B is not None else n, _mat_dtype(A), 0, _ptr(A), _ptr(u1),
+    flags = _capi.GEMVER_BARRIER if schedule == "barrier" else 0
+    d = _capi.GemverDesc(n, A.stride(0), B.stride(0) if B is not None else n, _mat_dtype(A), flags, _ptr(A), _ptr(u1),
                          _ptr(v1), _ptr(u2), _ptr(v2), _ptr(y), _ptr(z), float(alpha), float(beta), _ptr(B), _ptr(x),
                          _ptr(w), wp, wb)
     _raise(lib().cspb_gemver_fused(C.byref(d), C.c_void_p(_stream(stream))), "gemver")

@@ -22,13 +22,16 @@ ERR_NEGATIVE = 5
 ERR_EXCEEDS32 = 6
 ERR_UNSUPPORTED = 7
 ERR_CUDA = 8
+ERR_CAPACITY = 9
 
 DEV_TIMEOUT = 1
 DEV_NEGATIVE = 2
 DEV_EXCEEDS32 = 4
+DEV_CAPACITY = 8
 
 F32 = 0
 BF16 = 1
+GEMVER_BARRIER = 1
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p
@@ -88,6 +91,9 @@ PROTOTYPES = {
     "cspb_bicgk_fused": (C.c_int, [C.POINTER(BicgkDesc), vp]),
     "cspb_chain_workspace_bytes": (sz, [i64]),
     "cspb_gemver_chain": (C.c_int, [C.POINTER(ChainDesc), vp]),
+    "cspb_gemver_batched_workspace_bytes": (sz, [i64, i64, i64]),
+    "cspb_gemver_batched": (C.c_int, [C.POINTER(BatchedDesc), vp]),
+    "cspb_gemver_batched_tunings": (C.c_int, []),
     "cspb_ns_comp_workspace_bytes": (sz, [i32, i32]),
     "cspb_ns_compressible": (C.c_int, [C.POINTER(NsCompDesc), vp]),
     "cspb_ns_init_cons": (C.c_int, [vp, i32, i32, C.c_float, vp]),

@@ -74,6 +74,7 @@ const char* cspb_status_string(int status) {
         case CSPB_ERR_EXCEEDS32: return "a ragged value or total is past 2^32 - 1";
         case CSPB_ERR_UNSUPPORTED: return "unsupported dtype or option";
         case CSPB_ERR_CUDA: return "CUDA runtime error";
+        case CSPB_ERR_CAPACITY: return "device-computed totals exceed the declared capacities";
         default: return "unknown status";
     }
 }
@@ -91,6 +92,7 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream) {
     if (word & CSPB_DEV_TIMEOUT) return CSPB_ERR_TIMEOUT;
     if (word & CSPB_DEV_NEGATIVE) return CSPB_ERR_NEGATIVE;
     if (word & CSPB_DEV_EXCEEDS32) return CSPB_ERR_EXCEEDS32;
+    if (word & CSPB_DEV_CAPACITY) return CSPB_ERR_CAPACITY;
     return CSPB_OK;
 }
 

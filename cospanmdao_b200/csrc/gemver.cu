@@ -1,10 +1,18 @@
 // gemver.cu — GEMVER, BiCGK and the gemver chain as persistent cooperative kernels built from rowpass.cuh.
 //
-// GEMVER (one launch, 3 passes over n² elements — the minimum, since w needs all of x):
-//   pass 1   read A, write Â, f64 column partials of Â·y      (Rank2Update + GemvTPartial, fused)
-//   barrier, x = z + β·Σ partials (fixed order), barrier       (ColReduce<true>)
-//   pass 2   read Â (or A again, re-applying the update), row dots with x, last chunk of a strip writes w = α·dot
-//            (Gemv); walked from the last strip back, so the Â rows still in L2 are read first.
+// GEMVER, panel-pipelined (the default; one launch, no grid barrier):
+//   A column panel (CW columns × all n rows) is the unit of dependency: the row-dot partials of panel c need only
+//   x over panel c, which needs only panel c's column sums. The work list runs pass 1 over panel c (read A, write Â,
+//   f64 column partials of Â·y: Rank2Update + GemvTPartial fused), the block finishing the panel's last strip forms
+//   x over the panel (ColReduce<true>, fixed order) and raises the panel's flag, and pass 2 over panel c (row dots
+//   with x: Gemv) is scheduled one panel later, while the panel's Â (n·CW·4 bytes, 16 MB at n = 16384) is still in
+//   L2. HBM traffic is then A once and Â once (8n² bytes in f32) instead of the 12n² of three streaming passes; the
+//   last block to finish a strip's row partials writes w = α·dot. A pass-2 block waits (bounded) only on pass-1 work
+//   already taken by running blocks, which never waits itself: no co-residency is assumed.
+// GEMVER, three streaming passes (flag CSPB_GEMVER_BARRIER; cooperative launch):
+//   pass 1   read A, write Â, f64 column partials        | grid barrier, x = z + β·Σ partials, grid barrier
+//   pass 2   read Â (or A again), row dots with x, w;  walked from the last strip back (recently written Â in L2).
+// Both schedules produce bit-identical results (the same partials, combined in the same order).
 // BiCGK (one pass): q = B·p row dots and s = Bᵀ·r column partials from the same loads; one barrier; s.
 // Chain (G1 → BiCGK → G2, six passes — the reference's nominal traffic counts eight):
 //   1: A0 → B1 + x1 partials | 2: B1 → w1 = α·(B1·x1), q = B1·x1 (p = x1, so one dot gives both)
@@ -45,6 +53,72 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
             pass_unit<float, kWX, false, false, false, false, true>(g.p2, unit, vec_ok != 0, smem);
         else
             pass_unit<T, kWX, true, true, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+    }
+}
+
+struct PanelK {
+    PassArgs p1, p2;
+    uint32_t* ctrl;
+    uint32_t* chunk_done;  // [chunks]
+    uint32_t* x_ready;     // [chunks]
+    const float* z;
+    float beta;
+    float* x;
+    int64_t lag;           // pass 2 over panel c follows pass 1 over panel c + lag
+};
+
+// Block b of the work list (each block = one panel's strips) -> (pass, panel).
+__device__ __forceinline__ void panel_block(int64_t b, int64_t C, int64_t L, int& pass, int64_t& c) {
+    if (b < L) { pass = 1; c = b; return; }
+    const int64_t r = b - L;
+    if (r < 2 * (C - L)) {
+        const int64_t t = L + r / 2;
+        if ((r & 1) == 0) { pass = 1; c = t; }
+        else { pass = 2; c = t - L; }
+        return;
+    }
+    pass = 2;
+    c = C - L + (r - 2 * (C - L));
+}
+
+template <typename T, bool P2_FROM_B>
+__global__ void __launch_bounds__(kPassThreads, 2) k_gemver_panel(PanelK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    __shared__ int s_flag;
+    const int64_t S = g.p1.strips, C = g.p1.chunks, L = g.lag;
+    const int64_t items = 2 * S * C;
+    constexpr int CW = PassGeo<T, kWX>::CW;
+    for (;;) {
+        const uint32_t item = grab_work(g.ctrl, kWork0);
+        if (int64_t(item) >= items) break;
+        int pass;
+        int64_t c;
+        panel_block(int64_t(item) / S, C, L, pass, c);
+        const int64_t si = int64_t(item) % S;
+        if (pass == 1) {
+            pass_unit<T, kWX, true, true, false, true, false>(g.p1, si * C + c, vec_ok != 0, smem);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) s_flag = atomicAdd(g.chunk_done + c, 1u) == uint32_t(S - 1);
+            __syncthreads();
+            if (s_flag) {  // the panel's last strip: x over the panel
+                __threadfence();
+                const int64_t c0 = c * CW, c1 = min(g.p1.n, c0 + CW);
+                colsum_finish_cols(g.p1.PB, S, g.p1.n, c0, c1, g.z, g.beta, g.x);
+                __threadfence();
+                __syncthreads();
+                if (threadIdx.x == 0) st_release(g.x_ready + c, 1u);
+            }
+        } else {
+            if (threadIdx.x == 0) s_flag = ld_acquire(g.x_ready + c) != 0u || wait_change(g.x_ready + c, 0u, g.ctrl);
+            __syncthreads();
+            if (!s_flag) break;
+            const int64_t unit = (S - 1 - si) * C + c;  // the panel's strips from the last one back
+            if constexpr (P2_FROM_B)
+                pass_unit<float, kWX, false, false, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+            else
+                pass_unit<T, kWX, true, true, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+        }
     }
 }
 
@@ -126,10 +200,12 @@ namespace {
 
 struct PassLayout {
     int64_t strips = 0, chunks = 0, units = 0;
-    size_t off_done = 0, off_PA = 0, off_PB = 0, off_Wp = 0, total = 0;
+    size_t off_done = 0, off_chunk = 0, off_PA = 0, off_PB = 0, off_Wp = 0, total = 0;
 };
 
-// Workspace: [ctrl 256][strip_done: strips u32 × nsets][PA: strips×n f64][PB: strips×n f64][Wp: chunks×n f32]
+// Workspace: [ctrl 256][strip_done: strips u32 × nsets][chunk_done, x_ready: chunks u32 each]
+//            [PA: strips×n f64][PB: strips×n f64][Wp: chunks×n f32]
+// Everything before PA is zeroed per call.
 PassLayout pass_layout(int64_t n, int S, int CW, int done_sets, bool want_PA) {
     PassLayout L;
     L.strips = (n + S - 1) / S;
@@ -137,7 +213,9 @@ PassLayout pass_layout(int64_t n, int S, int CW, int done_sets, bool want_PA) {
     L.units = L.strips * L.chunks;
     size_t o = kCtrlBytes;
     L.off_done = o;
-    o = align_up(o + size_t(L.strips) * sizeof(uint32_t) * size_t(done_sets), 256);
+    o = o + size_t(L.strips) * sizeof(uint32_t) * size_t(done_sets);
+    L.off_chunk = o;
+    o = align_up(o + 2 * size_t(L.chunks) * sizeof(uint32_t), 256);
     L.off_PA = o;
     if (want_PA) o = align_up(o + size_t(L.strips) * size_t(n) * sizeof(double), 256);
     L.off_PB = o;
@@ -171,6 +249,22 @@ int launch_coop(K kernel, void** args, int64_t units, size_t zero_bytes, void* w
     return CSPB_OK;
 }
 
+template <typename K>
+int launch_persistent(K kernel, void** args, int64_t items, size_t zero_bytes, void* ws, cudaStream_t st) {
+    const cspb_host::DeviceInfo di = cspb_host::device_info();
+    if (di.device < 0) return CSPB_ERR_CUDA;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPassThreads, 0);
+    if (e != cudaSuccess || per_sm < 1) return e != cudaSuccess ? cspb_host::map_cuda_error(e) : CSPB_ERR_LAUNCH;
+    int64_t grid = int64_t(per_sm) * di.sms;
+    if (grid > items) grid = items;
+    if (grid < 1) grid = 1;
+    e = cudaMemsetAsync(ws, 0, zero_bytes, st);
+    if (e != cudaSuccess) return cspb_host::map_cuda_error(e);
+    e = cudaLaunchKernel(reinterpret_cast<const void*>(kernel), dim3(unsigned(grid)), dim3(kPassThreads), args, 0, st);
+    return e == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
 bool vec_aligned(const void* p, int64_t ld, int elem_bytes) {
     return p == nullptr || (aligned(p, 16) && (ld * elem_bytes) % 16 == 0);
 }
@@ -191,19 +285,14 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
     if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    if ((d->flags & ~CSPB_GEMVER_BARRIER) != 0) return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->a_dtype == CSPB_BF16;
     const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    if (2 * L.units >= int64_t(0xffffffffll)) return CSPB_ERR_ARGUMENT;
     char* ws = static_cast<char*>(d->workspace);
 
-    GemverK g{};
-    g.ctrl = reinterpret_cast<uint32_t*>(ws);
-    g.units = L.units;
-    g.z = d->z;
-    g.beta = d->beta;
-    g.x = d->x;
-    PassArgs& p1 = g.p1;
+    PassArgs p1{};
     p1.n = n;
     p1.src = d->A;
     p1.lds = d->lda;
@@ -214,8 +303,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     p1.PB = reinterpret_cast<double*>(ws + L.off_PB);
     p1.strips = L.strips;
     p1.chunks = L.chunks;
-    PassArgs& p2 = g.p2;
-    p2 = p1;
+    PassArgs p2 = p1;
     p2.dst = nullptr;
     p2.cyB = nullptr;
     p2.PB = nullptr;
@@ -231,12 +319,38 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     }
     const int eb = bf16 ? 2 : 4;
     const int vec_ok = vec_aligned(d->A, d->lda, eb) && vec_aligned(d->B, d->ldb, 4) ? 1 : 0;
-    void* args[] = {&g, const_cast<int*>(&vec_ok)};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t zero = L.off_PA;  // ctrl + strip_done
-    if (bf16) return launch_coop(k_gemver<__nv_bfloat16, false>, args, L.units, zero, ws, st);
-    if (from_B) return launch_coop(k_gemver<float, true>, args, L.units, zero, ws, st);
-    return launch_coop(k_gemver<float, false>, args, L.units, zero, ws, st);
+    const size_t zero = L.off_PA;  // ctrl, strip_done, chunk_done, x_ready
+
+    if (d->flags & CSPB_GEMVER_BARRIER) {
+        GemverK g{};
+        g.p1 = p1;
+        g.p2 = p2;
+        g.ctrl = reinterpret_cast<uint32_t*>(ws);
+        g.units = L.units;
+        g.z = d->z;
+        g.beta = d->beta;
+        g.x = d->x;
+        void* args[] = {&g, const_cast<int*>(&vec_ok)};
+        if (bf16) return launch_coop(k_gemver<__nv_bfloat16, false>, args, L.units, zero, ws, st);
+        if (from_B) return launch_coop(k_gemver<float, true>, args, L.units, zero, ws, st);
+        return launch_coop(k_gemver<float, false>, args, L.units, zero, ws, st);
+    }
+    PanelK g{};
+    g.p1 = p1;
+    g.p2 = p2;
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    g.chunk_done = reinterpret_cast<uint32_t*>(ws + L.off_chunk);
+    g.x_ready = g.chunk_done + L.chunks;
+    g.z = d->z;
+    g.beta = d->beta;
+    g.x = d->x;
+    g.lag = L.chunks < 1 ? 0 : (L.chunks < 2 ? L.chunks : 1);
+    void* args[] = {&g, const_cast<int*>(&vec_ok)};
+    const int64_t items = 2 * L.units;
+    if (bf16) return launch_persistent(k_gemver_panel<__nv_bfloat16, false>, args, items, zero, ws, st);
+    if (from_B) return launch_persistent(k_gemver_panel<float, true>, args, items, zero, ws, st);
+    return launch_persistent(k_gemver_panel<float, false>, args, items, zero, ws, st);
 }
 
 size_t cspb_bicgk_workspace_bytes(int64_t n) {

@@ -304,4 +304,27 @@ __device__ __forceinline__ void colsum_finish(const double* P, int64_t strips, i
     }
 }
 
+// The same sums for the columns [c0, c1) only, by the threads of ONE block (the identical order, so a result formed
+// here is bit-identical to one formed by colsum_finish).
+__device__ __forceinline__ void colsum_finish_cols(const double* P, int64_t strips, int64_t n, int64_t c0, int64_t c1,
+                                                   const float* z, float scale, float* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t items = 4 * (c1 - c0);
+    for (int64_t base = int64_t(threadIdx.x) - lane; base < items; base += blockDim.x) {
+        const int64_t item = base + lane;
+        const bool valid = item < items;
+        const int64_t j = c0 + (item >> 2);
+        const int q = int(item & 3);
+        double s = 0.0;
+        if (valid)
+            for (int64_t st = q; st < strips; st += 4) s += __ldcg(P + st * n + j);
+        s += __shfl_xor_sync(kFull, s, 1);
+        s += __shfl_xor_sync(kFull, s, 2);
+        if (valid && q == 0) {
+            const double zz = z ? double(__ldcg(z + j)) : 0.0;
+            out[j] = float(zz + double(scale) * s);
+        }
+    }
+}
+
 }  // namespace cspb

@@ -35,13 +35,15 @@ enum {
     CSPB_ERR_NEGATIVE = 5,    /* device status: a ragged count is negative, or offsets decrease or do not start at 0 */
     CSPB_ERR_EXCEEDS32 = 6,   /* device status: a ragged value or total is past 2^32 - 1 */
     CSPB_ERR_UNSUPPORTED = 7, /* a dtype / option combination this build does not provide */
-    CSPB_ERR_CUDA = 8         /* another CUDA runtime error (cudaMemsetAsync, cudaMemcpyAsync, ...) */
+    CSPB_ERR_CUDA = 8,        /* another CUDA runtime error (cudaMemsetAsync, cudaMemcpyAsync, ...) */
+    CSPB_ERR_CAPACITY = 9     /* device status: device-computed totals do not fit the capacities the caller declared */
 };
 
 /* bits of the device status word (the first 4 bytes of every workspace) */
 #define CSPB_DEV_TIMEOUT 1u
 #define CSPB_DEV_NEGATIVE 2u
 #define CSPB_DEV_EXCEEDS32 4u
+#define CSPB_DEV_CAPACITY 8u
 
 /* storage dtypes of the big operands (the matrix of a GEMVER, the fields of a stencil) */
 enum { CSPB_F32 = 0, CSPB_BF16 = 1 };
@@ -71,7 +73,11 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
  * (a + u1[i]·v1[j]) + u2[i]·v2[j] with each operation rounded separately (no fused multiply-add), and written to B
  * (row stride ldb) when B is not NULL. Âᵀy is accumulated in f64 and combined in a fixed order; Â·x in f32 with a
  * fixed reduction tree: results do not depend on the launch shape or on other work on the GPU. z may be NULL (zero).
+ * The default schedule pipelines column panels so that the second read of each panel of Â hits L2 (HBM traffic:
+ * A once, Â once); flags = CSPB_GEMVER_BARRIER selects three streaming passes with grid barriers instead
+ * (cooperative launch). Both give bit-identical results.
  * ================================================================================================================== */
+#define CSPB_GEMVER_BARRIER 1
 typedef struct cspb_gemver_desc {
     int64_t n;         /* rows = columns, >= 1 */
     int64_t lda;       /* row stride of A in elements, >= n */
@@ -143,6 +149,47 @@ typedef struct cspb_chain_desc {
 
 size_t cspb_chain_workspace_bytes(int64_t n);
 int cspb_gemver_chain(const cspb_chain_desc* d, void* stream);
+
+/* ==================================================================================================================
+ * Ragged batch of independent GEMVERs in ONE persistent launch.
+ *
+ * Instance k has size n[k] (1 <= n[k] <= 65536). Its matrix starts at element a_off[k] of A (row stride
+ * ld[k] = n[k] rounded up to a multiple of 8, so every row starts on a 16-byte boundary for both dtypes) and its
+ * vectors at element v_off[k] of each packed vector array. The offsets are computed ON THE DEVICE from n[] by the
+ * decoupled-lookback scan (cspb_exclusive_scan_u64) inside the call and written to a_off / v_off (count + 1 entries
+ * each; the last is the total). max_elems / max_vec are the capacities of A (and B) and of each vector array; the
+ * kernel checks the device-computed totals against them before touching memory and sets CSPB_DEV_CAPACITY when they
+ * do not fit (an invalid n[k] sets CSPB_DEV_NEGATIVE). Per-instance alpha[k], beta[k] are device arrays.
+ * `tune` holds 2 bits per size bucket (n < 512, < 1024, < 2048, >= 2048) choosing the tile geometry of that bucket
+ * (0: 8 warps as 2 × 4, 1: 1 × 8, 2: 4 × 2); results depend only on (n, dtype, tune), never on the rest of the batch.
+ * Replaces the per-request launches a caller of the gemver example would make; ragged offsets follow
+ * cs::ragged::counts_from (cospanmdao/include/naga/cospan/shape_hook.hpp:215-348) with u64 element offsets, since
+ * 4096 instances of n up to 4096 overflow the reference's 32-bit offsets (device_scan.hpp:20-23).
+ * ================================================================================================================== */
+typedef struct cspb_gemver_batched_desc {
+    int64_t count;          /* instances, >= 1 */
+    int64_t max_elems;      /* capacity of A and B in elements */
+    int64_t max_vec;        /* capacity of each packed vector array in elements */
+    int32_t a_dtype;        /* CSPB_F32 or CSPB_BF16 */
+    int32_t tune;           /* tile configuration index, 0 = default */
+    const uint32_t* n;      /* device, count */
+    const void* A;
+    const float *u1, *v1, *u2, *v2, *y, *z;  /* packed; z may be NULL */
+    const float* alpha;     /* device, count */
+    const float* beta;      /* device, count */
+    float* B;               /* may be NULL */
+    float* x;
+    float* w;
+    uint64_t* a_off;        /* device out, count + 1 */
+    uint64_t* v_off;        /* device out, count + 1 */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_gemver_batched_desc;
+
+size_t cspb_gemver_batched_workspace_bytes(int64_t count, int64_t max_elems, int64_t max_vec);
+int cspb_gemver_batched(const cspb_gemver_batched_desc* d, void* stream);
+/* Number of tile configurations `tune` may select (1..count-1 are alternatives the autotuner measures). */
+int cspb_gemver_batched_tunings(void);
 
 /* ==================================================================================================================
  * NS residual, compressible (the reference's examples/ns-residual): one evaluation of R = -div F_conv + div F_visc

@@ -101,12 +101,13 @@ def test_gemver_bf16_storage(cuda):
     xo, wo, _ = oracle.gemver_f64(n, A16h, h["u1"], h["v1"], h["u2"], h["v2"], h["y"], h["z"], 1.5, 1.2)
     assert oracle.rel_l2(_np(x), xo) < TOL and oracle.rel_l2(_np(w), wo) < TOL
     assert np.array_equal(_np(B), _rank2_f32(A16h, h["u1"], h["v1"], h["u2"], h["v2"]))
-    # against the f32 matrix's f64 result: the storage error, within the serving bound 1e-3 per output
+    # against the f32 matrix's f64 result: x and w within the serving bound 1e-3; Â carries the bf16 rounding of A
+    # itself (unit roundoff 2^-8, relative L2 about 1e-3 for these inputs), which no kernel can remove
     xf, wf, Bf = oracle.gemver_f64(n, h["A"], h["u1"], h["v1"], h["u2"], h["v2"], h["y"], h["z"], 1.5, 1.2,
                                    want_B=True)
     assert oracle.rel_l2(_np(x), xf) < 1e-3
     assert oracle.rel_l2(_np(w), wf) < 1e-3
-    assert oracle.rel_l2(_np(B), Bf) < 1e-3
+    assert oracle.rel_l2(_np(B), Bf) < 2e-3
 
 
 def test_gemver_deterministic_alone_and_in_the_mix(cuda):
@@ -127,6 +128,21 @@ def test_gemver_deterministic_alone_and_in_the_mix(cuda):
     B1, x1, w1 = cb.gemver(*args, alpha=1.5, beta=1.2)
     torch.cuda.synchronize()
     assert torch.equal(B0, B1) and torch.equal(x0, x1) and torch.equal(w0, w1)
+
+
+@pytest.mark.parametrize("n,dtype_name,want_B", [(1000, "float32", True), (2500, "float32", False),
+                                                 (1800, "bfloat16", True), (300, "float32", True)])
+def test_gemver_panel_and_barrier_schedules_are_bit_identical(cuda, n, dtype_name, want_B):
+    import torch
+    import cospanmdao_b200 as cb
+    d = _inputs(torch, n, seed=11, dtype=getattr(torch, dtype_name))
+    args = (d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"])
+    B0, x0, w0 = cb.gemver(*args, alpha=0.9, beta=1.1, want_B=want_B, schedule="panel")
+    B1, x1, w1 = cb.gemver(*args, alpha=0.9, beta=1.1, want_B=want_B, schedule="barrier")
+    torch.cuda.synchronize()
+    assert torch.equal(x0, x1) and torch.equal(w0, w1)
+    if want_B:
+        assert torch.equal(B0, B1)
 
 
 def test_bicgk(cuda):
