@@ -28,6 +28,8 @@ import tempfile
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -205,7 +207,7 @@ def bench_gemver(torch, cb, dist, args, peak):
 
     def step():
         cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=alpha, beta=beta, B=B, x=x, w=w,
-                  schedule=args.schedule, workspace=ws)
+                  schedule=args.schedule, lag=args.lag, workspace=ws)
 
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
@@ -369,6 +371,66 @@ def bench_ns(torch, cb, dist, args):
     return res
 
 
+def bench_ragged(torch, cb, dist, args, peak):
+    """4096 independent GEMVERs, n ~ log-U[64, 4096], f32, packed, in one persistent launch with device-scanned u64
+    offsets, replayed as a CUDA graph; the tile geometry per size bucket picked by the autotuner."""
+    from cospanmdao_b200 import workloads
+    from cospanmdao_b200.batched import RaggedBatch, autotune
+    sizes = workloads.ragged_sizes(args.ragged)
+    b = RaggedBatch(sizes).fill(seed=0)
+    b.run(check=True)
+    torch.cuda.synchronize()
+    offsets_ok = b.offsets_match()
+    tuned = autotune(b, reps=2)
+    tune = tuned["tune"]
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        b.run(tune=tune)  # warm the allocations outside the capture
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        b.run(tune=tune)
+    ms = timed(torch, dist, graph.replay, max(3, args.steps // 5), args.warmup)
+    nbytes = b.algorithmic_bytes()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    del graph, b
+    torch.cuda.empty_cache()
+    return {"instances": int(sizes.size), "sum_n2": float((sizes.astype(np.float64) ** 2).sum()),
+            "ms": ms, "gbs": gbs, "frac": gbs / peak["hbm_gbs"], "offsets_bit_exact": bool(offsets_ok),
+            "tune": tune, "tune_codes": tuned["codes"], "cuda_graph": True}
+
+
+def bench_serving(torch, dist, args):
+    """The serving stream: 20k requests, 70% GEMVER n ~ log-U[128, 8192], 30% NS residual grids {256², .., 2048²};
+    batched BF16 storage vs the per-request FP32 path; saturation throughput and latency at a Poisson rate."""
+    from cospanmdao_b200 import serving
+    res = {}
+    wl = serving.make_workload(args.requests, rate=None, seed=0)
+    srv = serving.Server(wl, budget_bytes=120e9, max_batch=args.max_batch, depth=4)
+    srv.run()  # warm-up pass (allocations, first launches)
+    sat = srv.run()
+    sample = [int(i) for i in np.linspace(0, wl.count - 1, 24).astype(int)]
+    res["batched_bf16_saturation"] = {k: v for k, v in sat.items()}
+    res["same_alone_and_in_mix"] = bool(serving.check_mix(srv, sample))
+    res["max_rel_err_vs_f64"] = serving.errors_vs_f64(srv, sample)
+    del srv
+    torch.cuda.empty_cache()
+    pl = serving.plain(wl)
+    res["plain_f32_saturation"] = {k: v for k, v in pl.items() if k not in ("out", "norms")}
+    res["throughput_ratio_batched_over_plain"] = sat["req_per_s"] / pl["req_per_s"]
+    rate = 0.5 * sat["req_per_s"]
+    wl2 = serving.make_workload(args.requests, rate=rate, seed=1)
+    srv2 = serving.Server(wl2, budget_bytes=120e9, max_batch=args.max_batch, depth=4)
+    res["batched_bf16_at_rate"] = dict(srv2.run(), rate_req_per_s=rate)
+    del srv2
+    torch.cuda.empty_cache()
+    pl2 = serving.plain(wl2)
+    res["plain_f32_at_rate"] = dict({k: v for k, v in pl2.items() if k not in ("out", "norms")}, rate_req_per_s=rate)
+    return res
+
+
 # ---- the CPU path ---------------------------------------------------------------------------------------------
 def cpu_gemver(n: int, target_s: float = 3.0, reps: int = 3) -> dict:
     """The reference's unfused GEMVER component loops in f32 (oracle port, OpenMP, every host thread) on a bounded
@@ -418,6 +480,10 @@ def main(argv=None) -> int:
     ap.add_argument("--quick", action="store_true", help="headline only (no secondary workloads, no CPU baseline)")
     ap.add_argument("--schedule", default="panel", choices=["panel", "barrier"], help="GEMVER schedule")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--lag", type=int, default=0, help="panel-schedule lag (0: automatic)")
+    ap.add_argument("--ragged", type=int, default=4096, help="instances of the ragged batch")
+    ap.add_argument("--requests", type=int, default=20000, help="requests of the serving stream")
+    ap.add_argument("--max-batch", type=int, default=512, help="serving: requests per batch at most")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     dist = Dist()
@@ -473,6 +539,8 @@ def main(argv=None) -> int:
         sec["gemver_bf16_storage"] = bench_gemver_bf16(torch, cb, dist, args)
         sec["gemver_chain"] = bench_chain(torch, cb, dist, args)
         sec["ns_residual"] = bench_ns(torch, cb, dist, args)
+        sec["ragged_batch"] = bench_ragged(torch, cb, dist, args, pk)
+        sec["serving"] = bench_serving(torch, dist, args)
         line["secondary"] = sec
     if dist.rank == 0 and not args.quick:
         line["cpu_baseline"] = cpu_gemver(args.n)

@@ -47,7 +47,7 @@ def _raise(status: int, what: str) -> None:
         return
     msg = f"{what}: {lib().cspb_status_string(status).decode()}"
     if status in (_capi.ERR_ARGUMENT, _capi.ERR_UNSUPPORTED, _capi.ERR_WORKSPACE, _capi.ERR_NEGATIVE,
-                  _capi.ERR_EXCEEDS32):
+                  _capi.ERR_EXCEEDS32, _capi.ERR_CAPACITY):
         raise ValueError(msg)
     if status == _capi.ERR_TIMEOUT:
         raise DeviceTimeout(msg)
@@ -142,7 +142,7 @@ def _mat_dtype(t):
 
 # ---- GEMVER family ------------------------------------------------------------------------------------------------
 def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: bool = True, B=None, x=None, w=None,
-           schedule: str = "panel", workspace: Workspace | None = None, stream=None):
+           schedule: str = "panel", lag: int = 0, workspace: Workspace | None = None, stream=None):
     """Â = A + u1·v1ᵀ + u2·v2ᵀ, x = β·Âᵀy + z, w = α·Â·x in one launch. A: (n, n) float32 or bfloat16 (a row
     stride from A.stride(0) is honoured). schedule 'panel' (column panels pipelined through L2, the default) or
     'barrier' (three streaming passes); both give the same bits. Returns (B or None, x, w)."""
@@ -171,7 +171,9 @@ def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: b
     ws = workspace or default_workspace(dev, stream)
     need = lib().cspb_gemver_workspace_bytes(n)
     wp, wb = ws.ptr(need)
-    flags = _capi.GEMVER_BARRIER if schedule == "barrier" else 0
+    if not 0 <= int(lag) <= 255:
+        raise ValueError("lag must be in [0, 255]")
+    flags = (_capi.GEMVER_BARRIER if schedule == "barrier" else 0) | (int(lag) << 8)
     d = _capi.GemverDesc(n, A.stride(0), B.stride(0) if B is not None else n, _mat_dtype(A), flags, _ptr(A), _ptr(u1),
                          _ptr(v1), _ptr(u2), _ptr(v2), _ptr(y), _ptr(z), float(alpha), float(beta), _ptr(B), _ptr(x),
                          _ptr(w), wp, wb)

@@ -69,6 +69,16 @@ class BatchedDesc(C.Structure):
                 ("workspace", vp), ("workspace_bytes", sz)]
 
 
+class GemverTask(C.Structure):
+    _fields_ = [("n", i64), ("lda", i64), ("ldb", i64), ("A", vp), ("B", vp), ("u1", vp), ("v1", vp), ("u2", vp),
+                ("v2", vp), ("y", vp), ("z", vp), ("x", vp), ("w", vp), ("alpha", C.c_float), ("beta", C.c_float)]
+
+
+class NsIncompTask(C.Structure):
+    _fields_ = [("nx", i32), ("ny", i32), ("h", C.c_double), ("nu", C.c_double), ("u", vp), ("v", vp), ("p", vp),
+                ("ru", vp), ("rv", vp), ("rc", vp), ("norms", vp)]
+
+
 class NsCompDesc(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("limiter", i32), ("walls", i32), ("U", vp), ("R", vp), ("diag", vp),
                 ("det_sq64", vp), ("workspace", vp), ("workspace_bytes", sz)]
@@ -94,6 +104,9 @@ PROTOTYPES = {
     "cspb_gemver_batched_workspace_bytes": (sz, [i64, i64, i64]),
     "cspb_gemver_batched": (C.c_int, [C.POINTER(BatchedDesc), vp]),
     "cspb_gemver_batched_tunings": (C.c_int, []),
+    "cspb_gemver_tasks": (C.c_int, [vp, i64, i64, i64, i32, i32, vp, sz, vp]),
+    "cspb_ns_incomp_tasks_workspace_bytes": (sz, [i64, i64]),
+    "cspb_ns_incomp_tasks": (C.c_int, [vp, i64, i64, i32, vp, sz, vp]),
     "cspb_ns_comp_workspace_bytes": (sz, [i32, i32]),
     "cspb_ns_compressible": (C.c_int, [C.POINTER(NsCompDesc), vp]),
     "cspb_ns_init_cons": (C.c_int, [vp, i32, i32, C.c_float, vp]),

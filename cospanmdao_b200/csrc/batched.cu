@@ -35,6 +35,7 @@ __host__ __device__ inline int cols_of(int wx, bool bf16) { return wx * 32 * (bf
 struct PlanK {
     int64_t count;
     const uint32_t* n;
+    const cspb_gemver_task* tasks;  // task mode when not NULL
     uint32_t tune;
     int bf16;
     uint64_t* sizes;  // [kSets][count]
@@ -44,8 +45,9 @@ struct PlanK {
 
 __global__ void k_plan(PlanK g) {
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < g.count; k += int64_t(gridDim.x) * blockDim.x) {
-        uint32_t n = g.n[k];
-        if (n < 1 || n > 65536) {
+        const int64_t n64 = g.tasks ? g.tasks[k].n : int64_t(g.n[k]);
+        uint32_t n = (n64 >= 1 && n64 <= 65536) ? uint32_t(n64) : 0u;
+        if (n == 0) {
             set_status(g.ctrl, CSPB_DEV_NEGATIVE);
             n = 0;
         }
@@ -66,6 +68,7 @@ __global__ void k_plan(PlanK g) {
 struct RunK {
     int64_t count;
     const uint32_t* n;
+    const cspb_gemver_task* tasks;  // task mode when not NULL
     const uint8_t* wx;
     const uint64_t* off[kSets];  // each count + 1
     uint64_t cap[kSets - 1];     // capacities of a, v, p, w, s (elements)
@@ -91,24 +94,50 @@ __device__ __forceinline__ int64_t find_instance(const uint64_t* uoff, int64_t c
 }
 
 template <typename T>
-__device__ __forceinline__ PassArgs instance_args(const RunK& g, int64_t k, int wx, bool bf16) {
+__device__ __forceinline__ PassArgs instance_args(const RunK& g, int64_t k, int wx, bool bf16, bool& vec_ok,
+                                                  const float*& z, float& beta, float*& x) {
     PassArgs a{};
-    const uint32_t n = g.n[k];
-    const uint64_t ld = (uint64_t(n) + 7) / 8 * 8;
-    const uint64_t ao = __ldcg(g.off[SA] + k), vo = __ldcg(g.off[SV] + k);
+    uint32_t n;
+    if (g.tasks) {
+        const cspb_gemver_task& t = g.tasks[k];
+        n = uint32_t(t.n);
+        a.src = t.A;
+        a.lds = t.lda;
+        a.dst = t.B;
+        a.ldd = t.ldb;
+        a.u1 = t.u1; a.v1 = t.v1; a.u2 = t.u2; a.v2 = t.v2;
+        a.cyB = t.y;
+        a.xv = t.x;
+        a.rout1 = t.w;
+        a.rscale1 = t.alpha;
+        z = t.z;
+        beta = t.beta;
+        x = t.x;
+        const int eb = bf16 ? 2 : 4;
+        vec_ok = (reinterpret_cast<uintptr_t>(t.A) % 16 == 0) && ((t.lda * eb) % 16 == 0) &&
+                 (t.B == nullptr || ((reinterpret_cast<uintptr_t>(t.B) % 16 == 0) && ((t.ldb * 4) % 16 == 0)));
+    } else {
+        n = g.n[k];
+        const uint64_t ld = (uint64_t(n) + 7) / 8 * 8;
+        const uint64_t ao = __ldcg(g.off[SA] + k), vo = __ldcg(g.off[SV] + k);
+        a.src = static_cast<const T*>(g.A) + ao;
+        a.lds = int64_t(ld);
+        a.dst = g.B ? g.B + ao : nullptr;
+        a.ldd = int64_t(ld);
+        a.u1 = g.u1 + vo; a.v1 = g.v1 + vo; a.u2 = g.u2 + vo; a.v2 = g.v2 + vo;
+        a.cyB = g.y + vo;
+        a.xv = g.x + vo;
+        a.rout1 = g.w + vo;
+        a.rscale1 = g.alpha[k];
+        z = g.z ? g.z + vo : nullptr;
+        beta = g.beta[k];
+        x = g.x + vo;
+        vec_ok = true;  // rows padded to 8 elements, A and B 16-byte aligned (checked by the host)
+    }
     a.n = n;
-    a.src = static_cast<const T*>(g.A) + ao;
-    a.lds = int64_t(ld);
-    a.dst = g.B ? g.B + ao : nullptr;
-    a.ldd = int64_t(ld);
-    a.u1 = g.u1 + vo; a.v1 = g.v1 + vo; a.u2 = g.u2 + vo; a.v2 = g.v2 + vo;
-    a.cyB = g.y + vo;
     a.PB = g.P + __ldcg(g.off[SP] + k);
-    a.xv = g.x + vo;
     a.Wp = g.Wp + __ldcg(g.off[SW] + k);
     a.strip_done = g.strip_done + __ldcg(g.off[SS] + k);
-    a.rout1 = g.w + vo;
-    a.rscale1 = g.alpha[k];
     const int64_t S = rows_of(wx), CW = cols_of(wx, bf16);
     a.strips = (n + S - 1) / S;
     a.chunks = (n + CW - 1) / CW;
@@ -119,29 +148,38 @@ __device__ __forceinline__ PassArgs instance_args(const RunK& g, int64_t k, int 
 __device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, float beta, float* x) {
     for (int64_t j = threadIdx.x; j < a.n; j += blockDim.x) {
         double s = 0.0;
-        for (int64_t st = 0; st < a.strips; ++st) s += __ldcg(a.PB + st * a.n + j);
+        int64_t st = 0;
+        for (; st + 8 <= a.strips; st += 8) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldcg(a.PB + (st + k) * a.n + j);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s += v[k];
+        }
+        for (; st < a.strips; ++st) s += __ldcg(a.PB + st * a.n + j);
         const double zz = z ? double(__ldcg(z + j)) : 0.0;
         x[j] = float(zz + double(beta) * s);
     }
 }
 
 template <typename T, int WX>
-__device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, unsigned char* smem) {
-    pass_unit<T, WX, true, true, false, true, false>(a, unit, true, smem);
+__device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
+    pass_unit<T, WX, true, true, false, true, false>(a, unit, vec_ok, smem);
 }
-template <typename T, int WX, bool FROM_B>
-__device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, unsigned char* smem) {
-    if constexpr (FROM_B) {
+// Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update.
+template <typename T, int WX>
+__device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
+    if (sizeof(T) == 4 && a.dst != nullptr) {
         PassArgs b = a;
         b.src = a.dst;
         b.lds = a.ldd;
-        pass_unit<float, WX, false, false, false, false, true>(b, unit, true, smem);
+        pass_unit<float, WX, false, false, false, false, true>(b, unit, vec_ok, smem);
     } else {
-        pass_unit<T, WX, true, true, false, false, true>(a, unit, true, smem);
+        pass_unit<T, WX, true, true, false, false, true>(a, unit, vec_ok, smem);
     }
 }
 
-template <typename T, bool FROM_B>
+template <typename T>
 __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     constexpr bool bf16 = sizeof(T) == 2;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, 1>() > pass_smem_bytes<T, 4>()
@@ -169,12 +207,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
         const int64_t k = find_instance(g.off[SU], g.count, u);
         const int64_t unit = int64_t(u - __ldcg(g.off[SU] + k));
         const int wx = g.wx[k];
-        const PassArgs a = instance_args<T>(g, k, wx, bf16);
+        bool vec_ok;
+        const float* z;
+        float beta;
+        float* x;
+        const PassArgs a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
         if (!pass2) {
             switch (wx) {
-                case 1: unit1<T, 1>(a, unit, smem); break;
-                case 4: unit1<T, 4>(a, unit, smem); break;
-                default: unit1<T, 2>(a, unit, smem); break;
+                case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
+                case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
+                default: unit1<T, 2>(a, unit, vec_ok, smem); break;
             }
             __threadfence();
             __syncthreads();
@@ -182,8 +224,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
             __syncthreads();
             if (s_last) {
                 __threadfence();
-                const uint64_t vo = __ldcg(g.off[SV] + k);
-                instance_x(a, g.z ? g.z + vo : nullptr, g.beta[k], g.x + vo);
+                instance_x(a, z, beta, x);
                 __threadfence();
                 __syncthreads();
                 if (threadIdx.x == 0) st_release(g.x_ready + k, 1u);
@@ -195,9 +236,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
             if (!s_ok) break;
             __threadfence();
             switch (wx) {
-                case 1: unit2<T, 1, FROM_B>(a, unit, smem); break;
-                case 4: unit2<T, 4, FROM_B>(a, unit, smem); break;
-                default: unit2<T, 2, FROM_B>(a, unit, smem); break;
+                case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
+                case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
+                default: unit2<T, 2>(a, unit, vec_ok, smem); break;
             }
         }
     }
@@ -258,77 +299,82 @@ size_t cspb_gemver_batched_workspace_bytes(int64_t count, int64_t max_elems, int
 
 int cspb_gemver_batched_tunings(void) { return 1 << 8; }
 
-int cspb_gemver_batched(const cspb_gemver_batched_desc* d, void* stream) {
-    if (!d) return CSPB_ERR_ARGUMENT;
-    if (d->count < 1 || d->count > (int64_t(1) << 26) || d->max_elems < 1 || d->max_vec < 1) return CSPB_ERR_ARGUMENT;
-    if (!d->n || !d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->alpha || !d->beta || !d->x || !d->w ||
-        !d->a_off || !d->v_off)
-        return CSPB_ERR_ARGUMENT;
-    if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if (d->tune < 0 || d->tune >= cspb_gemver_batched_tunings()) return CSPB_ERR_UNSUPPORTED;
+}  // extern "C"
+
+namespace {
+
+// The plan, the six scans and the run, for the packed layout (tasks == NULL) or a task table.
+int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype, int32_t tune, const uint32_t* n,
+              const cspb_gemver_task* tasks, const cspb_gemver_batched_desc* d, uint64_t* a_off, uint64_t* v_off,
+              void* workspace, size_t workspace_bytes, void* stream) {
+    if (count < 1 || count > (int64_t(1) << 26) || max_elems < 1 || max_vec < 1) return CSPB_ERR_ARGUMENT;
+    if (a_dtype != CSPB_F32 && a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    if (tune < 0 || tune >= cspb_gemver_batched_tunings()) return CSPB_ERR_UNSUPPORTED;
     for (uint32_t b = 0; b < 4; ++b)
-        if (((uint32_t(d->tune) >> (2 * b)) & 3u) == 3u) return CSPB_ERR_UNSUPPORTED;
-    if (!aligned(d->A, 16) || (d->B && !aligned(d->B, 16))) return CSPB_ERR_ARGUMENT;
-    const BatchLayout L = batch_layout(d->count, d->max_elems, d->max_vec);
-    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+        if (((uint32_t(tune) >> (2 * b)) & 3u) == 3u) return CSPB_ERR_UNSUPPORTED;
+    const BatchLayout L = batch_layout(count, max_elems, max_vec);
+    if (!workspace || !aligned(workspace, 256) || workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
     const cspb_host::DeviceInfo di = cspb_host::device_info();
     if (di.device < 0) return CSPB_ERR_CUDA;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    char* ws = static_cast<char*>(d->workspace);
-    const bool bf16 = d->a_dtype == CSPB_BF16;
-    // control block, p1_done, x_ready, strip counters: one zeroing of the contiguous range
+    char* ws = static_cast<char*>(workspace);
+    const bool bf16 = a_dtype == CSPB_BF16;
+    // control block, p1_done, x_ready, strip counters: zeroed per call
     if (cudaMemsetAsync(ws, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
     if (cudaMemsetAsync(ws + L.off_p1, 0, L.off_scan - L.off_p1, st) != cudaSuccess) return CSPB_ERR_CUDA;
 
     batch::PlanK pk{};
-    pk.count = d->count;
-    pk.n = d->n;
-    pk.tune = uint32_t(d->tune);
+    pk.count = count;
+    pk.n = n;
+    pk.tasks = tasks;
+    pk.tune = uint32_t(tune);
     pk.bf16 = bf16;
     pk.sizes = reinterpret_cast<uint64_t*>(ws + L.off_sizes);
     pk.wx = reinterpret_cast<uint8_t*>(ws + L.off_wx);
     pk.ctrl = reinterpret_cast<uint32_t*>(ws);
-    int64_t pb = (d->count + 255) / 256;
+    int64_t pb = (count + 255) / 256;
     if (pb > 4096) pb = 4096;
     batch::k_plan<<<unsigned(pb), 256, 0, st>>>(pk);
     if (cudaGetLastError() != cudaSuccess) return CSPB_ERR_LAUNCH;
 
     uint64_t* offs = reinterpret_cast<uint64_t*>(ws + L.off_offs);
-    uint64_t* outs[batch::kSets] = {d->a_off, d->v_off, offs, offs + (d->count + 1), offs + 2 * (d->count + 1),
-                                    offs + 3 * (d->count + 1)};
+    uint64_t* outs[batch::kSets] = {a_off, v_off, offs, offs + (count + 1), offs + 2 * (count + 1),
+                                    offs + 3 * (count + 1)};
     for (int s = 0; s < batch::kSets; ++s) {
-        const int r = cspb_exclusive_scan_u64(pk.sizes + size_t(s) * size_t(d->count), outs[s], d->count,
-                                              ws + L.off_scan, cspb_scan_workspace_bytes(d->count), stream);
+        if (!outs[s]) continue;  // task mode: no packed matrix / vector offsets
+        const int r = cspb_exclusive_scan_u64(pk.sizes + size_t(s) * size_t(count), outs[s], count, ws + L.off_scan,
+                                              cspb_scan_workspace_bytes(count), stream);
         if (r != CSPB_OK) return r;
     }
 
     batch::RunK g{};
-    g.count = d->count;
-    g.n = d->n;
+    g.count = count;
+    g.n = n;
+    g.tasks = tasks;
     g.wx = pk.wx;
     for (int s = 0; s < batch::kSets; ++s) g.off[s] = outs[s];
-    g.cap[batch::SA] = uint64_t(d->max_elems);
-    g.cap[batch::SV] = uint64_t(d->max_vec);
+    g.cap[batch::SA] = tasks ? ~0ull : uint64_t(max_elems);
+    g.cap[batch::SV] = tasks ? ~0ull : uint64_t(max_vec);
     g.cap[batch::SP] = L.capP;
     g.cap[batch::SW] = L.capW;
     g.cap[batch::SS] = L.capS;
-    g.A = d->A;
-    g.u1 = d->u1; g.v1 = d->v1; g.u2 = d->u2; g.v2 = d->v2; g.y = d->y; g.z = d->z;
-    g.alpha = d->alpha;
-    g.beta = d->beta;
-    g.B = d->B;
-    g.x = d->x;
-    g.w = d->w;
+    if (d) {
+        g.A = d->A;
+        g.u1 = d->u1; g.v1 = d->v1; g.u2 = d->u2; g.v2 = d->v2; g.y = d->y; g.z = d->z;
+        g.alpha = d->alpha;
+        g.beta = d->beta;
+        g.B = d->B;
+        g.x = d->x;
+        g.w = d->w;
+    }
     g.P = reinterpret_cast<double*>(ws + L.off_P);
     g.Wp = reinterpret_cast<float*>(ws + L.off_W);
     g.strip_done = reinterpret_cast<uint32_t*>(ws + L.off_S);
     g.p1_done = reinterpret_cast<uint32_t*>(ws + L.off_p1);
     g.x_ready = reinterpret_cast<uint32_t*>(ws + L.off_xr);
     g.ctrl = reinterpret_cast<uint32_t*>(ws);
-    const void* kern;
-    if (bf16) kern = reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, false>);
-    else if (d->B) kern = reinterpret_cast<const void*>(batch::k_run<float, true>);
-    else kern = reinterpret_cast<const void*>(batch::k_run<float, false>);
+    const void* kern = bf16 ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16>)
+                            : reinterpret_cast<const void*>(batch::k_run<float>);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, batch::kThreads, 0) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;
@@ -336,6 +382,27 @@ int cspb_gemver_batched(const cspb_gemver_batched_desc* d, void* stream) {
     if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(batch::kThreads), args, 0, st) != cudaSuccess)
         return CSPB_ERR_LAUNCH;
     return CSPB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cspb_gemver_batched(const cspb_gemver_batched_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    if (!d->n || !d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->alpha || !d->beta || !d->x || !d->w ||
+        !d->a_off || !d->v_off)
+        return CSPB_ERR_ARGUMENT;
+    if (!aligned(d->A, 16) || (d->B && !aligned(d->B, 16))) return CSPB_ERR_ARGUMENT;
+    return run_batch(d->count, d->max_elems, d->max_vec, d->a_dtype, d->tune, d->n, nullptr, d, d->a_off, d->v_off,
+                     d->workspace, d->workspace_bytes, stream);
+}
+
+int cspb_gemver_tasks(const cspb_gemver_task* tasks, int64_t count, int64_t max_elems, int64_t max_vec,
+                      int32_t a_dtype, int32_t tune, void* workspace, size_t workspace_bytes, void* stream) {
+    if (!tasks) return CSPB_ERR_ARGUMENT;
+    return run_batch(count, max_elems, max_vec, a_dtype, tune, nullptr, tasks, nullptr, nullptr, nullptr, workspace,
+                     workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -285,7 +285,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
     if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if ((d->flags & ~CSPB_GEMVER_BARRIER) != 0) return CSPB_ERR_UNSUPPORTED;
+    if ((d->flags & ~(CSPB_GEMVER_BARRIER | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->a_dtype == CSPB_BF16;
     const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
@@ -345,12 +345,23 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     g.z = d->z;
     g.beta = d->beta;
     g.x = d->x;
-    g.lag = L.chunks < 1 ? 0 : (L.chunks < 2 ? L.chunks : 1);
+    // Pass 2 over panel c is queued `lag` panels after pass 1 over it. The blocks in flight hold about grid/S panels'
+    // worth of pass-1 units, so a lag past that lets panel c finish before its pass 2 is taken (no waiting), while
+    // the lag+1 panels of Â between the two reads stay well inside L2. Flags bits 8..15 override it (tuning).
     void* args[] = {&g, const_cast<int*>(&vec_ok)};
     const int64_t items = 2 * L.units;
-    if (bf16) return launch_persistent(k_gemver_panel<__nv_bfloat16, false>, args, items, zero, ws, st);
-    if (from_B) return launch_persistent(k_gemver_panel<float, true>, args, items, zero, ws, st);
-    return launch_persistent(k_gemver_panel<float, false>, args, items, zero, ws, st);
+    auto kern = bf16 ? k_gemver_panel<__nv_bfloat16, false>
+                     : (from_B ? k_gemver_panel<float, true> : k_gemver_panel<float, false>);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPassThreads, 0) != cudaSuccess || per_sm < 1)
+        return CSPB_ERR_LAUNCH;
+    const cspb_host::DeviceInfo di = cspb_host::device_info();
+    const int64_t grid = int64_t(per_sm) * di.sms;
+    const int64_t user_lag = (d->flags & CSPB_GEMVER_LAG_MASK) >> 8;
+    int64_t lag = user_lag > 0 ? user_lag : (grid + L.strips - 1) / L.strips + 1;
+    if (lag > L.chunks) lag = L.chunks;
+    g.lag = lag;
+    return launch_persistent(kern, args, items, zero, ws, st);
 }
 
 size_t cspb_bicgk_workspace_bytes(int64_t n) {

@@ -86,10 +86,12 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
     right = need_r ? row.r : from_right;
 }
 
+// Block b (of nblocks) of one residual: its 8 warps take items 8b .. 8b+7. Its norm partial goes to part[b]; the last
+// block to finish (counter `done`) sums the partials in block order.
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
+__device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t item = int64_t(blockIdx.x) * kNsiWarps + warp;
+    const int64_t item = b * kNsiWarps + warp;
     double su = 0.0, sv = 0.0, sc = 0.0;
     if (item < g.items) {  // warp-uniform
         const int seg = int(item % g.segs);
@@ -190,17 +192,106 @@ __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
     if (threadIdx.x < 3) {
         double s = s_red[0][threadIdx.x];
         for (int w = 1; w < kNsiWarps; ++w) s += s_red[w][threadIdx.x];
-        g.part[int64_t(blockIdx.x) * 3 + threadIdx.x] = s;
+        g.part[b * 3 + threadIdx.x] = s;
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(g.ctrl + kDone0, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) s_last = atomicAdd(done, 1u) == uint32_t(nblocks - 1);
     __syncthreads();
     if (s_last && threadIdx.x < 3) {
         __threadfence();
         double s = 0.0;
-        for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(g.part + int64_t(b) * 3 + threadIdx.x);
+        for (int64_t q = 0; q < nblocks; ++q) s += __ldcg(g.part + q * 3 + threadIdx.x);
         if (g.norms) g.norms[threadIdx.x] = sqrt(s);
+    }
+    __syncthreads();  // s_red / s_last are reused by the next block of a persistent caller
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
+    nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
+}
+
+// ---- many residuals in one persistent launch -----------------------------------------------------------------
+__host__ __device__ inline void nsi_shape(int nx, int ny, int vec, int& H, int& segs, int64_t& items, int64_t& blocks) {
+    segs = (nx + 32 * vec - 1) / (32 * vec);
+    H = 32;
+    while (H > 4 && int64_t(segs) * ((ny + H - 1) / H) < 4096) H /= 2;
+    items = int64_t(segs) * ((ny + H - 1) / H);
+    blocks = (items + kNsiWarps - 1) / kNsiWarps;
+}
+
+__device__ __forceinline__ bool nsi_fast(const cspb_ns_incomp_task& t, int vfast) {
+    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    return al(t.u) && al(t.v) && al(t.p) && al(t.ru) && al(t.rv) && al(t.rc) && t.nx % vfast == 0;
+}
+
+struct NsiTasksK {
+    const cspb_ns_incomp_task* tasks;
+    int64_t count;
+    int bf16;
+    uint64_t* blocks;   // [count]
+    uint64_t* boff;     // [count + 1]
+    uint32_t* done;     // [count]
+    double* part;       // [Σ blocks][3]
+    uint64_t cap_blocks;
+    uint32_t* ctrl;
+};
+
+__global__ void k_nsi_plan(NsiTasksK g) {
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < g.count; k += int64_t(gridDim.x) * blockDim.x) {
+        const cspb_ns_incomp_task& t = g.tasks[k];
+        uint64_t nb = 0;
+        if (t.nx >= 3 && t.ny >= 3 && t.u && t.v && t.p && t.ru && t.rv && t.rc) {
+            const int vfast = g.bf16 ? 8 : 4;
+            int H, segs;
+            int64_t items, blocks;
+            nsi_shape(t.nx, t.ny, nsi_fast(t, vfast) ? vfast : 1, H, segs, items, blocks);
+            nb = uint64_t(blocks);
+        } else {
+            set_status(g.ctrl, CSPB_DEV_NEGATIVE);
+        }
+        g.blocks[k] = nb;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
+    __shared__ int s_go;
+    if (threadIdx.x == 0) s_go = __ldcg(g.boff + g.count) <= g.cap_blocks && !status_bad(g.ctrl);
+    __syncthreads();
+    if (!s_go) {
+        if (threadIdx.x == 0 && __ldcg(g.boff + g.count) > g.cap_blocks) set_status(g.ctrl, CSPB_DEV_CAPACITY);
+        return;
+    }
+    const uint64_t total = __ldcg(g.boff + g.count);
+    constexpr int vfast = sizeof(T) == 2 ? 8 : 4;
+    for (;;) {
+        const uint32_t v = grab_work(g.ctrl, kWork0);
+        if (uint64_t(v) >= total) break;
+        int64_t lo = 0, hi = g.count;  // boff[lo] <= v < boff[hi]
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (__ldcg(g.boff + mid) <= v) lo = mid; else hi = mid;
+        }
+        const cspb_ns_incomp_task& t = g.tasks[lo];
+        const bool fast = nsi_fast(t, vfast);
+        NsiK k{};
+        int64_t blocks;
+        nsi_shape(t.nx, t.ny, fast ? vfast : 1, k.H, k.segs, k.items, blocks);
+        k.nx = t.nx;
+        k.ny = t.ny;
+        k.inv2h = float(1.0 / (2.0 * t.h));
+        k.invh2 = float(1.0 / (t.h * t.h));
+        k.nu = float(t.nu);
+        k.u = t.u; k.v = t.v; k.p = t.p;
+        k.ru = t.ru; k.rv = t.rv; k.rc = t.rc;
+        k.norms = t.norms;
+        k.part = g.part + 3 * __ldcg(g.boff + lo);
+        k.ctrl = g.ctrl;
+        const int64_t b = int64_t(v) - int64_t(__ldcg(g.boff + lo));
+        if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
+        else nsi_block<T, 1>(k, b, blocks, g.done + lo);
     }
 }
 
@@ -222,13 +313,33 @@ struct NsiPlan {
 NsiPlan nsi_plan(int nx, int ny, int vec) {
     NsiPlan p;
     p.vec = vec;
-    p.segs = (nx + 32 * vec - 1) / (32 * vec);
-    p.H = 32;
-    while (p.H > 4 && int64_t(p.segs) * ((ny + p.H - 1) / p.H) < 4096) p.H /= 2;
-    p.items = int64_t(p.segs) * ((ny + p.H - 1) / p.H);
-    p.blocks = (p.items + kNsiWarps - 1) / kNsiWarps;
+    nsi_shape(nx, ny, vec, p.H, p.segs, p.items, p.blocks);
     p.ws = align_up(kCtrlBytes + size_t(p.blocks) * 3 * sizeof(double), 256);
     return p;
+}
+
+struct NsiTasksLayout {
+    size_t off_blocks = 0, off_boff = 0, off_done = 0, off_scan = 0, off_part = 0, total = 0;
+    uint64_t cap_blocks = 0;
+};
+
+// Σ blocks over tasks <= Σ (cells/1024 + (nx + ny)/32 + 2) <= max_cells/80 + 3·count (nx, ny >= 3)
+NsiTasksLayout nsi_tasks_layout(int64_t count, int64_t max_cells) {
+    NsiTasksLayout L;
+    L.cap_blocks = uint64_t(max_cells) / 80 + 3 * uint64_t(count);
+    size_t o = kCtrlBytes;
+    L.off_blocks = o;
+    o = align_up(o + size_t(count) * 8, 256);
+    L.off_boff = o;
+    o = align_up(o + size_t(count + 1) * 8, 256);
+    L.off_done = o;
+    o = align_up(o + size_t(count) * 4, 256);
+    L.off_scan = o;
+    o = align_up(o + cspb_scan_workspace_bytes(count), 256);
+    L.off_part = o;
+    o = align_up(o + size_t(L.cap_blocks) * 3 * sizeof(double), 256);
+    L.total = o;
+    return L;
 }
 
 }  // namespace
@@ -280,6 +391,52 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
         else k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+size_t cspb_ns_incomp_tasks_workspace_bytes(int64_t count, int64_t max_cells) {
+    if (count < 1 || max_cells < 1) return 0;
+    return nsi_tasks_layout(count, max_cells).total;
+}
+
+int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_t max_cells, int32_t dtype,
+                         void* workspace, size_t workspace_bytes, void* stream) {
+    if (!tasks || count < 1 || count > (int64_t(1) << 26) || max_cells < 1) return CSPB_ERR_ARGUMENT;
+    if (dtype != CSPB_F32 && dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    const NsiTasksLayout L = nsi_tasks_layout(count, max_cells);
+    if (!workspace || !aligned(workspace, 256) || workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    if (L.cap_blocks >= 0xffffffffull) return CSPB_ERR_ARGUMENT;
+    const cspb_host::DeviceInfo di = cspb_host::device_info();
+    if (di.device < 0) return CSPB_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* ws = static_cast<char*>(workspace);
+    if (cudaMemsetAsync(ws, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
+    if (cudaMemsetAsync(ws + L.off_done, 0, size_t(count) * 4, st) != cudaSuccess) return CSPB_ERR_CUDA;
+    NsiTasksK g{};
+    g.tasks = tasks;
+    g.count = count;
+    g.bf16 = dtype == CSPB_BF16;
+    g.blocks = reinterpret_cast<uint64_t*>(ws + L.off_blocks);
+    g.boff = reinterpret_cast<uint64_t*>(ws + L.off_boff);
+    g.done = reinterpret_cast<uint32_t*>(ws + L.off_done);
+    g.part = reinterpret_cast<double*>(ws + L.off_part);
+    g.cap_blocks = L.cap_blocks;
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    int64_t pb = (count + 255) / 256;
+    if (pb > 4096) pb = 4096;
+    k_nsi_plan<<<unsigned(pb), 256, 0, st>>>(g);
+    if (cudaGetLastError() != cudaSuccess) return CSPB_ERR_LAUNCH;
+    const int r = cspb_exclusive_scan_u64(g.blocks, g.boff, count, ws + L.off_scan, cspb_scan_workspace_bytes(count),
+                                          stream);
+    if (r != CSPB_OK) return r;
+    const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16>)
+                              : reinterpret_cast<const void*>(k_nsi_tasks<float>);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNsiThreads, 0) != cudaSuccess || per_sm < 1)
+        return CSPB_ERR_LAUNCH;
+    void* args[] = {&g};
+    if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(kNsiThreads), args, 0, st) != cudaSuccess)
+        return CSPB_ERR_LAUNCH;
+    return CSPB_OK;
 }
 
 }  // extern "C"

@@ -269,14 +269,38 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
             for (int t = threadIdx.x; t < S; t += kPassThreads) {
                 const int64_t row = strip * S + t;
                 if (row < n) {
+                    // chunks in order; 16 loads in flight at a time (the partials sit in L2)
                     float s = 0.f;
-                    for (int64_t c = 0; c < a.chunks; ++c) s += __ldcg(a.Wp + c * n + row);
+                    int64_t c = 0;
+                    for (; c + 16 <= a.chunks; c += 16) {
+                        float v[16];
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) v[q] = __ldcg(a.Wp + (c + q) * n + row);
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) s += v[q];
+                    }
+                    for (; c < a.chunks; ++c) s += __ldcg(a.Wp + c * n + row);
                     a.rout1[row] = a.rscale1 * s;
                     if (a.rout2) a.rout2[row] = a.rscale2 * s;
                 }
             }
         }
     }
+}
+
+// Σ P[st][j] over st = q, q+4, q+8, ... < strips, in that order, with 8 loads in flight.
+__device__ __forceinline__ double strided_strip_sum(const double* P, int64_t strips, int64_t n, int64_t j, int q) {
+    double s = 0.0;
+    int64_t st = q;
+    for (; st + 28 < strips; st += 32) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldcg(P + (st + 4 * k) * n + j);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s += v[k];
+    }
+    for (; st < strips; st += 4) s += __ldcg(P + st * n + j);
+    return s;
 }
 
 // out[j] = (z ? z[j] : 0) + scale · Σ_s P[s][j] over all strips in index order (f64), rounded once to f32.
@@ -292,9 +316,7 @@ __device__ __forceinline__ void colsum_finish(const double* P, int64_t strips, i
         const bool valid = item < 4 * n;
         const int64_t j = item >> 2;
         const int q = int(item & 3);
-        double s = 0.0;
-        if (valid)
-            for (int64_t st = q; st < strips; st += 4) s += __ldcg(P + st * n + j);
+        double s = valid ? strided_strip_sum(P, strips, n, j, q) : 0.0;
         s += __shfl_xor_sync(kFull, s, 1);
         s += __shfl_xor_sync(kFull, s, 2);
         if (valid && q == 0) {
@@ -315,9 +337,7 @@ __device__ __forceinline__ void colsum_finish_cols(const double* P, int64_t stri
         const bool valid = item < items;
         const int64_t j = c0 + (item >> 2);
         const int q = int(item & 3);
-        double s = 0.0;
-        if (valid)
-            for (int64_t st = q; st < strips; st += 4) s += __ldcg(P + st * n + j);
+        double s = valid ? strided_strip_sum(P, strips, n, j, q) : 0.0;
         s += __shfl_xor_sync(kFull, s, 1);
         s += __shfl_xor_sync(kFull, s, 2);
         if (valid && q == 0) {

@@ -78,6 +78,9 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
  * (cooperative launch). Both give bit-identical results.
  * ================================================================================================================== */
 #define CSPB_GEMVER_BARRIER 1
+/* bits 8..15 of flags: the panel schedule's lag (pass 2 over a panel follows pass 1 over it by this many panels);
+ * 0 = automatic (the panels the blocks in flight hold, plus one). A tuning knob: results do not depend on it. */
+#define CSPB_GEMVER_LAG_MASK 0xff00
 typedef struct cspb_gemver_desc {
     int64_t n;         /* rows = columns, >= 1 */
     int64_t lda;       /* row stride of A in elements, >= n */
@@ -188,8 +191,28 @@ typedef struct cspb_gemver_batched_desc {
 
 size_t cspb_gemver_batched_workspace_bytes(int64_t count, int64_t max_elems, int64_t max_vec);
 int cspb_gemver_batched(const cspb_gemver_batched_desc* d, void* stream);
-/* Number of tile configurations `tune` may select (1..count-1 are alternatives the autotuner measures). */
+/* Number of values `tune` may take (words with a bucket code of 3 are rejected). */
 int cspb_gemver_batched_tunings(void);
+
+/* The same launch over independent GEMVERs that live anywhere (a serving loop's resident models): a DEVICE array of
+ * task descriptors instead of the packed layout. max_elems bounds Σ n·n and max_vec Σ n over the tasks (they size the
+ * workspace: cspb_gemver_batched_workspace_bytes(count, max_elems, max_vec)). Per-task results are bit-identical to
+ * cspb_gemver_fused on the same task (the same tile geometry at tune 0, the same reduction order). */
+typedef struct cspb_gemver_task {
+    int64_t n;
+    int64_t lda;
+    int64_t ldb;
+    const void* A;           /* the call's a_dtype */
+    float* B;                /* may be NULL */
+    const float *u1, *v1, *u2, *v2, *y, *z;  /* z may be NULL */
+    float* x;
+    float* w;
+    float alpha;
+    float beta;
+} cspb_gemver_task;
+
+int cspb_gemver_tasks(const cspb_gemver_task* tasks, int64_t count, int64_t max_elems, int64_t max_vec,
+                      int32_t a_dtype, int32_t tune, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ==================================================================================================================
  * NS residual, compressible (the reference's examples/ns-residual): one evaluation of R = -div F_conv + div F_visc
@@ -250,6 +273,26 @@ typedef struct cspb_ns_incomp_desc {
 
 size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny);
 int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream);
+
+/* Many incompressible residuals (any sizes, one storage dtype) in ONE persistent launch, from a DEVICE array of task
+ * descriptors. max_cells bounds Σ nx·ny (it sizes the workspace). Per-task results, norms included, are bit-identical
+ * to cspb_ns_incompressible on the same task (the same decomposition, the same reduction order). */
+typedef struct cspb_ns_incomp_task {
+    int32_t nx, ny;
+    double h;
+    double nu;
+    const void* u;
+    const void* v;
+    const void* p;
+    float* ru;
+    float* rv;
+    float* rc;
+    double* norms;       /* 3 doubles, may be NULL */
+} cspb_ns_incomp_task;
+
+size_t cspb_ns_incomp_tasks_workspace_bytes(int64_t count, int64_t max_cells);
+int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_t max_cells, int32_t dtype,
+                         void* workspace, size_t workspace_bytes, void* stream);
 
 /* ==================================================================================================================
  * Device scan: out[0..n] = the exclusive scan of in[0..n), out[n] = the total, in ONE single-pass launch
