@@ -478,7 +478,7 @@ def main(argv=None) -> int:
     ap.add_argument("--grid", type=int, default=4096)
     ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed steps before the timed region")
     ap.add_argument("--quick", action="store_true", help="headline only (no secondary workloads, no CPU baseline)")
-    ap.add_argument("--schedule", default="panel", choices=["panel", "barrier"], help="GEMVER schedule")
+    ap.add_argument("--schedule", default="barrier", choices=["panel", "barrier"], help="GEMVER schedule")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--lag", type=int, default=0, help="panel-schedule lag (0: automatic)")
     ap.add_argument("--ragged", type=int, default=4096, help="instances of the ragged batch")

@@ -31,7 +31,7 @@ DEV_CAPACITY = 8
 
 F32 = 0
 BF16 = 1
-GEMVER_BARRIER = 1
+GEMVER_PANEL = 1
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p

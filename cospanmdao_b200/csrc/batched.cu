@@ -191,7 +191,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     __shared__ int s_go;
     if (threadIdx.x == 0) {
         bool fits = 2 * U1 < 0xffffffffull;
-        for (int s = 0; s < kSets - 1; ++s) fits = fits && __ldcg(g.off[s] + g.count) <= g.cap[s];
+        for (int s = 0; s < kSets - 1; ++s)  // task mode has no packed matrix / vector offsets
+            if (g.off[s] != nullptr) fits = fits && __ldcg(g.off[s] + g.count) <= g.cap[s];
         if (!fits) set_status(g.ctrl, CSPB_DEV_CAPACITY);
         s_go = fits && !status_bad(g.ctrl);  // status set by the plan: an invalid size
     }

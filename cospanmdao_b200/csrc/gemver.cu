@@ -1,6 +1,6 @@
 // gemver.cu — GEMVER, BiCGK and the gemver chain as persistent cooperative kernels built from rowpass.cuh.
 //
-// GEMVER, panel-pipelined (the default; one launch, no grid barrier):
+// GEMVER, panel-pipelined (flag CSPB_GEMVER_PANEL; one launch, no grid barrier):
 //   A column panel (CW columns × all n rows) is the unit of dependency: the row-dot partials of panel c need only
 //   x over panel c, which needs only panel c's column sums. The work list runs pass 1 over panel c (read A, write Â,
 //   f64 column partials of Â·y: Rank2Update + GemvTPartial fused), the block finishing the panel's last strip forms
@@ -9,7 +9,9 @@
 //   L2. HBM traffic is then A once and Â once (8n² bytes in f32) instead of the 12n² of three streaming passes; the
 //   last block to finish a strip's row partials writes w = α·dot. A pass-2 block waits (bounded) only on pass-1 work
 //   already taken by running blocks, which never waits itself: no co-residency is assumed.
-// GEMVER, three streaming passes (flag CSPB_GEMVER_BARRIER; cooperative launch):
+// GEMVER, three streaming passes (the default; cooperative launch). Measured faster than the panel schedule at
+// n = 16384 on B200 although it moves a third more bytes: the panel order reads 1 KB row segments of ~2 panels at
+// a time across every row, which HBM serves less efficiently than the strip order's whole rows.
 //   pass 1   read A, write Â, f64 column partials        | grid barrier, x = z + β·Σ partials, grid barrier
 //   pass 2   read Â (or A again), row dots with x, w;  walked from the last strip back (recently written Â in L2).
 // Both schedules produce bit-identical results (the same partials, combined in the same order).
@@ -285,7 +287,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
     if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if ((d->flags & ~(CSPB_GEMVER_BARRIER | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
+    if ((d->flags & ~(CSPB_GEMVER_PANEL | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->a_dtype == CSPB_BF16;
     const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
@@ -322,7 +324,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t zero = L.off_PA;  // ctrl, strip_done, chunk_done, x_ready
 
-    if (d->flags & CSPB_GEMVER_BARRIER) {
+    if (!(d->flags & CSPB_GEMVER_PANEL)) {
         GemverK g{};
         g.p1 = p1;
         g.p2 = p2;

@@ -73,11 +73,11 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
  * (a + u1[i]·v1[j]) + u2[i]·v2[j] with each operation rounded separately (no fused multiply-add), and written to B
  * (row stride ldb) when B is not NULL. Âᵀy is accumulated in f64 and combined in a fixed order; Â·x in f32 with a
  * fixed reduction tree: results do not depend on the launch shape or on other work on the GPU. z may be NULL (zero).
- * The default schedule pipelines column panels so that the second read of each panel of Â hits L2 (HBM traffic:
- * A once, Â once); flags = CSPB_GEMVER_BARRIER selects three streaming passes with grid barriers instead
- * (cooperative launch). Both give bit-identical results.
+ * The default schedule is three streaming passes with grid barriers (cooperative launch); flags = CSPB_GEMVER_PANEL
+ * pipelines column panels instead, so that the second read of each panel of Â hits L2 (HBM traffic: A once, Â once).
+ * Both give bit-identical results.
  * ================================================================================================================== */
-#define CSPB_GEMVER_BARRIER 1
+#define CSPB_GEMVER_PANEL 1
 /* bits 8..15 of flags: the panel schedule's lag (pass 2 over a panel follows pass 1 over it by this many panels);
  * 0 = automatic (the panels the blocks in flight hold, plus one). A tuning knob: results do not depend on it. */
 #define CSPB_GEMVER_LAG_MASK 0xff00
