@@ -1,0 +1,69 @@
+"""Builds the reference's example programs, unchanged, against the cs:: runtime of this package.
+
+    python -m cospanmdao_b200.examples [--reference /path/to/CospanMDAO]
+
+The sources are read from the reference tree (gemver-chain, ns-residual, getting-started), passed through the
+annotation step (annotate.py: nvcc needs __host__ __device__ on what kernels call), and compiled with nvcc for sm_100a
+against cospanmdao_b200/include. Binaries go to cospanmdao_b200/_examples/ (built here, next to the library, so they
+travel with the tree); the annotated copies go to cospanmdao_b200/_examples/src/. Nothing of the reference is kept in
+the repository.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+from .annotate import annotate_tree
+from .build import ARCH, nvcc
+
+PKG = Path(__file__).resolve().parent
+OUT = PKG / "_examples"
+PROGRAMS = {
+    "gemver-chain": ("examples/gemver-chain", "main.cpp"),
+    "ns-residual": ("examples/ns-residual", "main.cpp"),
+    "getting-started": ("getting-started", "main.cpp"),
+}
+
+
+def build_examples(reference: str | os.PathLike | None = None, verbose: bool = False) -> dict[str, Path]:
+    ref = Path(reference or os.environ.get("CSPB_REFERENCE_DIR", "/root/reference"))
+    if not (ref / "examples").is_dir():
+        raise FileNotFoundError(f"no reference tree at {ref}")
+    built = {}
+    procs = []
+    for name, (sub, main) in PROGRAMS.items():
+        src = OUT / "src" / name
+        annotate_tree(ref / sub, src)
+        exe = OUT / name
+        cmd = [nvcc(), "-std=c++20", "-O2", *ARCH, "-I", str(PKG / "include"), "--extended-lambda",
+               "--expt-relaxed-constexpr", "-x", "cu", str(src / main), "-o", str(exe)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((name, exe, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    errors = []
+    for name, exe, cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            errors.append(f"{name}: {' '.join(cmd)}\n{out}")
+        else:
+            built[name] = exe
+    if errors:
+        raise RuntimeError("building the examples failed:\n" + "\n".join(errors))
+    return built
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", default=None)
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args(argv)
+    for k, v in build_examples(a.reference, a.verbose).items():
+        print(k, v)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,667 @@
+// naga/cospan/model.hpp — cs::Model and the runtime under it.
+//
+// Lifecycle (model.hpp:447-532 of the reference): create_model<Root>(args) builds the root System; setup() runs the
+// user's setup (children are declared / set up as they are added); the first run() or update_input() finalizes the
+// wiring into VARIABLES (one device buffer each: a connect, a tie or a promotion names the same variable); run()
+// walks the leaves in declaration order on one CUDA stream — each component's inputs are shaped and materialized
+// (allocated, initialized when stale), prepare_forward() shapes its outputs, define_forward() says how it launches —
+// and pushes open host views; wait() synchronizes and raises device-side failures.
+//
+// Leaves whose stages form a chain the cspb library implements as one hand-written kernel (the GEMVER and BiCGK
+// stages of the gemver example, the NS fused group of the ns-residual example) run that kernel through the C ABI
+// (patterns.hpp); every other leaf runs its own component bodies (component.hpp, system.hpp).
+#pragma once
+
+#include <map>
+#include <numeric>
+#include <set>
+
+#include "naga/slabkit/slabkit.hpp"
+#include "system.hpp"
+
+namespace naga::cospan {
+
+namespace detail {
+
+inline void cuda_check(cudaError_t e, const std::string& what) {
+    if (e != cudaSuccess) throw std::runtime_error("naga::cospan: " + what + ": " + cudaGetErrorString(e));
+}
+
+struct ViewState {
+    int var = -1;
+    void* host = nullptr;
+    std::size_t bytes = 0;
+    std::array<std::size_t, 4> shape{};
+    cudaEvent_t ev = nullptr;
+    ~ViewState() {
+        if (host) cudaFreeHost(host);
+        if (ev) cudaEventDestroy(ev);
+    }
+};
+
+struct Var {
+    int id = -1;
+    std::string name;
+    DType dtype = DType::f32;
+    int rank = -1;
+    ShapeSpec spec;                   // what declarations and ties fix
+    std::vector<HookDim> hook;        // a shape hook on it
+    System* hook_sys = nullptr;
+    std::array<std::size_t, 4> shape{};
+    bool shape_known = false;
+    bool shape_from_prepare = false;  // set by a producer's prepare_forward (re-derived every run)
+    void* data = nullptr;
+    std::size_t capacity = 0;
+    std::optional<InitSpec> init;
+    bool stale = false;
+    bool produced = false;
+    std::size_t elements() const {
+        std::size_t n = 1;
+        for (int d = 0; d < rank; ++d) n *= shape[d];
+        return n;
+    }
+    std::size_t bytes() const { return elements() * dtype_size(dtype); }
+};
+
+struct InitTarget {
+    Runtime& rt;
+    Var& var;
+};
+
+class Runtime {
+public:
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::uint32_t* ctrl = nullptr;  // 256 bytes: status word, barrier counters
+    std::vector<Var> vars;
+    std::vector<Node*> leaves;
+    std::vector<ComponentBase*> components;  // every component, stages included
+    std::vector<std::shared_ptr<ViewState>> views;
+    std::unique_ptr<sk::unordered_queue> uq;
+    std::map<std::string, int> key_var;      // port / tie key -> variable
+    std::map<std::string, std::string> tie_keys;  // system path + "/" + alias -> tie key
+    std::vector<std::function<bool(Runtime&, std::size_t&)>> pattern_runs;  // per leaf index: a fast path
+    std::vector<int> pattern_at;             // leaf index -> pattern index or -1 (-2: covered, skip)
+    std::vector<struct PatternRec*> pattern_recs;
+    int sms = 0;
+
+    Runtime() {
+        cuda_check(cudaGetDevice(&device), "cudaGetDevice");
+        cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+        cuda_check(cudaMalloc(&ctrl, 256), "control block");
+        cuda_check(cudaMemset(ctrl, 0, 256), "control block");
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        uq = std::make_unique<sk::unordered_queue>(stream);
+    }
+    ~Runtime() {
+        cudaStreamSynchronize(stream);
+        for (auto& v : vars)
+            if (v.data) cudaFree(v.data);
+        if (ctrl) cudaFree(ctrl);
+        views.clear();
+        uq.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // ---- shapes and memory ----
+    void shape_from_hook(Var& v) {
+        if (v.hook.empty()) return;
+        if (int(v.hook.size()) != v.rank)
+            throw std::invalid_argument("naga::cospan: the shape hook of '" + v.name + "' has " + std::to_string(v.hook.size()) +
+                                        " dimensions, the variable has rank " + std::to_string(v.rank));
+        for (int d = 0; d < v.rank; ++d) {
+            const HookDim& h = v.hook[d];
+            if (auto f = std::get_if<dim::FixedAtRun>(&h)) v.shape[d] = f->v;
+            else if (auto s = std::get_if<dim::FromShape>(&h)) {
+                Var& o = var_of_path(v.hook_sys, s->path);
+                ensure_shape(o);
+                v.shape[d] = o.shape[s->d];
+            } else if (!v.shape_known)
+                throw std::invalid_argument("naga::cospan: '" + v.name + "': as_is on a dimension with no shape");
+        }
+        v.shape_known = true;
+    }
+    void ensure_shape(Var& v) {
+        if (v.shape_known) return;
+        if (!v.hook.empty()) {
+            shape_from_hook(v);
+            return;
+        }
+        if (!v.spec.empty()) {
+            bool all = true;
+            for (int d = 0; d < v.rank; ++d) all = all && v.spec.known[d];
+            if (all) {
+                for (int d = 0; d < v.rank; ++d) v.shape[d] = v.spec.ext[d];
+                v.shape_known = true;
+                return;
+            }
+        }
+        if (v.init && !v.init->shape && v.init->flat && v.rank == 1) {
+            v.shape[0] = *v.init->flat;
+            v.shape_known = true;
+            return;
+        }
+        if (v.init && v.init->shape && int(v.init->shape->size()) == v.rank) {
+            for (int d = 0; d < v.rank; ++d) v.shape[d] = (*v.init->shape)[d];
+            v.shape_known = true;
+            return;
+        }
+        throw std::invalid_argument("naga::cospan: the shape of '" + v.name + "' is not known (no declaration, hook, "
+                                    "initializer or producer gives it)");
+    }
+    void allocate(Var& v) {
+        const std::size_t b = std::max<std::size_t>(v.bytes(), 16);
+        if (v.data && v.capacity >= b) return;
+        if (v.data) {
+            cuda_check(cudaStreamSynchronize(stream), "resize");
+            cudaFree(v.data);
+        }
+        cuda_check(cudaMalloc(&v.data, b), "allocating '" + v.name + "'");
+        v.capacity = b;
+    }
+    void materialize(Var& v) {
+        ensure_shape(v);
+        allocate(v);
+        if (v.stale && v.init) {
+            if (v.init->shape) {
+                std::size_t n = 1;
+                for (auto e : *v.init->shape) n *= e;
+                if (n != v.elements())
+                    throw std::invalid_argument("naga::cospan: the initializer of '" + v.name + "' has " + std::to_string(n) +
+                                                " elements, the variable " + std::to_string(v.elements()));
+            }
+            InitTarget t{*this, v};
+            v.init->run(t);
+            v.stale = false;
+        }
+    }
+
+    // ---- names ----
+    std::string resolve(System* s, const std::string& path) {
+        auto a = s->aliases_.find(path);
+        if (a != s->aliases_.end()) return resolve(s, a->second.target);
+        auto t = tie_keys.find(s->path() + "/" + path);
+        if (t != tie_keys.end()) return t->second;
+        const auto dot = path.find('.');
+        const std::string head = path.substr(0, dot);
+        Node* c = s->child(head);
+        if (!c)
+            throw std::invalid_argument("naga::cospan: '" + (s->path().empty() ? std::string("<root>") : s->path()) +
+                                        "' has no port or name '" + path + "'");
+        if (dot == std::string::npos)
+            throw std::invalid_argument("naga::cospan: '" + c->path() + "' is a subsystem, not a port");
+        const std::string rest = path.substr(dot + 1);
+        if (c->kind == Node::Kind::component) {
+            auto* comp = static_cast<ComponentBase*>(c);
+            if (!comp->port(rest))
+                throw std::invalid_argument("naga::cospan: '" + comp->path() + "' has no port '" + rest + "'");
+            return comp->path() + "." + rest;
+        }
+        return resolve(static_cast<System*>(c), rest);
+    }
+    Var& var_of_path(System* s, const std::string& path) {
+        const std::string k = resolve(s, path);
+        auto it = key_var.find(k);
+        if (it == key_var.end()) throw std::logic_error("naga::cospan: '" + k + "' has no variable");
+        return vars[it->second];
+    }
+    Var& var_of_port(ComponentBase* c, const std::string& port) { return vars[key_var.at(c->path() + "." + port)]; }
+
+    // ---- running one component (a solo leaf, or a stage of a fused group) ----
+    void prepare(ComponentBase* c) {
+        c->rt_ = this;
+        for (auto& p : c->ports_) {
+            if (p.output) continue;
+            Var& v = vars[p.var];
+            if (!v.produced && !v.init && !v.data)
+                throw std::invalid_argument("naga::cospan: the input '" + c->path() + "." + p.name + "' (variable '" +
+                                            v.name + "') is never initialized");
+            materialize(v);
+            p.bind(v.data, v.shape.data());
+        }
+        for (auto& p : c->ports_)
+            if (p.output) {
+                Var& v = vars[p.var];
+                if (v.shape_from_prepare) v.shape_known = false;
+            }
+        c->prepare_forward();
+        for (auto& p : c->ports_) {
+            if (!p.output) continue;
+            Var& v = vars[p.var];
+            materialize(v);
+            p.bind(v.data, v.shape.data());
+        }
+    }
+    void run_component(ComponentBase* c) {
+        prepare(c);
+        std::unique_ptr<LaunchDescription> d = c->define_forward();
+        if (d) c->launch_solo(*this, *d);
+    }
+};
+
+// ---- initializer kernels ----
+template <class T>
+__global__ void k_fill(T* p, std::size_t n, T v) {
+    for (std::size_t i = std::size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += std::size_t(gridDim.x) * blockDim.x)
+        p[i] = v;
+}
+template <class T>
+inline void fill_var(Runtime& rt, Var& v, T value) {
+    const std::size_t n = v.elements();
+    if (n == 0) return;
+    const unsigned blocks = unsigned(std::min<std::size_t>((n + 255) / 256, 65535));
+    k_fill<T><<<blocks, 256, 0, rt.stream>>>(static_cast<T*>(v.data), n, value);
+    cuda_check(cudaGetLastError(), "fill");
+}
+template <class V>
+inline void fill_any(Runtime& rt, Var& v, V value) {
+    switch (value_dtype(v.dtype)) {
+        case DType::f32: fill_var<float>(rt, v, float(value)); break;
+        case DType::f64: fill_var<double>(rt, v, double(value)); break;
+        case DType::i32: fill_var<std::int32_t>(rt, v, std::int32_t(value)); break;
+        case DType::u32: fill_var<std::uint32_t>(rt, v, std::uint32_t(value)); break;
+        case DType::i64: fill_var<std::int64_t>(rt, v, std::int64_t(value)); break;
+        case DType::u64: fill_var<std::uint64_t>(rt, v, std::uint64_t(value)); break;
+        default: fill_var<std::uint8_t>(rt, v, std::uint8_t(value)); break;
+    }
+}
+
+template <int R>
+inline void set_range(sycl::range<R>& shape, sycl::range<R>& stride, const std::array<std::size_t, 4>& s) {
+    std::size_t st = 1;
+    for (int d = R - 1; d >= 0; --d) {
+        shape[d] = s[d];
+        stride[d] = st;
+        st *= s[d];
+    }
+}
+
+}  // namespace detail
+
+// ---- initializers (init.hpp) ----------------------------------------------------------------------------------------
+namespace init {
+template <class T>
+InitSpec fill(T value) {
+    InitSpec s;
+    s.scalar = double(value);
+    s.run = [value](detail::InitTarget& t) { detail::fill_any(t.rt, t.var, value); };
+    return s;
+}
+template <class T>
+InitSpec fill(T value, const Shape& shape) {
+    InitSpec s = fill(value);
+    s.shape = shape.ext;
+    return s;
+}
+inline InitSpec zero() { return fill(0); }
+inline InitSpec zero(const Shape& shape) { return fill(0, shape); }
+template <class T>
+InitSpec from_host(std::vector<T> values) {
+    // the flat form checks the element count only (the variable's own shape decides its rank)
+    InitSpec s;
+    auto data = std::make_shared<std::vector<T>>(std::move(values));
+    const std::size_t n = data->size();
+    s.run = [data, n](detail::InitTarget& t) {
+        if (n != t.var.elements())
+            throw std::invalid_argument("naga::cospan: init::from_host has " + std::to_string(n) + " values, '" + t.var.name +
+                                        "' has " + std::to_string(t.var.elements()) + " elements");
+        if (sizeof(T) != dtype_size(t.var.dtype))
+            throw std::invalid_argument("naga::cospan: init::from_host for '" + t.var.name + "' has the wrong element type");
+        detail::cuda_check(cudaMemcpyAsync(t.var.data, data->data(), n * sizeof(T), cudaMemcpyHostToDevice, t.rt.stream),
+                           "from_host");
+        detail::cuda_check(cudaStreamSynchronize(t.rt.stream), "from_host");
+    };
+    s.flat = n;
+    return s;
+}
+template <class T>
+InitSpec from_host(std::vector<T> values, const Shape& shape) {
+    if (shape.elements() != values.size())
+        throw std::invalid_argument("naga::cospan: init::from_host has " + std::to_string(values.size()) +
+                                    " values but its shape has " + std::to_string(shape.elements()) + " elements");
+    InitSpec s = from_host(std::move(values));
+    s.shape = shape.ext;
+    return s;
+}
+template <DType DT, int R>
+InitSpec custom(CustomFn<DT, R> fn) {
+    InitSpec s;
+    s.run = [fn = std::move(fn)](detail::InitTarget& t) {
+        if (!dtype_compatible(t.var.dtype, DT) || t.var.rank != R)
+            throw std::invalid_argument("naga::cospan: init::custom for '" + t.var.name +
+                                        "' was declared with the wrong dtype or rank");
+        Initializer<DT, R> w;
+        w.data_ = static_cast<cpp_type_t<DT>*>(t.var.data);
+        detail::set_range<R>(w.shape_, w.stride_, t.var.shape);
+        sycl::device dev(t.rt.device);
+        fn(*t.rt.uq, dev, std::vector<sycl::event>{}, w);
+    };
+    return s;
+}
+template <DType DT, int R>
+InitSpec custom(CustomFn<DT, R> fn, const Shape& shape) {
+    InitSpec s = custom<DT, R>(std::move(fn));
+    s.shape = shape.ext;
+    return s;
+}
+}  // namespace init
+
+// ---- component pieces that need the runtime -------------------------------------------------------------------------
+template <DType DT, int R>
+sycl::range<R> ComponentBase::shape_of(const Input<DT, R>& w) const {
+    for (const auto& p : ports_)
+        if (p.wrapper == static_cast<const void*>(&w)) {
+            detail::Var& v = rt_->vars[p.var];
+            rt_->ensure_shape(v);
+            sycl::range<R> r;
+            for (int d = 0; d < R; ++d) r[d] = v.shape[d];
+            return r;
+        }
+    throw std::logic_error("naga::cospan: '" + path() + "': shape_of on a port it does not own");
+}
+template <DType DT, int R, class... E>
+void ComponentBase::set_shape(Output<DT, R>& w, E... e) {
+    static_assert(sizeof...(E) == R, "set_shape needs one extent per dimension");
+    for (auto& p : ports_)
+        if (p.wrapper == static_cast<const void*>(&w)) {
+            detail::Var& v = rt_->vars[p.var];
+            const std::array<std::size_t, 4> s{static_cast<std::size_t>(e)...};
+            for (int d = 0; d < R; ++d) v.shape[d] = s[d];
+            v.shape_known = true;
+            v.shape_from_prepare = true;
+            return;
+        }
+    throw std::logic_error("naga::cospan: '" + path() + "': set_shape on a port it does not own");
+}
+
+namespace detail {
+inline LocalLayout local_layout(const std::vector<std::size_t>& elem, const LaunchDescription& d, std::uint32_t base,
+                                std::size_t& bytes, const std::string& who) {
+    LocalLayout L;
+    L.base = base;
+    if (elem.size() != d.local.size())
+        throw std::invalid_argument("naga::cospan: '" + who + "' declares " + std::to_string(elem.size()) +
+                                    " local arrays but its launch describes " + std::to_string(d.local.size()));
+    if (elem.size() > L.shapes.size()) throw std::invalid_argument("naga::cospan: '" + who + "': too many local arrays");
+    std::size_t off = 0;
+    for (std::size_t i = 0; i < elem.size(); ++i) {
+        off = (off + 15) / 16 * 16;
+        L.offsets[i] = off;
+        L.shapes[i] = d.local[i];
+        off += elem[i] * d.local[i][0] * d.local[i][1] * d.local[i][2];
+    }
+    bytes = (off + 15) / 16 * 16;
+    return L;
+}
+inline void group_geometry(const LaunchDescription& d, int R, std::array<std::size_t, 3>& groups,
+                           std::array<std::size_t, 3>& local, std::uint64_t& count, const std::string& who) {
+    if (d.rank != R)
+        throw std::invalid_argument("naga::cospan: '" + who + "': the launch range has rank " + std::to_string(d.rank) +
+                                    ", the body " + std::to_string(R));
+    count = 1;
+    for (int k = 0; k < R; ++k) {
+        local[k] = d.has_wg ? d.wg[k] : (k == R - 1 ? 128 : 1);
+        if (local[k] == 0 || d.range[k] % local[k] != 0)
+            throw std::invalid_argument("naga::cospan: '" + who + "': the launch range is not a multiple of the work-group");
+        groups[k] = d.range[k] / local[k];
+        count *= groups[k];
+    }
+}
+}  // namespace detail
+
+template <class X>
+void Component<X>::launch_solo(detail::Runtime& rt, const LaunchDescription& d) {
+    constexpr int R = detail::body_rank<X>;
+    X* self = static_cast<X*>(this);
+    if constexpr (!detail::is_group_body<X>) {
+        if (d.rank != R) throw std::invalid_argument("naga::cospan: '" + path() + "': launch range of the wrong rank");
+        sycl::range<R> r;
+        std::uint64_t total = 1;
+        for (int k = 0; k < R; ++k) {
+            r[k] = d.range[k];
+            total *= d.range[k];
+        }
+        if (total == 0) return;
+        const unsigned blocks = unsigned(std::min<std::uint64_t>((total + 255) / 256, std::uint64_t(rt.sms) * 16));
+        detail::k_index<X, R><<<blocks, 256, 0, rt.stream>>>(self->inputs, self->outputs, r, total);
+    } else {
+        std::array<std::size_t, 3> g3, l3;
+        std::uint64_t count;
+        detail::group_geometry(d, R, g3, l3, count, path());
+        if (count == 0) return;
+        sycl::range<R> groups, local;
+        std::size_t threads = 1;
+        for (int k = 0; k < R; ++k) {
+            groups[k] = g3[k];
+            local[k] = l3[k];
+            threads *= l3[k];
+        }
+        std::size_t smem = 0;
+        const detail::LocalLayout L = detail::local_layout(local_elem_sizes(), d, 0, smem, path());
+        auto kern = detail::k_group<X, R>;
+        if (smem > 48 * 1024)
+            detail::cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), path());
+        const unsigned blocks = unsigned(std::min<std::uint64_t>(count, std::uint64_t(rt.sms) * 32));
+        kern<<<blocks, unsigned(threads), smem, rt.stream>>>(self->inputs, self->outputs, groups, local, count, L);
+    }
+    detail::cuda_check(cudaGetLastError(), "launching '" + path() + "'");
+}
+
+namespace detail {
+template <class List> struct fused_params_of;
+template <class... Xs> struct fused_params_of<tlist<Xs...>> {
+    using type = FusedParams<Xs...>;
+    static constexpr std::size_t n = sizeof...(Xs);
+    template <std::size_t... I>
+    static void bind_io(type& p, const std::vector<ComponentBase*>& st, std::index_sequence<I...>) {
+        ((std::get<I>(p.io) = std::make_pair(static_cast<Xs*>(st[I])->inputs, static_cast<Xs*>(st[I])->outputs)), ...);
+    }
+    static std::vector<std::vector<std::size_t>> elems() {
+        return {[] {
+            using LM = body_local_t<Xs>;
+            if constexpr (std::is_void_v<LM>) return std::vector<std::size_t>{};
+            else {
+                auto a = local_arrays<LM>::elem_sizes();
+                return std::vector<std::size_t>(a.begin(), a.end());
+            }
+        }()...};
+    }
+    static std::vector<int> ranks() { return {body_rank<Xs>...}; }
+    static std::vector<bool> groups() { return {is_group_body<Xs>...}; }
+    static const void* kernel() { return reinterpret_cast<const void*>(k_fused<Xs...>); }
+};
+}  // namespace detail
+
+template <class Opts, class... Items>
+void FusedGroup<Opts, Items...>::launch(detail::Runtime& rt) {
+    using List = typename detail::stages_of_all<Items...>::type;
+    using FP = detail::fused_params_of<List>;
+    using P = typename FP::type;
+    static_assert(FP::n <= detail::kMaxStages, "too many stages in one fused group");
+    P p{};
+    const auto elems = FP::elems();
+    const auto ranks = FP::ranks();
+    const auto kinds = FP::groups();
+    const int nseg = int(segment_local_shared_.size());
+    if (nseg > detail::kMaxSegments) throw std::invalid_argument("naga::cospan: '" + path() + "': too many segments");
+    std::vector<std::size_t> seg_base(nseg, 0), seg_bytes(nseg, 0);
+    std::size_t threads = 0;
+    for (std::size_t i = 0; i < stages_.size(); ++i) {
+        ComponentBase* c = stages_[i];
+        if (!kinds[i])
+            throw std::invalid_argument("naga::cospan: '" + c->path() + "': index-range stages in a fused group are not "
+                                        "provided by this backend (give the stage a work-group body)");
+        rt.prepare(c);
+        std::unique_ptr<LaunchDescription> d = c->define_forward();
+        if (!d) throw std::invalid_argument("naga::cospan: '" + c->path() + "' describes no launch");
+        detail::StageGeom& g = p.st[i];
+        const int s = stage_segment_[i];
+        g.segment = std::uint32_t(s);
+        g.whole = std::uint32_t(segment_whole_[s]);
+        detail::group_geometry(*d, ranks[i], g.groups, g.local, g.count, c->path());
+        std::size_t th = g.local[0] * g.local[1] * g.local[2];
+        if (threads == 0) threads = th;
+        else if (threads != th)
+            throw std::invalid_argument("naga::cospan: '" + path() + "': its stages have different work-group sizes");
+        std::size_t bytes = 0;
+        const std::uint32_t base = segment_local_shared_[s] ? 0u : std::uint32_t(seg_bytes[s]);
+        g.local_mem = detail::local_layout(elems[i], *d, base, bytes, c->path());
+        seg_bytes[s] = segment_local_shared_[s] ? std::max(seg_bytes[s], bytes) : seg_bytes[s] + bytes;
+        p.seg[s].count = std::max<std::uint64_t>(p.seg[s].count, g.count);
+    }
+    FP::bind_io(p, stages_, std::make_index_sequence<FP::n>{});
+    p.nseg = std::uint32_t(nseg);
+    p.ctrl = rt.ctrl;
+    std::size_t smem = 0;
+    for (auto b : seg_bytes) smem = std::max(smem, b);
+    std::uint64_t most = 0;
+    for (int s = 0; s < nseg; ++s) most = std::max(most, p.seg[s].count);
+    if (most == 0 || threads == 0) return;
+    const void* kern = FP::kernel();
+    if (smem > 48 * 1024)
+        detail::cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), path());
+    int per_sm = 0;
+    detail::cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(threads), smem), path());
+    if (per_sm < 1) throw std::invalid_argument("naga::cospan: '" + path() + "': a work-group does not fit an SM");
+    const unsigned grid = unsigned(std::min<std::uint64_t>(most, std::uint64_t(per_sm) * rt.sms));
+    detail::cuda_check(cudaMemsetAsync(rt.ctrl + 1, 0, 8, rt.stream), "fused group barrier");
+    void* args[] = {&p};
+    if (nseg > 1)
+        detail::cuda_check(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(unsigned(threads)), args, smem, rt.stream),
+                           "launching '" + path() + "'");
+    else
+        detail::cuda_check(cudaLaunchKernel(kern, dim3(grid), dim3(unsigned(threads)), args, smem, rt.stream),
+                           "launching '" + path() + "'");
+}
+
+// ---- host views (host_view.hpp:103-152) ------------------------------------------------------------------------------
+template <DType DT, int R>
+class HostView {
+public:
+    using value_type = cpp_type_t<DT>;
+    explicit HostView(std::shared_ptr<detail::ViewState> s) : s_(std::move(s)) {}
+    void sync() const {
+        if (s_->ev) detail::cuda_check(cudaEventSynchronize(s_->ev), "view sync");
+    }
+    std::span<const value_type> span() const {
+        return std::span<const value_type>(static_cast<const value_type*>(s_->host), s_->bytes / sizeof(value_type));
+    }
+    sycl::range<R> shape() const {
+        sycl::range<R> r;
+        for (int d = 0; d < R; ++d) r[d] = s_->shape[d];
+        return r;
+    }
+    const value_type& operator[](std::size_t i) const { return span()[i]; }
+
+private:
+    std::shared_ptr<detail::ViewState> s_;
+};
+
+// ---- the model --------------------------------------------------------------------------------------------------------
+namespace detail {
+void register_patterns(Runtime& rt);  // patterns.hpp
+}
+
+class Model {
+public:
+    explicit Model(std::unique_ptr<System> root) : root_(std::move(root)), rt_(std::make_unique<detail::Runtime>()) {}
+    Model(Model&&) = default;
+    Model& operator=(Model&&) = default;
+
+    template <class T, class... A>
+    void add_subsystem(const SubsystemDesc<T, A...>& d) { root_->add_subsystem(d); }
+    template <class D, class = decltype(std::declval<const D&>().build())>
+    void add_subsystem(const D& d) { root_->add_subsystem(d); }
+
+    void setup() {
+        if (setup_done_) return;
+        root_->setup();
+        setup_done_ = true;
+    }
+    void update_input(const std::string& path, InitSpec init) {
+        finalize();
+        detail::Var& v = rt_->var_of_path(root_.get(), path);
+        if (v.produced)
+            throw std::invalid_argument("naga::cospan: update_input('" + path + "'): the variable is an output of a component");
+        v.init = std::move(init);
+        v.stale = true;
+        if (!v.hook.empty() || v.spec.empty()) v.shape_known = false;
+    }
+    void run() {
+        finalize();
+        auto& rt = *rt_;
+        for (std::size_t i = 0; i < rt.leaves.size(); ++i) {
+            const int pat = rt.pattern_at.empty() ? -1 : rt.pattern_at[i];
+            if (pat == -2) continue;
+            if (pat >= 0) {
+                std::size_t next = i;
+                if (rt.pattern_runs[std::size_t(pat)](rt, next)) continue;
+            }
+            Node* n = rt.leaves[i];
+            if (n->kind == Node::Kind::component) rt.run_component(static_cast<ComponentBase*>(n));
+            else static_cast<FusedGroupBase*>(n)->launch(rt);
+        }
+        for (auto& v : rt.views) push(*v);
+    }
+    void wait() {
+        detail::cuda_check(cudaStreamSynchronize(rt_->stream), "wait");
+        std::uint32_t status = 0;
+        detail::cuda_check(cudaMemcpy(&status, rt_->ctrl, 4, cudaMemcpyDeviceToHost), "status");
+        if (status != 0) {
+            cudaMemset(rt_->ctrl, 0, 256);
+            throw std::runtime_error("naga::cospan: a device-side wait gave up (status " + std::to_string(status) + ")");
+        }
+    }
+    template <DType DT, int R>
+    HostView<DT, R> view_output(const std::string& path) {
+        finalize();
+        detail::Var& v = rt_->var_of_path(root_.get(), path);
+        if (v.rank != R || !dtype_compatible(v.dtype, DT))
+            throw std::invalid_argument("naga::cospan: view_output('" + path + "'): the variable is " +
+                                        std::string(dtype_name(v.dtype)) + " of rank " + std::to_string(v.rank));
+        auto s = std::make_shared<detail::ViewState>();
+        s->var = v.id;
+        rt_->views.push_back(s);
+        push(*s);
+        return HostView<DT, R>(s);
+    }
+    System& root() { return *root_; }
+    detail::Runtime& runtime() { return *rt_; }
+    /// device bytes held by the model's variables (Model::memory_report's total)
+    std::size_t memory_bytes() const {
+        std::size_t b = 0;
+        for (auto& v : rt_->vars) b += v.capacity;
+        return b;
+    }
+
+private:
+    std::unique_ptr<System> root_;
+    std::unique_ptr<detail::Runtime> rt_;
+    bool setup_done_ = false, finalized_ = false;
+
+    void push(detail::ViewState& s) {
+        detail::Var& v = rt_->vars[s.var];
+        if (!v.data) return;
+        const std::size_t b = v.bytes();
+        if (b != s.bytes) {
+            if (s.host) cudaFreeHost(s.host);
+            detail::cuda_check(cudaMallocHost(&s.host, std::max<std::size_t>(b, 16)), "host view");
+            s.bytes = b;
+        }
+        s.shape = v.shape;
+        if (!s.ev) detail::cuda_check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "view event");
+        detail::cuda_check(cudaMemcpyAsync(s.host, v.data, b, cudaMemcpyDeviceToHost, rt_->stream), "view push");
+        detail::cuda_check(cudaEventRecord(s.ev, rt_->stream), "view event");
+    }
+
+    void finalize();
+};
+
+template <class T, class... Args>
+Model create_model(Args&&... args) {
+    auto root = std::make_unique<T>(std::forward<Args>(args)...);
+    root->name = "";
+    return Model(std::move(root));
+}
+
+}  // namespace naga::cospan

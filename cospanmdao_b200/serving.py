@@ -2,9 +2,13 @@
 
 Requests arrive over time (a Poisson process, or all at once for saturation). Each names a MODEL — a GEMVER matrix A
 of size n, or an NS state (u, v, p) on an N×N grid — and brings its own small inputs (a GEMVER's six vectors; an NS
-evaluation needs none). Models stay resident on the device, in BF16 storage, under an HBM budget: a model is loaded
-(generated on the device) on first use and evicted least-recently-used when the budget needs room and no in-flight
-batch uses it.
+evaluation needs none). Models stay resident on the device under an HBM budget: a model is loaded (generated on the
+device) on first use and evicted least-recently-used when the budget needs room and no in-flight batch uses it.
+
+Storage precision per kind: GEMVER matrices in BF16 (x and w stay within 2e-4 of f64: the row and column sums average
+the rounding out), NS fields in FP32. BF16 fields cannot carry a finite-difference residual: neighbouring cells
+differ by about h·|∂f| ≈ 1e-3·|f| on these grids, below BF16's resolution (2^-8 relative), and the measured residual
+error against f64 is of order 1 (0.6 to 1.4 on the 4096² fields).
 
 The loop admits requests as they arrive: whenever one of `depth` launch slots (a stream each) is free and requests are
 waiting, it takes up to `max_batch` of them in arrival order — requests that arrived while earlier batches are still
@@ -120,9 +124,11 @@ class Model:
 class ModelStore:
     """Device-resident models under a byte budget, loaded on first use, evicted least-recently-used."""
 
-    def __init__(self, wl: Workload, *, dtype, budget_bytes: float, device, h_of=lambda N: 2 * math.pi / N):
+    def __init__(self, wl: Workload, *, dtype, budget_bytes: float, device, ns_dtype=None,
+                 h_of=lambda N: 2 * math.pi / N):
         self.wl = wl
         self.dtype = dtype
+        self.ns_dtype = ns_dtype or _torch().float32
         self.budget = float(budget_bytes)
         self.device = device
         self.models: dict[int, Model] = {}
@@ -134,7 +140,8 @@ class ModelStore:
 
     def bytes_of(self, mid: int) -> int:
         kind, size = self.wl.model_size[mid]
-        es = 2 if self.dtype == _torch().bfloat16 else 4
+        dt = self.dtype if kind == KIND_GEMVER else self.ns_dtype
+        es = 2 if dt == _torch().bfloat16 else 4
         return size * size * es * (1 if kind == KIND_GEMVER else 3)
 
     def _load(self, mid: int) -> Model:
@@ -147,7 +154,7 @@ class ModelStore:
             cb.fill_hash(A, 16 * (1000 + mid) + 1, 0)
             t = {"A": A}
         else:
-            u, v, p, h = workloads.ns_fields(size, seed=1000 + mid, dtype=self.dtype, device=self.device)
+            u, v, p, h = workloads.ns_fields(size, seed=1000 + mid, dtype=self.ns_dtype, device=self.device)
             t = {"u": u, "v": v, "p": p, "h": h}
         self.loads += 1
         return Model(mid, kind, size, t, self.bytes_of(mid))
@@ -289,7 +296,7 @@ class Server:
                 t["rv"] = base + 4 * (ns_cells + coff)
                 t["rc"] = base + 4 * (2 * ns_cells + coff)
                 t["norms"] = int(slot.dev_norm.data_ptr()) + 8 * 3 * (ni - lo)
-                slot.runner_n.ns(t, bf16=self.dtype == torch.bfloat16, stream=s, host_staging=slot.stage_n)
+                slot.runner_n.ns(t, bf16=self.store.ns_dtype == torch.bfloat16, stream=s, host_staging=slot.stage_n)
             if o1 > o0:
                 self.out[o0:o1].copy_(slot.dev_out[:o1 - o0], non_blocking=True)
             self.norms[lo:hi].view(-1).copy_(slot.dev_norm[:3 * (hi - lo)], non_blocking=True)
