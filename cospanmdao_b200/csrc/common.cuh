@@ -148,6 +148,13 @@ __device__ __forceinline__ uint4 ld_stream_u4(const void* p) {
         : "l"(p), "l"(evict_first_policy()));
     return v;
 }
+__device__ __forceinline__ uint2 ld_stream_u2(const void* p) {
+    uint2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+        : "=r"(v.x), "=r"(v.y)
+        : "l"(p), "l"(evict_first_policy()));
+    return v;
+}
 // Coherent loads through L2 (data written earlier in the same kernel by other blocks).
 __device__ __forceinline__ float4 ld_cg_f4(const float* p) {
     float4 v;

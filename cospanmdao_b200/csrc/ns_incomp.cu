@@ -11,7 +11,7 @@
 // formula is the workload's definition, and the oracle is an f64 restatement of it.
 //
 // Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. Work item = one warp on a strip of 32·VEC columns × H rows:
-// each lane owns VEC consecutive cells of a row (one 16-byte load per field per row), x-neighbours come from the
+// each lane owns 4 consecutive cells of a row (one 16-byte f32 / 8-byte bf16 load per field per row), x-neighbours come from the
 // adjacent lanes by shuffle (the warp's edge lanes load one wrapped scalar), and the warp marches down its rows
 // keeping the rows above and below in registers, two rows of loads in flight. Each input is read from HBM once (the
 // 2 halo rows of a strip are L2 hits of the neighbouring strip); 24 B/cell in f32 storage, 18 B/cell in bf16.
@@ -57,11 +57,10 @@ __device__ __forceinline__ void load_cells(const T* f, int64_t rowoff, int c0, i
             out[0] = q.x; out[1] = q.y; out[2] = q.z; out[3] = q.w;
             return;
         }
-    } else if constexpr (VEC == 8 && sizeof(T) == 2) {
-        if (ncols == 8) {
-            const uint4 q = ld_stream_u4(f + rowoff + c0);
+    } else if constexpr (VEC == 4 && sizeof(T) == 2) {
+        if (ncols == 4) {
+            const uint2 q = ld_stream_u2(f + rowoff + c0);
             out[0] = bf16_lo(q.x); out[1] = bf16_hi(q.x); out[2] = bf16_lo(q.y); out[3] = bf16_hi(q.y);
-            out[4] = bf16_lo(q.z); out[5] = bf16_hi(q.z); out[6] = bf16_lo(q.w); out[7] = bf16_hi(q.w);
             return;
         }
     }
@@ -243,7 +242,7 @@ __global__ void k_nsi_plan(NsiTasksK g) {
         const cspb_ns_incomp_task& t = g.tasks[k];
         uint64_t nb = 0;
         if (t.nx >= 3 && t.ny >= 3 && t.u && t.v && t.p && t.ru && t.rv && t.rc) {
-            const int vfast = g.bf16 ? 8 : 4;
+            const int vfast = 4;
             int H, segs;
             int64_t items, blocks;
             nsi_shape(t.nx, t.ny, nsi_fast(t, vfast) ? vfast : 1, H, segs, items, blocks);
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
         return;
     }
     const uint64_t total = __ldcg(g.boff + g.count);
-    constexpr int vfast = sizeof(T) == 2 ? 8 : 4;
+    constexpr int vfast = 4;
     for (;;) {
         const uint32_t v = grab_work(g.ctrl, kWork0);
         if (uint64_t(v) >= total) break;
@@ -360,7 +359,7 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     if (d->dtype != CSPB_F32 && d->dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
     if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->dtype == CSPB_BF16;
-    const int vfast = bf16 ? 8 : 4;
+    const int vfast = 4;  // 4 cells per lane: 16-byte loads in f32, 8-byte loads in bf16
     const bool in_al = aligned(d->u, 16) && aligned(d->v, 16) && aligned(d->p, 16);
     const bool out_al = aligned(d->ru, 16) && aligned(d->rv, 16) && aligned(d->rc, 16);
     const bool fast = in_al && out_al && d->nx % vfast == 0;
@@ -384,7 +383,7 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     g.part = reinterpret_cast<double*>(static_cast<char*>(d->workspace) + kCtrlBytes);
     const dim3 grid(unsigned(P.blocks)), block(kNsiThreads);
     if (bf16) {
-        if (fast) k_ns_incomp<__nv_bfloat16, 8><<<grid, block, 0, st>>>(g);
+        if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
     } else {
         if (fast) k_ns_incomp<float, 4><<<grid, block, 0, st>>>(g);

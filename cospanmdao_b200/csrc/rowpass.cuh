@@ -20,7 +20,7 @@ namespace cspb {
 
 template <typename T> struct VecOf;
 template <> struct VecOf<float> { static constexpr int N = 4; static constexpr int RB = 8; };
-template <> struct VecOf<__nv_bfloat16> { static constexpr int N = 8; static constexpr int RB = 4; };
+template <> struct VecOf<__nv_bfloat16> { static constexpr int N = 8; static constexpr int RB = 8; };
 
 constexpr int kPassThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
@@ -71,45 +71,44 @@ __device__ __forceinline__ float transpose_reduce32(float (&v)[32]) {
     return v[0];
 }
 
-// One lane's VEC elements of a row. NC: the matrix is read-only for the whole kernel (an input), so the
-// non-coherent path with evict-first is allowed; otherwise (a matrix written earlier in the same kernel) the load
-// goes through L2 coherently.
+// One lane's VEC elements of a row as ONE raw 16-byte vector (4 f32 or 8 bf16), so that a batch of rows in flight
+// costs 4 registers per row whatever the dtype; unpack() turns it into floats when the row is used. NC: the matrix is
+// read-only for the whole kernel (an input), so the non-coherent path with evict-first is allowed; otherwise (a
+// matrix written earlier in the same kernel) the load goes through L2 coherently. Lanes at the matrix edge (or rows
+// that are not 16-byte aligned) load element by element into the same raw layout, zero-filled.
 template <typename T, bool NC>
-__device__ __forceinline__ void load_vec(const T* row, int64_t c0, int ncols, bool vec_ok, float (&out)[VecOf<T>::N]);
-
-template <>
-__device__ __forceinline__ void load_vec<float, true>(const float* row, int64_t c0, int ncols, bool vec_ok, float (&out)[4]) {
-    if (vec_ok && ncols == 4) {
-        const float4 v = ld_stream_f4(row + c0);
-        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
-    } else {
-#pragma unroll
-        for (int e = 0; e < 4; ++e) out[e] = e < ncols ? __ldg(row + c0 + e) : 0.0f;
+__device__ __forceinline__ uint4 load_raw(const T* row, int64_t c0, int ncols, bool vec_ok) {
+    constexpr int VEC = VecOf<T>::N;
+    if (vec_ok && ncols == VEC) {
+        if constexpr (NC) return ld_stream_u4(row + c0);
+        else {
+            const float4 f = ld_cg_f4(reinterpret_cast<const float*>(row + c0));
+            return make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z), __float_as_uint(f.w));
+        }
     }
-}
-template <>
-__device__ __forceinline__ void load_vec<float, false>(const float* row, int64_t c0, int ncols, bool vec_ok, float (&out)[4]) {
-    if (vec_ok && ncols == 4) {
-        const float4 v = ld_cg_f4(row + c0);
-        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
-    } else {
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) out[e] = e < ncols ? __ldcg(row + c0 + e) : 0.0f;
+        for (int e = 0; e < 4; ++e)
+            if (e < ncols) w[e] = __float_as_uint(NC ? __ldg(reinterpret_cast<const float*>(row) + c0 + e)
+                                                     : __ldcg(reinterpret_cast<const float*>(row) + c0 + e));
+    } else {
+        const unsigned short* h = reinterpret_cast<const unsigned short*>(row) + c0;
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            if (e < ncols) w[e >> 1] |= uint32_t(h[e]) << (16 * (e & 1));
     }
+    return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-template <>
-__device__ __forceinline__ void load_vec<__nv_bfloat16, true>(const __nv_bfloat16* row, int64_t c0, int ncols, bool vec_ok,
-                                                              float (&out)[8]) {
-    if (vec_ok && ncols == 8) {
-        const uint4 v = ld_stream_u4(row + c0);
-        out[0] = bf16_lo(v.x); out[1] = bf16_hi(v.x);
-        out[2] = bf16_lo(v.y); out[3] = bf16_hi(v.y);
-        out[4] = bf16_lo(v.z); out[5] = bf16_hi(v.z);
-        out[6] = bf16_lo(v.w); out[7] = bf16_hi(v.w);
+template <typename T>
+__device__ __forceinline__ void unpack(const uint4& v, float (&out)[VecOf<T>::N]) {
+    if constexpr (sizeof(T) == 4) {
+        out[0] = __uint_as_float(v.x); out[1] = __uint_as_float(v.y);
+        out[2] = __uint_as_float(v.z); out[3] = __uint_as_float(v.w);
     } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) out[e] = e < ncols ? __bfloat162float(row[c0 + e]) : 0.0f;
+        out[0] = bf16_lo(v.x); out[1] = bf16_hi(v.x); out[2] = bf16_lo(v.y); out[3] = bf16_hi(v.y);
+        out[4] = bf16_lo(v.z); out[5] = bf16_hi(v.z); out[6] = bf16_lo(v.w); out[7] = bf16_hi(v.w);
     }
 }
 
@@ -178,15 +177,11 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
 #pragma unroll
     for (int kb = 0; kb < 32; kb += RB) {
         if (kb < nrows) {  // warp-uniform
-            float val[RB][VEC];
+            uint4 raw[RB];
 #pragma unroll
-            for (int k = 0; k < RB; ++k) {
-                if (kb + k < nrows && ncols > 0) load_vec<LT, NC>(src + (r0 + kb + k) * a.lds, c0, ncols, vec_ok, val[k]);
-                else {
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) val[k][e] = 0.f;
-                }
-            }
+            for (int k = 0; k < RB; ++k)
+                raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<LT, NC>(src + (r0 + kb + k) * a.lds, c0, ncols, vec_ok)
+                                                       : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
             for (int k = 0; k < RB; ++k) {
                 const int kk = kb + k;
@@ -195,15 +190,17 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
                 const float cyak = __shfl_sync(kFull, cyar, kk);
                 const float cybk = __shfl_sync(kFull, cybr, kk);
                 if (kk < nrows) {
+                    float val[VEC];
+                    unpack<LT>(raw[k], val);
                     float b[VEC];
 #pragma unroll
                     for (int e = 0; e < VEC; ++e)
-                        b[e] = RANK2 ? __fadd_rn(__fadd_rn(val[k][e], __fmul_rn(u1k, v1c[e])), __fmul_rn(u2k, v2c[e]))
-                                     : val[k][e];
+                        b[e] = RANK2 ? __fadd_rn(__fadd_rn(val[e], __fmul_rn(u1k, v1c[e])), __fmul_rn(u2k, v2c[e]))
+                                     : val[e];
                     if (store && ncols > 0) store_vec<VEC>(a.dst + (r0 + kk) * a.ldd, c0, ncols, vec_ok, b);
                     if (CSA) {
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) accA[e] = __fma_rn(double(val[k][e]), double(cyak), accA[e]);
+                        for (int e = 0; e < VEC; ++e) accA[e] = __fma_rn(double(val[e]), double(cyak), accA[e]);
                     }
                     if (CSB) {
 #pragma unroll

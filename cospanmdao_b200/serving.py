@@ -337,9 +337,14 @@ class Server:
                 lim = min(N, i + self.max_batch)
                 while j < lim and wl.arrival[j] <= now:
                     j += 1
-                if not self.store.acquire(wl.model[i:j]):
-                    if not busy:
-                        raise RuntimeError("the HBM budget cannot hold the models of one batch")
+                while not self.store.acquire(wl.model[i:j]):
+                    if busy:
+                        j = i  # wait for in-flight batches to release models
+                        break
+                    if j - i == 1:
+                        raise RuntimeError("the HBM budget cannot hold the model of one request")
+                    j = i + (j - i) // 2  # admit fewer requests whose models fit
+                if j == i:
                     continue
                 sl = free.popleft()
                 self._launch(sl, i, j)
