@@ -20,6 +20,8 @@ from .annotate import annotate_tree
 from .build import ARCH, nvcc
 
 PKG = Path(__file__).resolve().parent
+# a host-only function called from device code (nvcc's diagnostic 20011) would run nothing on the GPU: make it an error
+STRICT = ["--diag-error=20011,20014"]
 OUT = PKG / "_examples"
 PROGRAMS = {
     "gemver-chain": ("examples/gemver-chain", "main.cpp"),
@@ -39,7 +41,7 @@ def build_examples(reference: str | os.PathLike | None = None, verbose: bool = F
         annotate_tree(ref / sub, src)
         exe = OUT / name
         cmd = [nvcc(), "-std=c++20", "-O2", *ARCH, "-I", str(PKG / "include"), "--extended-lambda",
-               "--expt-relaxed-constexpr", "-x", "cu", str(src / main), "-o", str(exe)]
+               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src / main), "-o", str(exe)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((name, exe, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
@@ -55,12 +57,33 @@ def build_examples(reference: str | os.PathLike | None = None, verbose: bool = F
     return built
 
 
+RUNTIME_TESTS = {"runtime-fused-groups": "fused_groups.cu"}
+
+
+def build_runtime_tests(verbose: bool = False) -> dict[str, Path]:
+    """The runtime's own test programs (tests/runtime/*.cu, written against the cs:: API) -> cospanmdao_b200/_examples/."""
+    src_dir = PKG.parent / "tests" / "runtime"
+    OUT.mkdir(parents=True, exist_ok=True)
+    built = {}
+    for name, src in RUNTIME_TESTS.items():
+        exe = OUT / name
+        cmd = [nvcc(), "-std=c++20", "-O2", *ARCH, "-I", str(PKG / "include"), "--extended-lambda",
+               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src_dir / src), "-o", str(exe)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"building {name} failed: {' '.join(cmd)}\n{r.stdout}")
+        built[name] = exe
+    return built
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default=None)
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args(argv)
-    for k, v in build_examples(a.reference, a.verbose).items():
+    for k, v in {**build_runtime_tests(a.verbose), **build_examples(a.reference, a.verbose)}.items():
         print(k, v)
     return 0
 

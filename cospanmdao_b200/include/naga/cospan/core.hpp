@@ -307,8 +307,37 @@ struct LocalArray {
     static constexpr int rank = Rank;
 };
 
+/// LocalViews<V...>: what LocalMem::get returns, the views in declaration order. A tuple-like type of its own (std::tuple
+/// is host-only code under nvcc) that structured bindings unpack: auto [a, b] = lm.get(it).
+namespace detail {
+template <std::size_t I, class T>
+struct ViewSlot {
+    T v;
+};
+template <class Seq, class... V> struct ViewPack;
+template <std::size_t... I, class... V>
+struct ViewPack<std::index_sequence<I...>, V...> : ViewSlot<I, V>... {
+    CS_HD explicit ViewPack(V... v) : ViewSlot<I, V>{v}... {}
+};
+template <std::size_t I, class T>
+CS_HD T& slot_ref(ViewSlot<I, T>& s) { return s.v; }
+template <std::size_t I, class T>
+CS_HD const T& slot_cref(const ViewSlot<I, T>& s) { return s.v; }
+}  // namespace detail
+
+template <class... V>
+struct LocalViews : detail::ViewPack<std::index_sequence_for<V...>, V...> {
+    CS_HD explicit LocalViews(V... v) : detail::ViewPack<std::index_sequence_for<V...>, V...>(v...) {}
+    template <std::size_t I> CS_HD auto& get() & { return detail::slot_ref<I>(*this); }
+    template <std::size_t I> CS_HD const auto& get() const& { return detail::slot_cref<I>(*this); }
+    template <std::size_t I> CS_HD auto&& get() && {
+        auto& r = detail::slot_ref<I>(*this);
+        return static_cast<std::remove_reference_t<decltype(r)>&&>(r);
+    }
+};
+
 /// LocalMem<Arrays...>: a group-range stage's local memory (kernel.hpp:515-570). get(it) returns the views of its
-/// arrays, in declaration order (a tuple, for structured bindings). The runtime fills base and shapes.
+/// arrays, in declaration order (LocalViews, for structured bindings). The runtime fills base and shapes.
 template <class... Arrays>
 struct LocalMem {
     unsigned char* base = nullptr;
@@ -320,8 +349,8 @@ struct LocalMem {
 
 private:
     template <std::size_t... I>
-    CS_HD auto views(std::index_sequence<I...>) const {
-        return std::make_tuple(view<Arrays>(I)...);
+    CS_HD LocalViews<typename Arrays::view_type...> views(std::index_sequence<I...>) const {
+        return LocalViews<typename Arrays::view_type...>(view<Arrays>(I)...);
     }
     template <class A>
     CS_HD typename A::view_type view(std::size_t i) const {
@@ -394,3 +423,10 @@ using CustomFn = std::function<sycl::event(sk::unordered_queue&, const sycl::dev
                                            Initializer<DT, Rank>)>;
 
 }  // namespace naga::cospan
+
+template <class... V>
+struct std::tuple_size<naga::cospan::LocalViews<V...>> : std::integral_constant<std::size_t, sizeof...(V)> {};
+template <std::size_t I, class... V>
+struct std::tuple_element<I, naga::cospan::LocalViews<V...>> {
+    using type = std::tuple_element_t<I, std::tuple<V...>>;
+};

@@ -12,6 +12,8 @@
 // (patterns.hpp); every other leaf runs its own component bodies (component.hpp, system.hpp).
 #pragma once
 
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <numeric>
 #include <set>
@@ -84,8 +86,10 @@ public:
     std::vector<int> pattern_at;             // leaf index -> pattern index or -1 (-2: covered, skip)
     std::vector<struct PatternRec*> pattern_recs;
     int sms = 0;
+    bool trace = false;  // NAGA_COSPAN_TRACE set: every launch and initializer is printed to stderr
 
     Runtime() {
+        trace = std::getenv("NAGA_COSPAN_TRACE") != nullptr;
         cuda_check(cudaGetDevice(&device), "cudaGetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
         cuda_check(cudaMalloc(&ctrl, 256), "control block");
@@ -173,6 +177,8 @@ public:
             InitTarget t{*this, v};
             v.init->run(t);
             v.stale = false;
+            if (trace) std::fprintf(stderr, "[cospan] init var %d '%s' at %p (%zu elements)\n", v.id, v.name.c_str(), v.data,
+                                    v.elements());
         }
     }
 
@@ -232,8 +238,21 @@ public:
             p.bind(v.data, v.shape.data());
         }
     }
+    void trace_ports(ComponentBase* c) {
+        for (auto& p : c->ports_) {
+            const Var& v = vars[p.var];
+            std::fprintf(stderr, "[cospan]   %s %-8s var %3d %-28s %p shape", p.output ? "out" : "in ", p.name.c_str(), v.id,
+                         v.name.c_str(), v.data);
+            for (int d = 0; d < v.rank; ++d) std::fprintf(stderr, " %zu", v.shape[d]);
+            std::fprintf(stderr, "\n");
+        }
+    }
     void run_component(ComponentBase* c) {
         prepare(c);
+        if (trace) {
+            std::fprintf(stderr, "[cospan] launch '%s'\n", c->path().c_str());
+            trace_ports(c);
+        }
         std::unique_ptr<LaunchDescription> d = c->define_forward();
         if (d) c->launch_solo(*this, *d);
     }
@@ -518,6 +537,17 @@ void FusedGroup<Opts, Items...>::launch(detail::Runtime& rt) {
     for (int s = 0; s < nseg; ++s) most = std::max(most, p.seg[s].count);
     if (most == 0 || threads == 0) return;
     const void* kern = FP::kernel();
+    if (rt.trace) {
+        std::fprintf(stderr, "[cospan] fused '%s': %d segments, %zu threads, %zu B local memory\n", path().c_str(), nseg,
+                     threads, smem);
+        for (std::size_t i = 0; i < stages_.size(); ++i) {
+            const detail::StageGeom& g = p.st[i];
+            std::fprintf(stderr, "[cospan]  stage '%s' segment %u %s count %llu groups %zu %zu %zu local %zu %zu %zu base %u\n",
+                         stages_[i]->path().c_str(), g.segment, g.whole ? "whole" : "own", (unsigned long long)g.count,
+                         g.groups[0], g.groups[1], g.groups[2], g.local[0], g.local[1], g.local[2], g.local_mem.base);
+            rt.trace_ports(stages_[i]);
+        }
+    }
     if (smem > 48 * 1024)
         detail::cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), path());
     int per_sm = 0;
@@ -532,6 +562,13 @@ void FusedGroup<Opts, Items...>::launch(detail::Runtime& rt) {
     else
         detail::cuda_check(cudaLaunchKernel(kern, dim3(grid), dim3(unsigned(threads)), args, smem, rt.stream),
                            "launching '" + path() + "'");
+    if (rt.trace) {
+        const cudaError_t e = cudaStreamSynchronize(rt.stream);
+        std::uint32_t st[3] = {0, 0, 0};
+        cudaMemcpy(st, rt.ctrl, sizeof(st), cudaMemcpyDeviceToHost);
+        std::fprintf(stderr, "[cospan] fused '%s': grid %u (%d per SM), sync %s, status %u barrier %u/%u\n", path().c_str(),
+                     grid, per_sm, cudaGetErrorString(e), st[0], st[1], st[2]);
+    }
 }
 
 // ---- host views (host_view.hpp:103-152) ------------------------------------------------------------------------------

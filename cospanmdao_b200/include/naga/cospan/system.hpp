@@ -343,15 +343,31 @@ FusedBuilder<Opts, Items...> make_fused(std::string name, ConnectsDesc c, TiesDe
 }
 }  // namespace detail
 
+namespace detail {
+template <class... Items> inline constexpr bool leads_with_connects_v = false;
+template <class I, class... R> inline constexpr bool leads_with_connects_v<I, R...> = std::is_same_v<I, ConnectsDesc>;
+template <class... Items> inline constexpr bool leads_with_ties_v = false;
+template <class I, class... R> inline constexpr bool leads_with_ties_v<I, R...> = std::is_same_v<I, TiesDesc>;
+}  // namespace detail
+
+/// fuse_components[<options>](name, [connects_desc(...)], [ties_desc(...)], items...): both descriptions are optional,
+/// connects first (fused_component.hpp:524-569).
 template <class... Opts, class... Items>
 auto fuse_components(std::string name, ConnectsDesc c, TiesDesc t, Items... items) {
     return detail::make_fused<std::tuple<Opts...>>(std::move(name), std::move(c), std::move(t), std::move(items)...);
 }
 template <class... Opts, class... Items>
+    requires(!detail::leads_with_ties_v<Items...>)
 auto fuse_components(std::string name, ConnectsDesc c, Items... items) {
     return detail::make_fused<std::tuple<Opts...>>(std::move(name), std::move(c), TiesDesc{}, std::move(items)...);
 }
 template <class... Opts, class... Items>
+    requires(!detail::leads_with_connects_v<Items...>)
+auto fuse_components(std::string name, TiesDesc t, Items... items) {
+    return detail::make_fused<std::tuple<Opts...>>(std::move(name), ConnectsDesc{}, std::move(t), std::move(items)...);
+}
+template <class... Opts, class... Items>
+    requires(sizeof...(Items) >= 1 && !detail::leads_with_connects_v<Items...> && !detail::leads_with_ties_v<Items...>)
 auto fuse_components(std::string name, Items... items) {
     return detail::make_fused<std::tuple<Opts...>>(std::move(name), ConnectsDesc{}, TiesDesc{}, std::move(items)...);
 }

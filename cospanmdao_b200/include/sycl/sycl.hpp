@@ -29,7 +29,7 @@ namespace sycl {
 template <int R>
 struct range {
     std::size_t v[R > 0 ? R : 1] = {};
-    CS_HD range() = default;
+    range() = default;
     template <class... I, class = std::enable_if_t<sizeof...(I) == R && (std::is_integral_v<I> && ...)>>
     CS_HD range(I... i) : v{static_cast<std::size_t>(i)...} {}
     CS_HD std::size_t& operator[](int d) { return v[d]; }
@@ -51,7 +51,7 @@ struct range {
 template <int R>
 struct id {
     std::size_t v[R > 0 ? R : 1] = {};
-    CS_HD id() = default;
+    id() = default;
     template <class... I, class = std::enable_if_t<sizeof...(I) == R && (std::is_integral_v<I> && ...)>>
     CS_HD id(I... i) : v{static_cast<std::size_t>(i)...} {}
     CS_HD std::size_t& operator[](int d) { return v[d]; }

@@ -21,6 +21,13 @@ def _run(args, timeout=300):
     return r.returncode, r.stdout
 
 
+def test_runtime_fused_groups(cuda):
+    """The runtime's own fused-group cases (tests/runtime/fused_groups.cu): shared and partitioned local memory, a tie
+    declared by the group, a stage without local memory in a launch that has some."""
+    rc, out = _run(["runtime-fused-groups"])
+    assert rc == 0 and "ALL OK" in out, out
+
+
 def test_getting_started(cuda):
     rc, out = _run(["getting-started"])
     assert rc == 0, out
