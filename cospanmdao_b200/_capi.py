@@ -23,6 +23,7 @@ ERR_EXCEEDS32 = 6
 ERR_UNSUPPORTED = 7
 ERR_CUDA = 8
 ERR_CAPACITY = 9
+ERR_TOO_LARGE = 10
 
 DEV_TIMEOUT = 1
 DEV_NEGATIVE = 2
@@ -116,6 +117,7 @@ PROTOTYPES = {
     "cspb_exclusive_scan_u32": (C.c_int, [vp, vp, i64, vp, sz, vp]),
     "cspb_exclusive_scan_u64": (C.c_int, [vp, vp, i64, vp, sz, vp]),
     "cspb_build_column": (C.c_int, [vp, i32, i64, i64, i32, vp, vp, vp, vp, sz, vp]),
+    "cspb_build_column_static": (C.c_int, [vp, i32, i64, i64, i32, vp, vp, vp, vp]),
     "cspb_fill_hash": (C.c_int, [vp, i32, i64, u64, u32, i32, vp]),
 }
 

@@ -75,6 +75,7 @@ const char* cspb_status_string(int status) {
         case CSPB_ERR_UNSUPPORTED: return "unsupported dtype or option";
         case CSPB_ERR_CUDA: return "CUDA runtime error";
         case CSPB_ERR_CAPACITY: return "device-computed totals exceed the declared capacities";
+        case CSPB_ERR_TOO_LARGE: return "input larger than the fixed scratch allows (CSPB_BUILD_COLUMN_STATIC_MAX)";
         default: return "unknown status";
     }
 }

@@ -14,6 +14,8 @@
 // kernel: the narrowing of the source values (negative -> flag 1, past 32 bits -> flag 2) happens as the tile loads,
 // the running sum is carried in 64 bits so that a total past 2^32 - 1 is known exactly (the reference detects the same
 // thing as a decrease of the wrapped u32 offsets), and the last tile writes [total, flag].
+#include <mutex>
+
 #include "common.cuh"
 
 namespace cspb {
@@ -405,3 +407,47 @@ int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t
 }
 
 }  // extern "C"
+
+// ---- build_column on a fixed scratch ---------------------------------------------------------------------------------
+// The scratch of a u64 scan of CSPB_BUILD_COLUMN_STATIC_MAX items (scan_layout: control block, tile flags, tile
+// aggregates, tile prefixes; 2048 items per tile), as a file-scope device array: the call needs no workspace and
+// allocates nothing. run_scan / cspb_build_column zero the control block and the tile flags on every call.
+namespace {
+constexpr int64_t kStaticTiles = (int64_t(CSPB_BUILD_COLUMN_STATIC_MAX) + kScanThreads * ScanItems<uint64_t>::N - 1) /
+                                 (kScanThreads * ScanItems<uint64_t>::N);
+constexpr size_t kStaticScratchBytes =
+    kCtrlBytes + ((size_t(kStaticTiles) * 4 + 255) / 256 * 256) + 2 * ((size_t(kStaticTiles) * 8 + 255) / 256 * 256);
+static_assert(kStaticScratchBytes <= 160 * 1024 + 256, "the fixed scratch stays modest");
+
+static __device__ __align__(256) unsigned char g_column_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// The device address of g_column_scratch on the current device, looked up once per device.
+int column_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CSPB_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_column_scratch) != cudaSuccess || !p) return CSPB_ERR_CUDA;
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return CSPB_OK;
+}
+}  // namespace
+
+extern "C" int cspb_build_column_static(const void* src, int32_t src_dtype, int64_t count, int64_t k,
+                                        int32_t offsets_mode, uint32_t* extents, uint32_t* offs, uint32_t* total_flag,
+                                        void* stream) {
+    const int64_t n = offsets_mode ? count - 1 : count;
+    if (n > int64_t(CSPB_BUILD_COLUMN_STATIC_MAX)) return CSPB_ERR_TOO_LARGE;
+    void* scratch = nullptr;
+    const int rc = column_scratch(&scratch);
+    if (rc != CSPB_OK) return rc;
+    return cspb_build_column(src, src_dtype, count, k, offsets_mode, extents, offs, total_flag, scratch,
+                             kStaticScratchBytes, stream);
+}

@@ -36,7 +36,8 @@ enum {
     CSPB_ERR_EXCEEDS32 = 6,   /* device status: a ragged value or total is past 2^32 - 1 */
     CSPB_ERR_UNSUPPORTED = 7, /* a dtype / option combination this build does not provide */
     CSPB_ERR_CUDA = 8,        /* another CUDA runtime error (cudaMemsetAsync, cudaMemcpyAsync, ...) */
-    CSPB_ERR_CAPACITY = 9     /* device status: device-computed totals do not fit the capacities the caller declared */
+    CSPB_ERR_CAPACITY = 9,    /* device status: device-computed totals do not fit the capacities the caller declared */
+    CSPB_ERR_TOO_LARGE = 10   /* the input is larger than the fixed scratch of cspb_build_column_static allows */
 };
 
 /* bits of the device status word (the first 4 bytes of every workspace) */
@@ -318,6 +319,21 @@ int cspb_exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, void* 
 int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
                       uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* workspace,
                       size_t workspace_bytes, void* stream);
+
+/* ==================================================================================================================
+ * cspb_build_column_static: cspb_build_column with no workspace argument, for callers that cannot allocate device
+ * memory at the call site (a foreign-language binding that holds only the column's pointers and no allocator, code
+ * running where an allocation would stall or be refused). It allocates nothing: its scratch is a fixed 164,096-byte array
+ * in the library's device image (one per device), found once per device by the first call made with that device
+ * current; make that first call before any stream capture begins. Results are bit-identical to cspb_build_column.
+ * Limit: at most CSPB_BUILD_COLUMN_STATIC_MAX extents (count in counts mode, count - 1 in offsets mode); larger inputs
+ * return CSPB_ERR_TOO_LARGE before any device work. The scratch is shared by every call on a device, so calls on one
+ * device must not overlap in time (same stream, or ordered by events); overlapping calls race on it.
+ * No counterpart in the reference (its build_column allocates its temporaries on every call).
+ * ================================================================================================================== */
+#define CSPB_BUILD_COLUMN_STATIC_MAX (1 << 24)
+int cspb_build_column_static(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
+                             uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* stream);
 
 /* ==================================================================================================================
  * Seeded inputs on the device: the reference's generator gemver_chain::hash_unit (common/chain_data.hpp:34-49).
