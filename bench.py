@@ -484,6 +484,8 @@ def main(argv=None) -> int:
     ap.add_argument("--ragged", type=int, default=4096, help="instances of the ragged batch")
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving stream")
     ap.add_argument("--max-batch", type=int, default=512, help="serving: requests per batch at most")
+    ap.add_argument("--only", default="", help="comma list of secondary workloads to run (gemver_bf16_storage, "
+                    "gemver_chain, ns_residual, ragged_batch, serving); default all, none with --quick")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     dist = Dist()
@@ -534,14 +536,19 @@ def main(argv=None) -> int:
         "clocks": g["clocks"],
         "err_vs_f64": g["err"],
     }
-    if not args.quick:
-        sec = {}
-        sec["gemver_bf16_storage"] = bench_gemver_bf16(torch, cb, dist, args)
-        sec["gemver_chain"] = bench_chain(torch, cb, dist, args)
-        sec["ns_residual"] = bench_ns(torch, cb, dist, args)
-        sec["ragged_batch"] = bench_ragged(torch, cb, dist, args, pk)
-        sec["serving"] = bench_serving(torch, dist, args)
-        line["secondary"] = sec
+    secondaries = {
+        "gemver_bf16_storage": lambda: bench_gemver_bf16(torch, cb, dist, args),
+        "gemver_chain": lambda: bench_chain(torch, cb, dist, args),
+        "ns_residual": lambda: bench_ns(torch, cb, dist, args),
+        "ragged_batch": lambda: bench_ragged(torch, cb, dist, args, pk),
+        "serving": lambda: bench_serving(torch, dist, args),
+    }
+    wanted = [w for w in args.only.split(",") if w] or ([] if args.quick else list(secondaries))
+    unknown = [w for w in wanted if w not in secondaries]
+    if unknown:
+        raise SystemExit(f"bench.py: unknown workload(s) {unknown}; choose from {list(secondaries)}")
+    if wanted:
+        line["secondary"] = {w: secondaries[w]() for w in wanted}
     if dist.rank == 0 and not args.quick:
         line["cpu_baseline"] = cpu_gemver(args.n)
     if dist.rank == 0:
