@@ -68,35 +68,25 @@ def profile_traffic(name: str):
 
 # ---- distributed plumbing ----------------------------------------------------------------------------------------
 class Dist:
+    """One rank per GPU (cospanmdao_b200.replicas.Ranks): each rank runs its own replica of the workload, the step
+    time is the max over ranks, and no collective touches the data path."""
+
     def __init__(self):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
+        from cospanmdao_b200.replicas import Ranks
+        self.r = Ranks()
+        self.world, self.rank, self.local = self.r.world, self.r.rank, self.r.local
 
     def init(self, torch):
-        torch.cuda.set_device(self.local)
-        if self.world > 1:
-            import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = dist
+        self.r.init("nccl", timeout_s=120)
 
     def barrier(self, torch):
-        if self.pg:
-            self.pg.barrier()
-        torch.cuda.synchronize()
+        self.r.barrier()
 
     def max(self, torch, x: float) -> float:
-        if not self.pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
-        return float(t.item())
+        return self.r.max(x)
 
     def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
+        self.r.close()
 
 
 # ---- clocks -----------------------------------------------------------------------------------------------------
