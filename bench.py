@@ -468,7 +468,7 @@ def main(argv=None) -> int:
     ap.add_argument("--grid", type=int, default=4096)
     ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed steps before the timed region")
     ap.add_argument("--quick", action="store_true", help="headline only (no secondary workloads, no CPU baseline)")
-    ap.add_argument("--schedule", default="barrier", choices=["panel", "barrier"], help="GEMVER schedule")
+    ap.add_argument("--schedule", default="barrier", choices=["panel", "barrier", "bulk"], help="GEMVER schedule")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--lag", type=int, default=0, help="panel-schedule lag (0: automatic)")
     ap.add_argument("--ragged", type=int, default=4096, help="instances of the ragged batch")
@@ -519,8 +519,9 @@ def main(argv=None) -> int:
         "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": kernel_gbs / pk["hbm_gbs"], "peak_source": pk["source"],
                      "traffic": traffic, "algorithmic_bytes_per_launch": g["bytes"],
-                     "kernel": "cspb::k_gemver_panel<float, true>" if args.schedule == "panel"
-                     else "cspb::k_gemver<float, true>"},
+                     "kernel": {"panel": "cspb::k_gemver_panel<float, true>",
+                                "bulk": "cspb::k_gemver_bulk<float, true, 6>"}.get(args.schedule,
+                                                                                  "cspb::k_gemver<float, true>")},
         "e2e": g["e2e"],
         "gpu_launches": args.steps,
         "clocks": g["clocks"],

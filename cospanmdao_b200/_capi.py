@@ -33,6 +33,7 @@ DEV_CAPACITY = 8
 F32 = 0
 BF16 = 1
 GEMVER_PANEL = 1
+GEMVER_BULK = 2
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p

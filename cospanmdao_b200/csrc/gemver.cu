@@ -13,15 +13,23 @@
 // n = 16384 on B200 although it moves a third more bytes: the panel order reads 1 KB row segments of ~2 panels at
 // a time across every row, which HBM serves less efficiently than the strip order's whole rows.
 //   pass 1   read A, write Â, f64 column partials        | grid barrier, x = z + β·Σ partials, grid barrier
-//   pass 2   read Â (or A again), row dots with x, w;  walked from the last strip back (recently written Â in L2).
-// Both schedules produce bit-identical results (the same partials, combined in the same order).
+//   pass 2   read Â (or A again), row dot partials with x, walked from the last strip back (recently written Â in
+//            L2), 16 rows in flight per lane | grid barrier, w = α·Σ partials (rowsum_finish)
+// Deferring the row sums to a phase of their own keeps the fence, the atomic and the last block's sums off every
+// pass-2 unit (at n = 16384 pass 2 went from 4.3 to 5.5 TB/s); the sums run in the same order either way.
+// flags = CSPB_GEMVER_BULK runs the same three passes with the matrix streamed through a shared-memory ring by bulk
+// asynchronous copies (bulkpass.cuh). Measured at n = 16384 on B200 it is slower (0.87 vs 0.58 ms: pass 1 at
+// 4.3 TB/s and pass 2 at 3.1 TB/s against 6.0 and 5.5): one CTA per SM leaves 8 consumer warps where the register
+// pipeline runs 16, and the per-stage hand-off serialises them. It is kept as an option; results are the same bits.
+// All schedules produce bit-identical results (the same partials, combined in the same order).
 // BiCGK (one pass): q = B·p row dots and s = Bᵀ·r column partials from the same loads; one barrier; s.
 // Chain (G1 → BiCGK → G2, six passes — the reference's nominal traffic counts eight):
 //   1: A0 → B1 + x1 partials | 2: B1 → w1 = α·(B1·x1), q = B1·x1 (p = x1, so one dot gives both)
 //   3: B1 → s partials (with w1) + B2 + x2 partials (with q) | 4: B2 → w2.
 #include <cstdio>
+#include <initializer_list>
 
-#include "rowpass.cuh"
+#include "bulkpass.cuh"
 
 namespace cspb {
 
@@ -52,10 +60,59 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
         if (u >= g.units) break;
         const int64_t unit = g.units - 1 - int64_t(u);
         if constexpr (P2_FROM_B)
-            pass_unit<float, kWX, false, false, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+            pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, unit, vec_ok != 0, smem);
         else
-            pass_unit<T, kWX, true, true, false, false, true>(g.p2, unit, vec_ok != 0, smem);
+            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p2, unit, vec_ok != 0, smem);
     }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish(g.p2);
+}
+
+// The same three passes with the matrix streamed through a shared-memory ring by bulk copies (bulkpass.cuh): one
+// CTA per SM, 8 consumer warps and a producer warp; the results are bit-identical to k_gemver's.
+template <typename T, bool P2_FROM_B, int NST>
+__global__ void __launch_bounds__(kBulkThreads, 1) k_gemver_bulk(GemverK g) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    const Ring<T, NST> R{dsm};
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NST; ++i) {
+            mbar_init(R.full(i), 1);
+            mbar_init(R.empty(i), kPassThreads / 32);
+        }
+        R.verdict()[0] = 0;
+        R.verdict()[1] = 0;
+        *R.abort_flag() = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t q = 0;
+    const uint64_t first = evict_first_policy();
+    {
+        BulkPass P{g.p1, true, false, true, false, false, kWork0, g.units, first};
+        if (warp == kPassThreads / 32) {
+            if (!bulk_produce<T, NST>(R, P, g.ctrl, q)) bulk_drain<T, NST>(R, q, g.ctrl);
+        } else {
+            bulk_consume<T, NST, true, false, true, false>(R, g.p1, g.ctrl, q);
+        }
+    }
+    // pass 1's Â stores and the x of the finish are read by pass 2's bulk copies (the async proxy) in other CTAs
+    fence_proxy_async_global();
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
+    fence_proxy_async_global();
+    if (!grid_barrier(g.ctrl)) return;
+    fence_proxy_async_global();
+    {
+        BulkPass P{g.p2, !P2_FROM_B, false, false, true, true, kWork0 + 1, g.units, first};
+        if (warp == kPassThreads / 32) {
+            if (!bulk_produce<T, NST>(R, P, g.ctrl, q)) bulk_drain<T, NST>(R, q, g.ctrl);
+        } else {
+            bulk_consume<T, NST, !P2_FROM_B, false, false, true, true>(R, g.p2, g.ctrl, q);
+        }
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish(g.p2);
 }
 
 struct PanelK {
@@ -137,10 +194,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_bicgk(BicgkK g, int vec_ok)
     for (;;) {
         const uint32_t u = grab_work(g.ctrl, kWork0);
         if (u >= g.units) break;
-        pass_unit<T, kWX, true, false, false, true, true>(g.p, u, vec_ok != 0, smem);
+        pass_unit<T, kWX, true, false, false, true, true, 0, true>(g.p, u, vec_ok != 0, smem);
     }
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p.PB, g.p.strips, g.p.n, nullptr, 1.0f, g.s);
+    rowsum_finish(g.p);
 }
 
 struct ChainK {
@@ -168,8 +226,10 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain(ChainK g, int vec_ok)
     for (;;) {
         const uint32_t u = grab_work(g.ctrl, kWork0 + 1);
         if (u >= g.units) break;
-        pass_unit<float, kWX, false, false, false, false, true>(g.p2, g.units - 1 - int64_t(u), vo, smem);
+        pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, g.units - 1 - int64_t(u), vo, smem);
     }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish(g.p2);
     if (!grid_barrier(g.ctrl)) return;
     // 3: B1 -> partials of B1ᵀ·w1 (s); B2 = B1 + update; partials of B2ᵀ·q (x2)
     for (;;) {
@@ -185,8 +245,10 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain(ChainK g, int vec_ok)
     for (;;) {
         const uint32_t u = grab_work(g.ctrl, kWork0 + 3);
         if (u >= g.units) break;
-        pass_unit<float, kWX, false, false, false, false, true>(g.p4, g.units - 1 - int64_t(u), vo, smem);
+        pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p4, g.units - 1 - int64_t(u), vo, smem);
     }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish(g.p4);
 }
 
 }  // namespace cspb
@@ -267,6 +329,31 @@ int launch_persistent(K kernel, void** args, int64_t items, size_t zero_bytes, v
     return e == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
+template <typename K>
+int launch_coop_bulk(K kernel, void** args, size_t smem, size_t zero_bytes, void* ws, cudaStream_t st) {
+    const cspb_host::DeviceInfo di = cspb_host::device_info();
+    if (di.device < 0) return CSPB_ERR_CUDA;
+    if (!di.coop) return CSPB_ERR_UNSUPPORTED;
+    cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return cspb_host::map_cuda_error(e);
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBulkThreads, smem);
+    if (e != cudaSuccess || per_sm < 1) return e != cudaSuccess ? cspb_host::map_cuda_error(e) : CSPB_ERR_LAUNCH;
+    const int64_t grid = int64_t(per_sm) * di.sms;
+    e = cudaMemsetAsync(ws, 0, zero_bytes, st);
+    if (e != cudaSuccess) return cspb_host::map_cuda_error(e);
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(unsigned(grid)), dim3(kBulkThreads),
+                                    args, smem, st);
+    return e == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+bool aligned16(std::initializer_list<const void*> ps) {
+    for (const void* p : ps)
+        if (p && !aligned(p, 16)) return false;
+    return true;
+}
+
 bool vec_aligned(const void* p, int64_t ld, int elem_bytes) {
     return p == nullptr || (aligned(p, 16) && (ld * elem_bytes) % 16 == 0);
 }
@@ -287,7 +374,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
     if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if ((d->flags & ~(CSPB_GEMVER_PANEL | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
+    if ((d->flags & ~(CSPB_GEMVER_PANEL | CSPB_GEMVER_BULK | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->a_dtype == CSPB_BF16;
     const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
@@ -324,6 +411,25 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t zero = L.off_PA;  // ctrl, strip_done, chunk_done, x_ready
 
+    // the bulk-copy ring: every row segment and vector piece must start on 16 bytes and be a multiple of 16 bytes long
+    const int vw = bf16 ? 8 : 4;
+    const bool bulk_ok = vec_ok && n % vw == 0 && (d->lda * eb) % 16 == 0 && (!d->B || (d->ldb * 4) % 16 == 0) &&
+                         aligned16({d->A, d->B, d->u1, d->v1, d->u2, d->v2, d->y, d->x});
+    if ((d->flags & CSPB_GEMVER_BULK) && !(d->flags & CSPB_GEMVER_PANEL) && bulk_ok) {
+        GemverK g{};
+        g.p1 = p1;
+        g.p2 = p2;
+        g.ctrl = reinterpret_cast<uint32_t*>(ws);
+        g.units = L.units;
+        g.z = d->z;
+        g.beta = d->beta;
+        g.x = d->x;
+        void* args[] = {&g};
+        if (bf16) return launch_coop_bulk(k_gemver_bulk<__nv_bfloat16, false, 5>, args,
+                                          Ring<__nv_bfloat16, 5>::total, zero, ws, st);
+        if (from_B) return launch_coop_bulk(k_gemver_bulk<float, true, 6>, args, Ring<float, 6>::total, zero, ws, st);
+        return launch_coop_bulk(k_gemver_bulk<float, false, 6>, args, Ring<float, 6>::total, zero, ws, st);
+    }
     if (!(d->flags & CSPB_GEMVER_PANEL)) {
         GemverK g{};
         g.p1 = p1;

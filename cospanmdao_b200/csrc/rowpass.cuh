@@ -133,12 +133,102 @@ __host__ __device__ constexpr size_t pass_smem_bytes() {
     return cs > rd ? cs : rd;
 }
 
+// Synchronisation of the threads that run a unit's epilogue: the whole block (pass_unit) or, in a kernel with a
+// producer warp, the 256 consumer threads only (named barrier 1).
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct ConsumerSync {
+    __device__ __forceinline__ void operator()() const { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+};
+
+// The end of a unit, run by threads 0..255: column sums (the WY warps of a column combined in a fixed order, one f64
+// partial per (strip, column)) and row dots (warp tree, then the WX warps of a row in order; the last chunk of a strip
+// combines the chunks in order and writes the row results). Every order here depends on (n, S, CW) only.
+// DEFER: the row dots stop at the per-chunk partials (Wp); rowsum_finish combines them after a grid barrier, in the
+// same order, so the unit ends without a fence, an atomic and the last block's sums.
+template <typename LT, int WX, bool CSA, bool CSB, bool RDOT, typename Sync, bool DEFER = false>
+__device__ __forceinline__ void unit_epilogue(const PassArgs& a, int64_t strip, int64_t chunk,
+                                              const double (&accA)[VecOf<LT>::N], const double (&accB)[VecOf<LT>::N],
+                                              float (&racc)[32], unsigned char* smem, Sync sync) {
+    using G = PassGeo<LT, WX>;
+    constexpr int VEC = G::VEC, WY = G::WY, S = G::S, CW = G::CW;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wx = warp % WX, wy = warp / WX;
+    const int64_t n = a.n;
+    __shared__ int s_last;
+    if (CSA || CSB) {
+        double* red = reinterpret_cast<double*>(smem);
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            if ((which == 0 && !CSA) || (which == 1 && !CSB)) continue;
+            sync();
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) red[wy * CW + (wx * 32 + lane) * VEC + e] = which == 0 ? accA[e] : accB[e];
+            sync();
+            double* P = which == 0 ? a.PA : a.PB;
+            for (int t = threadIdx.x; t < CW; t += kPassThreads) {
+                const int64_t col = chunk * CW + t;
+                if (col < n) {
+                    double s = red[t];
+#pragma unroll
+                    for (int y = 1; y < WY; ++y) s += red[y * CW + t];
+                    P[strip * n + col] = s;
+                }
+            }
+        }
+    }
+    if (RDOT) {
+        const float v = transpose_reduce32(racc);
+        float* red2 = reinterpret_cast<float*>(smem);
+        sync();
+        red2[wx * S + wy * 32 + lane] = v;
+        sync();
+        for (int t = threadIdx.x; t < S; t += kPassThreads) {
+            const int64_t row = strip * S + t;
+            if (row < n) {
+                float s = red2[t];
+#pragma unroll
+                for (int x = 1; x < WX; ++x) s += red2[x * S + t];
+                a.Wp[chunk * n + row] = s;
+            }
+        }
+        if (DEFER) return;
+        __threadfence();
+        sync();
+        if (threadIdx.x == 0) s_last = atomicAdd(a.strip_done + strip, 1u) == uint32_t(a.chunks - 1);
+        sync();
+        if (s_last) {
+            __threadfence();
+            for (int t = threadIdx.x; t < S; t += kPassThreads) {
+                const int64_t row = strip * S + t;
+                if (row < n) {
+                    // chunks in order; 16 loads in flight at a time (the partials sit in L2)
+                    float s = 0.f;
+                    int64_t c = 0;
+                    for (; c + 16 <= a.chunks; c += 16) {
+                        float v[16];
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) v[q] = __ldcg(a.Wp + (c + q) * n + row);
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) s += v[q];
+                    }
+                    for (; c < a.chunks; ++c) s += __ldcg(a.Wp + c * n + row);
+                    a.rout1[row] = a.rscale1 * s;
+                    if (a.rout2) a.rout2[row] = a.rscale2 * s;
+                }
+            }
+        }
+    }
+}
+
 // One unit of a pass. LT: the loaded element type; NC: see load_vec. Flags: RANK2 add the update; CSA / CSB column sums of the loaded /
-// updated values; RDOT row dots of the updated values. Stores happen when a.dst != NULL.
-template <typename LT, int WX, bool NC, bool RANK2, bool CSA, bool CSB, bool RDOT>
+// updated values; RDOT row dots of the updated values. Stores happen when a.dst != NULL. RBX: rows each lane keeps in
+// flight (0: VecOf's default; only the batching changes, not the arithmetic). DEFER: see unit_epilogue.
+template <typename LT, int WX, bool NC, bool RANK2, bool CSA, bool CSB, bool RDOT, int RBX = 0, bool DEFER = false>
 __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
     using G = PassGeo<LT, WX>;
-    constexpr int VEC = G::VEC, WY = G::WY, S = G::S, CW = G::CW, RB = VecOf<LT>::RB;
+    constexpr int VEC = G::VEC, WY = G::WY, S = G::S, CW = G::CW, RB = RBX ? RBX : VecOf<LT>::RB;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wx = warp % WX, wy = warp / WX;
     const int64_t n = a.n;
@@ -217,71 +307,26 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
         }
     }
 
-    // ---- column sums: combine the WY warps of a column in a fixed order, one f64 partial per (strip, column) ----
-    if (CSA || CSB) {
-        double* red = reinterpret_cast<double*>(smem);
-#pragma unroll
-        for (int which = 0; which < 2; ++which) {
-            if ((which == 0 && !CSA) || (which == 1 && !CSB)) continue;
-            __syncthreads();
-#pragma unroll
-            for (int e = 0; e < VEC; ++e) red[wy * CW + (wx * 32 + lane) * VEC + e] = which == 0 ? accA[e] : accB[e];
-            __syncthreads();
-            double* P = which == 0 ? a.PA : a.PB;
-            for (int t = threadIdx.x; t < CW; t += kPassThreads) {
-                const int64_t col = chunk * CW + t;
-                if (col < n) {
-                    double s = red[t];
-#pragma unroll
-                    for (int y = 1; y < WY; ++y) s += red[y * CW + t];
-                    P[strip * n + col] = s;
-                }
-            }
-        }
-    }
+    unit_epilogue<LT, WX, CSA, CSB, RDOT, BlockSync, DEFER>(a, strip, chunk, accA, accB, racc, smem, BlockSync{});
+}
 
-    // ---- row dots: warp tree, then the WX warps of a row in order; the last chunk of a strip finishes its rows ----
-    if (RDOT) {
-        const float v = transpose_reduce32(racc);
-        float* red2 = reinterpret_cast<float*>(smem);
-        __syncthreads();
-        red2[wx * S + wy * 32 + lane] = v;
-        __syncthreads();
-        for (int t = threadIdx.x; t < S; t += kPassThreads) {
-            const int64_t row = strip * S + t;
-            if (row < n) {
-                float s = red2[t];
+// rout1[row] = rscale1 · Σ_c Wp[c][row] over the chunks in index order (f32: the order of unit_epilogue's last
+// block, so a deferred pass gives the same bits), and rout2 likewise; by every thread of the grid, no barrier inside.
+__device__ __forceinline__ void rowsum_finish(const PassArgs& a) {
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t row = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < a.n; row += gthreads) {
+        float s = 0.f;
+        int64_t c = 0;
+        for (; c + 16 <= a.chunks; c += 16) {
+            float v[16];
 #pragma unroll
-                for (int x = 1; x < WX; ++x) s += red2[x * S + t];
-                a.Wp[chunk * n + row] = s;
-            }
+            for (int q = 0; q < 16; ++q) v[q] = __ldcg(a.Wp + (c + q) * a.n + row);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) s += v[q];
         }
-        __threadfence();
-        __syncthreads();
-        __shared__ int s_last;
-        if (threadIdx.x == 0) s_last = atomicAdd(a.strip_done + strip, 1u) == uint32_t(a.chunks - 1);
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            for (int t = threadIdx.x; t < S; t += kPassThreads) {
-                const int64_t row = strip * S + t;
-                if (row < n) {
-                    // chunks in order; 16 loads in flight at a time (the partials sit in L2)
-                    float s = 0.f;
-                    int64_t c = 0;
-                    for (; c + 16 <= a.chunks; c += 16) {
-                        float v[16];
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) v[q] = __ldcg(a.Wp + (c + q) * n + row);
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) s += v[q];
-                    }
-                    for (; c < a.chunks; ++c) s += __ldcg(a.Wp + c * n + row);
-                    a.rout1[row] = a.rscale1 * s;
-                    if (a.rout2) a.rout2[row] = a.rscale2 * s;
-                }
-            }
-        }
+        for (; c < a.chunks; ++c) s += __ldcg(a.Wp + c * a.n + row);
+        a.rout1[row] = a.rscale1 * s;
+        if (a.rout2) a.rout2[row] = a.rscale2 * s;
     }
 }
 

@@ -76,9 +76,13 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
  * fixed reduction tree: results do not depend on the launch shape or on other work on the GPU. z may be NULL (zero).
  * The default schedule is three streaming passes with grid barriers (cooperative launch); flags = CSPB_GEMVER_PANEL
  * pipelines column panels instead, so that the second read of each panel of Â hits L2 (HBM traffic: A once, Â once).
- * Both give bit-identical results.
+ * flags = CSPB_GEMVER_BULK runs the three passes with the matrix streamed through a shared-memory ring by bulk
+ * asynchronous copies (one CTA per SM: 8 consumer warps and a producer warp); it applies when n is a multiple of 4
+ * (f32) or 8 (bf16), the row strides are multiples of 16 bytes and every pointer is 16-byte aligned, and otherwise
+ * falls back to the default. All schedules give bit-identical results.
  * ================================================================================================================== */
 #define CSPB_GEMVER_PANEL 1
+#define CSPB_GEMVER_BULK 2
 /* bits 8..15 of flags: the panel schedule's lag (pass 2 over a panel follows pass 1 over it by this many panels);
  * 0 = automatic (the panels the blocks in flight hold, plus one). A tuning knob: results do not depend on it. */
 #define CSPB_GEMVER_LAG_MASK 0xff00

@@ -131,18 +131,36 @@ def test_gemver_deterministic_alone_and_in_the_mix(cuda):
 
 
 @pytest.mark.parametrize("n,dtype_name,want_B", [(1000, "float32", True), (2500, "float32", False),
-                                                 (1800, "bfloat16", True), (300, "float32", True)])
-def test_gemver_panel_and_barrier_schedules_are_bit_identical(cuda, n, dtype_name, want_B):
+                                                 (1800, "bfloat16", True), (300, "float32", True),
+                                                 (1001, "float32", True), (4104, "bfloat16", False),
+                                                 (4100, "float32", True), (8, "float32", True)])
+def test_gemver_schedules_are_bit_identical(cuda, n, dtype_name, want_B):
+    """panel, barrier and bulk (the bulk-copy ring; n = 1001 takes its fallback) give the same bits."""
     import torch
     import cospanmdao_b200 as cb
     d = _inputs(torch, n, seed=11, dtype=getattr(torch, dtype_name))
     args = (d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"])
-    B0, x0, w0 = cb.gemver(*args, alpha=0.9, beta=1.1, want_B=want_B, schedule="panel")
     B1, x1, w1 = cb.gemver(*args, alpha=0.9, beta=1.1, want_B=want_B, schedule="barrier")
-    torch.cuda.synchronize()
-    assert torch.equal(x0, x1) and torch.equal(w0, w1)
-    if want_B:
-        assert torch.equal(B0, B1)
+    for sched in ("panel", "bulk", "bulk"):
+        B0, x0, w0 = cb.gemver(*args, alpha=0.9, beta=1.1, want_B=want_B, schedule=sched)
+        torch.cuda.synchronize()
+        assert torch.equal(x0, x1) and torch.equal(w0, w1), sched
+        if want_B:
+            assert torch.equal(B0, B1), sched
+
+
+def test_gemver_bulk_schedule_against_the_oracle(cuda):
+    import torch
+    import cospanmdao_b200 as cb
+    n = 4096
+    d = _inputs(torch, n, seed=12)
+    ws = cb.Workspace(cuda)
+    B, x, w = cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2,
+                        schedule="bulk", workspace=ws)
+    xo, wo, _ = oracle.gemver_f64(n, _np(d["A"]), _np(d["u1"]), _np(d["v1"]), _np(d["u2"]), _np(d["v2"]),
+                                  _np(d["y"]), _np(d["z"]), 1.5, 1.2)
+    assert oracle.rel_l2(_np(x), xo) < TOL and oracle.rel_l2(_np(w), wo) < TOL
+    assert cb.read_status(ws) == 0
 
 
 def test_bicgk(cuda):
