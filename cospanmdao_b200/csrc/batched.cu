@@ -164,7 +164,7 @@ __device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, fl
 
 template <typename T, int WX>
 __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    pass_unit<T, WX, true, true, false, true, false>(a, unit, vec_ok, smem);
+    pass_unit<T, WX, true, true, false, true, false, 16>(a, unit, vec_ok, smem);
 }
 // Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update.
 template <typename T, int WX>
@@ -173,7 +173,7 @@ __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_
         PassArgs b = a;
         b.src = a.dst;
         b.lds = a.ldd;
-        pass_unit<float, WX, false, false, false, false, true>(b, unit, vec_ok, smem);
+        pass_unit<float, WX, false, false, false, false, true, 16>(b, unit, vec_ok, smem);
     } else {
         pass_unit<T, WX, true, true, false, false, true>(a, unit, vec_ok, smem);
     }
@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     __syncthreads();
     if (!s_go) return;
     __shared__ int s_last;
-    for (;;) {
-        const uint32_t item32 = grab_work(g.ctrl, kWork0);
+    for (uint32_t item32 = grab_work(g.ctrl, kWork0);;) {
         const uint64_t item = item32;
         if (item >= 2 * U1) break;
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
         const bool pass2 = item >= U1;
         const uint64_t u = pass2 ? item - U1 : item;
         const int64_t k = find_instance(g.off[SU], g.count, u);
@@ -219,29 +219,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
                 default: unit1<T, 2>(a, unit, vec_ok, smem); break;
             }
-            __threadfence();
+            // one thread fences for the block after the barrier (the cooperative grid-sync pattern)
             __syncthreads();
-            if (threadIdx.x == 0) s_last = atomicAdd(g.p1_done + k, 1u) == uint32_t(a.strips * a.chunks - 1);
+            if (threadIdx.x == 0) {
+                __threadfence();
+                s_last = atomicAdd(g.p1_done + k, 1u) == uint32_t(a.strips * a.chunks - 1);
+                if (s_last) __threadfence();
+            }
             __syncthreads();
             if (s_last) {
-                __threadfence();
                 instance_x(a, z, beta, x);
-                __threadfence();
                 __syncthreads();
-                if (threadIdx.x == 0) st_release(g.x_ready + k, 1u);
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    st_release(g.x_ready + k, 1u);
+                }
             }
         } else {
             __shared__ int s_ok;
             if (threadIdx.x == 0) s_ok = ld_acquire(g.x_ready + k) != 0u || wait_change(g.x_ready + k, 0u, g.ctrl);
             __syncthreads();
             if (!s_ok) break;
-            __threadfence();
             switch (wx) {
                 case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
                 case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
                 default: unit2<T, 2>(a, unit, vec_ok, smem); break;
             }
         }
+        item32 = share_work(next);
     }
 }
 

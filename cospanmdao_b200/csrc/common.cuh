@@ -126,6 +126,19 @@ __device__ __forceinline__ uint32_t grab_work(uint32_t* ctrl, int word) {
     return s_item;
 }
 
+// The next work item, fetched while the current one runs: thread 0 issues the atomic before the item's work and the
+// block reads the value after it (the atomic's latency is hidden behind the item instead of preceding it).
+__device__ __forceinline__ uint32_t prefetch_work(uint32_t* ctrl, int word) {
+    return threadIdx.x == 0 ? atomicAdd(ctrl + word, 1u) : 0u;
+}
+__device__ __forceinline__ uint32_t share_work(uint32_t v) {
+    __shared__ uint32_t s_next;
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = v;
+    __syncthreads();
+    return s_next;
+}
+
 // ---- loads and stores with cache hints -------------------------------------------------------------------------
 // Streaming loads of data read once and never written by the kernel (evict-first in L2, no L1 allocation). Not
 // volatile: the compiler may schedule them freely.

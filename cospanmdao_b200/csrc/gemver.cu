@@ -47,22 +47,22 @@ struct GemverK {
 template <typename T, bool P2_FROM_B>
 __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_ok) {
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0);
-        if (u >= g.units) break;
-        pass_unit<T, kWX, true, true, false, true, false>(g.p1, u, vec_ok != 0, smem);
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        pass_unit<T, kWX, true, true, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
     if (!grid_barrier(g.ctrl)) return;
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0 + 1);
-        if (u >= g.units) break;
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
         const int64_t unit = g.units - 1 - int64_t(u);
         if constexpr (P2_FROM_B)
             pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, unit, vec_ok != 0, smem);
         else
             pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p2, unit, vec_ok != 0, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p2);
@@ -191,10 +191,10 @@ struct BicgkK {
 template <typename T>
 __global__ void __launch_bounds__(kPassThreads, 2) k_bicgk(BicgkK g, int vec_ok) {
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0);
-        if (u >= g.units) break;
-        pass_unit<T, kWX, true, false, false, true, true, 0, true>(g.p, u, vec_ok != 0, smem);
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        pass_unit<T, kWX, true, false, false, true, true, sizeof(T) == 4 ? 16 : 0, true>(g.p, u, vec_ok != 0, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p.PB, g.p.strips, g.p.n, nullptr, 1.0f, g.s);
@@ -214,38 +214,38 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain(ChainK g, int vec_ok)
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<float, kWX>()];
     const bool vo = vec_ok != 0;
     // 1: A0 -> B1, partials of B1ᵀ·ya
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0);
-        if (u >= g.units) break;
-        pass_unit<float, kWX, true, true, false, true, false>(g.p1, u, vo, smem);
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        pass_unit<float, kWX, true, true, false, true, false, 16>(g.p1, u, vo, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.za, g.beta, g.x1);
     if (!grid_barrier(g.ctrl)) return;
     // 2: B1 · x1 -> w1 (α) and q (1), from the last strip back
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0 + 1);
-        if (u >= g.units) break;
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
         pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, g.units - 1 - int64_t(u), vo, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p2);
     if (!grid_barrier(g.ctrl)) return;
     // 3: B1 -> partials of B1ᵀ·w1 (s); B2 = B1 + update; partials of B2ᵀ·q (x2)
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0 + 2);
-        if (u >= g.units) break;
-        pass_unit<float, kWX, false, true, true, true, false>(g.p3, u, vo, smem);
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 2); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 2);
+        pass_unit<float, kWX, false, true, true, true, false, 16>(g.p3, u, vo, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p3.PA, g.p3.strips, g.p3.n, nullptr, 1.0f, g.s);    // s = B1ᵀ·w1
     colsum_finish(g.p3.PB, g.p3.strips, g.p3.n, g.s, g.beta, g.x2);     // x2 = s + β·B2ᵀ·q (same thread owns s[j])
     if (!grid_barrier(g.ctrl)) return;
     // 4: B2 · x2 -> w2
-    for (;;) {
-        const uint32_t u = grab_work(g.ctrl, kWork0 + 3);
-        if (u >= g.units) break;
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 3); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 3);
         pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p4, g.units - 1 - int64_t(u), vo, smem);
+        u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p4);

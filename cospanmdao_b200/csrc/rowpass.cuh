@@ -194,12 +194,16 @@ __device__ __forceinline__ void unit_epilogue(const PassArgs& a, int64_t strip, 
             }
         }
         if (DEFER) return;
-        __threadfence();
+        // the last block of the strip: one thread fences after the barrier, for the whole block (the pattern of a
+        // cooperative grid sync: the barrier orders the other threads' partials before that fence)
         sync();
-        if (threadIdx.x == 0) s_last = atomicAdd(a.strip_done + strip, 1u) == uint32_t(a.chunks - 1);
+        if (threadIdx.x == 0) {
+            __threadfence();
+            s_last = atomicAdd(a.strip_done + strip, 1u) == uint32_t(a.chunks - 1);
+            if (s_last) __threadfence();
+        }
         sync();
         if (s_last) {
-            __threadfence();
             for (int t = threadIdx.x; t < S; t += kPassThreads) {
                 const int64_t row = strip * S + t;
                 if (row < n) {
