@@ -9,9 +9,11 @@
 //      n ~ log-U[64, 4096] hold ≈ 8.4e9 elements);
 //   3. k_run: a persistent grid pulls work items from one counter: first every pass-1 unit of every instance (read A,
 //      write Â, f64 column partials), then every pass-2 unit (row dots with x). The block that finishes the last
-//      pass-1 unit of an instance forms its x (fixed order) and publishes a flag; a pass-2 unit waits (bounded) for
-//      its instance's flag. A waiting block only ever waits on work that running blocks hold and that never waits
-//      itself, so the launch needs no co-residency guarantee.
+//      pass-1 unit of a column chunk of an instance forms x over that chunk (strips in order) and publishes the
+//      chunk's flag; a pass-2 unit waits (bounded) for the flag of its own chunk only, so x of a large instance is
+//      formed by as many blocks as it has chunks, and pass 2 starts on a chunk as soon as that chunk is done. A
+//      waiting block only ever waits on work that running blocks hold and that never waits itself, so the launch
+//      needs no co-residency guarantee.
 // Per-instance results do not depend on the rest of the batch: the geometry is a function of (n, dtype, tuning) and
 // every reduction runs in a fixed order (rowpass.cuh).
 #include "rowpass.cuh"
@@ -78,14 +80,36 @@ struct RunK {
     double* P;
     float* Wp;
     uint32_t* strip_done;
-    uint32_t* p1_done;   // [count]
-    uint32_t* x_ready;   // [count]
+    uint32_t* chunk_done;  // [Σ units]: per instance, from its unit offset, one counter per column chunk
+    uint32_t* x_ready;     // [Σ units]: likewise, one flag per column chunk
+    uint64_t cap_units;
     uint32_t* ctrl;
 };
 
 // the instance holding unit u (u_off[k] <= u < u_off[k+1]); instances with no units are skipped by construction
 __device__ __forceinline__ int64_t find_instance(const uint64_t* uoff, int64_t count, uint64_t u) {
     int64_t lo = 0, hi = count;  // uoff[lo] <= u < uoff[hi]
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldcg(uoff + mid) <= u) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// The same, starting from the instance of the block's previous item: a block takes items in increasing order, so
+// its next unit is usually in the same instance or a little later (two loads instead of a ~12-step search).
+__device__ __forceinline__ int64_t find_instance_from(const uint64_t* uoff, int64_t count, uint64_t u, int64_t hint) {
+    if (hint < 0 || hint >= count) return find_instance(uoff, count, u);
+    const uint64_t a = __ldcg(uoff + hint), b = __ldcg(uoff + hint + 1);
+    if (a <= u && u < b) return hint;
+    if (a > u) return find_instance(uoff, count, u);
+    int64_t lo = hint, hi = count;  // uoff[lo] <= u < uoff[hi] (uoff[count] is the total, > u)
+    for (int64_t step = 1;; step <<= 1) {  // gallop forward to bracket u
+        const int64_t t = lo + step;
+        if (t >= count) break;
+        if (__ldcg(uoff + t) > u) { hi = t; break; }
+        lo = t;
+    }
     while (hi - lo > 1) {
         const int64_t mid = (lo + hi) >> 1;
         if (__ldcg(uoff + mid) <= u) lo = mid; else hi = mid;
@@ -144,9 +168,11 @@ __device__ __forceinline__ PassArgs instance_args(const RunK& g, int64_t k, int 
     return a;
 }
 
-// x of one instance by one block: x[j] = z[j] + β · Σ_s P[s][j], strips in order (f64), then rounded.
-__device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, float beta, float* x) {
-    for (int64_t j = threadIdx.x; j < a.n; j += blockDim.x) {
+// x of one instance over columns [c0, c1) by one block: x[j] = z[j] + β · Σ_s P[s][j], strips in order (f64), then
+// rounded.
+__device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, float beta, float* x, int64_t c0,
+                                           int64_t c1) {
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += blockDim.x) {
         double s = 0.0;
         int64_t st = 0;
         for (; st + 8 <= a.strips; st += 8) {
@@ -190,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     const uint64_t U1 = __ldcg(g.off[SU] + g.count);
     __shared__ int s_go;
     if (threadIdx.x == 0) {
-        bool fits = 2 * U1 < 0xffffffffull;
+        bool fits = 2 * U1 < 0xffffffffull && U1 <= g.cap_units;
         for (int s = 0; s < kSets - 1; ++s)  // task mode has no packed matrix / vector offsets
             if (g.off[s] != nullptr) fits = fits && __ldcg(g.off[s] + g.count) <= g.cap[s];
         if (!fits) set_status(g.ctrl, CSPB_DEV_CAPACITY);
@@ -199,13 +225,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     __syncthreads();
     if (!s_go) return;
     __shared__ int s_last;
+    int64_t hint = 0;
     for (uint32_t item32 = grab_work(g.ctrl, kWork0);;) {
         const uint64_t item = item32;
         if (item >= 2 * U1) break;
         const uint32_t next = prefetch_work(g.ctrl, kWork0);
         const bool pass2 = item >= U1;
         const uint64_t u = pass2 ? item - U1 : item;
-        const int64_t k = find_instance(g.off[SU], g.count, u);
+        const int64_t k = find_instance_from(g.off[SU], g.count, u, hint);
+        hint = k;
         const int64_t unit = int64_t(u - __ldcg(g.off[SU] + k));
         const int wx = g.wx[k];
         bool vec_ok;
@@ -219,25 +247,31 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
                 default: unit1<T, 2>(a, unit, vec_ok, smem); break;
             }
-            // one thread fences for the block after the barrier (the cooperative grid-sync pattern)
+            // the chunk's counter; one thread fences for the block after the barrier (the cooperative grid-sync
+            // pattern). The last strip of the chunk forms x over the chunk's columns.
+            const int64_t c = unit % a.chunks;
+            const uint64_t slot = __ldcg(g.off[SU] + k) + uint64_t(c);
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                s_last = atomicAdd(g.p1_done + k, 1u) == uint32_t(a.strips * a.chunks - 1);
+                s_last = atomicAdd(g.chunk_done + slot, 1u) == uint32_t(a.strips - 1);
                 if (s_last) __threadfence();
             }
             __syncthreads();
             if (s_last) {
-                instance_x(a, z, beta, x);
+                const int64_t CW = cols_of(wx, bf16);
+                const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
+                instance_x(a, z, beta, x, c * CW, c1);
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     __threadfence();
-                    st_release(g.x_ready + k, 1u);
+                    st_release(g.x_ready + slot, 1u);
                 }
             }
         } else {
             __shared__ int s_ok;
-            if (threadIdx.x == 0) s_ok = ld_acquire(g.x_ready + k) != 0u || wait_change(g.x_ready + k, 0u, g.ctrl);
+            const uint64_t slot = __ldcg(g.off[SU] + k) + uint64_t(unit % a.chunks);
+            if (threadIdx.x == 0) s_ok = ld_acquire(g.x_ready + slot) != 0u || wait_change(g.x_ready + slot, 0u, g.ctrl);
             __syncthreads();
             if (!s_ok) break;
             switch (wx) {
@@ -262,7 +296,7 @@ namespace {
 struct BatchLayout {
     size_t off_sizes = 0, off_offs = 0, off_wx = 0, off_p1 = 0, off_xr = 0, off_scan = 0, off_P = 0, off_W = 0,
            off_S = 0, total = 0;
-    uint64_t capP = 0, capW = 0, capS = 0;
+    uint64_t capP = 0, capW = 0, capS = 0, capU = 0;
 };
 
 BatchLayout batch_layout(int64_t count, int64_t max_elems, int64_t max_vec) {
@@ -271,6 +305,8 @@ BatchLayout batch_layout(int64_t count, int64_t max_elems, int64_t max_vec) {
     L.capP = uint64_t(max_elems) / Smin + uint64_t(max_vec);
     L.capW = uint64_t(max_elems) / CWmin + uint64_t(max_vec);
     L.capS = uint64_t(max_vec) / Smin + uint64_t(count);
+    // units of an instance: ceil(n/S)·ceil(n/CW) <= n²/(S·CW) + n/S + n/CW + 1 <= n²/8192 + n/32 + 1
+    L.capU = uint64_t(max_elems) / (Smin * CWmin) + uint64_t(max_vec) / 32 + uint64_t(count);
     size_t o = kCtrlBytes;
     L.off_sizes = o;
     o = align_up(o + size_t(batch::kSets) * size_t(count) * 8, 256);
@@ -278,10 +314,10 @@ BatchLayout batch_layout(int64_t count, int64_t max_elems, int64_t max_vec) {
     o = align_up(o + 4 * size_t(count + 1) * 8, 256);
     L.off_wx = o;
     o = align_up(o + size_t(count), 256);
-    L.off_p1 = o;  // p1_done then x_ready, zeroed together with the strip counters
-    o = align_up(o + size_t(count) * 4, 256);
+    L.off_p1 = o;  // chunk counters then chunk flags, zeroed together with the strip counters
+    o = align_up(o + size_t(L.capU) * 4, 256);
     L.off_xr = o;
-    o = align_up(o + size_t(count) * 4, 256);
+    o = align_up(o + size_t(L.capU) * 4, 256);
     L.off_S = o;
     o = align_up(o + size_t(L.capS) * 4, 256);
     L.off_scan = o;
@@ -325,7 +361,7 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     char* ws = static_cast<char*>(workspace);
     const bool bf16 = a_dtype == CSPB_BF16;
-    // control block, p1_done, x_ready, strip counters: zeroed per call
+    // control block, chunk counters and flags, strip counters: zeroed per call
     if (cudaMemsetAsync(ws, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
     if (cudaMemsetAsync(ws + L.off_p1, 0, L.off_scan - L.off_p1, st) != cudaSuccess) return CSPB_ERR_CUDA;
 
@@ -376,8 +412,9 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     g.P = reinterpret_cast<double*>(ws + L.off_P);
     g.Wp = reinterpret_cast<float*>(ws + L.off_W);
     g.strip_done = reinterpret_cast<uint32_t*>(ws + L.off_S);
-    g.p1_done = reinterpret_cast<uint32_t*>(ws + L.off_p1);
+    g.chunk_done = reinterpret_cast<uint32_t*>(ws + L.off_p1);
     g.x_ready = reinterpret_cast<uint32_t*>(ws + L.off_xr);
+    g.cap_units = L.capU;
     g.ctrl = reinterpret_cast<uint32_t*>(ws);
     const void* kern = bf16 ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16>)
                             : reinterpret_cast<const void*>(batch::k_run<float>);

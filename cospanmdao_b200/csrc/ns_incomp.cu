@@ -85,14 +85,138 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
     right = need_r ? row.r : from_right;
 }
 
+// ---- f32 rows through a shared-memory ring (cp.async) -------------------------------------------------------------
+// A warp keeps kNsiRing rows of u, v, p in flight in its own ring of shared-memory slots instead of registers: each
+// lane copies its 16-byte cells of a row (cp.async, no register held while the copy is in flight), lane 0 and the
+// last active lane copy the two wrapped halo cells of the strip, and the warp computes row j from the slots of rows
+// j-1, j, j+1 while rows j+2 .. j+kNsiRing-2 are still arriving. A slot is one row of one field: [3] the cell left of
+// the strip, [4 .. 4+128) the strip's cells, [4 + cells] the cell right of it.
+constexpr int kNsiRing = 8;
+constexpr int kNsiSlot = 136;  // floats
+constexpr size_t kNsiRingBytes = size_t(kNsiWarps) * kNsiRing * 3 * kNsiSlot * sizeof(float);
+
+__device__ __forceinline__ uint32_t nsi_smem(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void nsi_cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(nsi_smem(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void nsi_cp4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(nsi_smem(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void nsi_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void nsi_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One warp item (a strip of 128 columns × H rows) of an f32 residual with nx % 4 == 0 and 16-byte aligned fields.
+// The arithmetic per cell is the register path's, operation for operation.
+__device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float* ring, double& su, double& sv,
+                                              double& sc) {
+    const int lane = threadIdx.x & 31;
+    const int seg = int(item % g.segs);
+    const int strip = int(item / g.segs);
+    const int sc0 = seg * 128;                               // first column of the strip
+    const int scols = g.nx - sc0 >= 128 ? 128 : g.nx - sc0;  // a multiple of 4
+    const int c0 = sc0 + lane * 4;
+    const bool active = lane * 4 < scols;
+    const bool last = active && (lane + 1) * 4 >= scols;
+    const int j0 = strip * g.H;
+    const int j1 = min(g.ny, j0 + g.H);
+    const int64_t nx = g.nx;
+    const float* F[3] = {static_cast<const float*>(g.u), static_cast<const float*>(g.v),
+                         static_cast<const float*>(g.p)};
+    const int lcol = sc0 == 0 ? g.nx - 1 : sc0 - 1;
+    const int rcol = (sc0 + scols) % g.nx;
+    auto wrapj = [&](int j) { return j < 0 ? j + g.ny : (j >= g.ny ? j - g.ny : j); };
+    auto slot = [&](int r, int f) { return ring + ((r - (j0 - 1)) % kNsiRing * 3 + f) * kNsiSlot; };
+    // rows j0-1 .. j1 are read; one commit group per row, empty past j1
+    auto issue = [&](int r) {
+        if (r <= j1) {
+            const int64_t ro = int64_t(wrapj(r)) * nx;
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                float* sl = slot(r, f);
+                if (active) nsi_cp16(sl + 4 + lane * 4, F[f] + ro + c0);
+                if (lane == 0) nsi_cp4(sl + 3, F[f] + ro + lcol);
+                if (last) nsi_cp4(sl + 4 + scols, F[f] + ro + rcol);
+            }
+        }
+        nsi_commit();
+    };
+#pragma unroll 1
+    for (int q = 0; q < kNsiRing - 1; ++q) issue(j0 - 1 + q);
+    const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
+#pragma unroll 1
+    for (int j = j0; j < j1; ++j) {
+        issue(j + kNsiRing - 2);  // into the slot row j-2 left (free since the last iteration's __syncwarp)
+        // issued: rows j0-1 .. j+kNsiRing-2, one group each; rows up to j+1 must have landed (for this lane)
+        nsi_wait<kNsiRing - 3>();
+        __syncwarp();              // and every lane's copies are visible to the warp
+        if (active) {
+            float cu[6], cv[6], cp[6];  // W, 4 cells, E of row j
+            float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
+            {
+                const float* a = slot(j, 0) + 4 + lane * 4;
+                const float* b = slot(j, 1) + 4 + lane * 4;
+                const float* c = slot(j, 2) + 4 + lane * 4;
+                const float4 ua = *reinterpret_cast<const float4*>(a), va = *reinterpret_cast<const float4*>(b),
+                             pa = *reinterpret_cast<const float4*>(c);
+                cu[0] = a[-1]; cu[1] = ua.x; cu[2] = ua.y; cu[3] = ua.z; cu[4] = ua.w; cu[5] = a[4];
+                cv[0] = b[-1]; cv[1] = va.x; cv[2] = va.y; cv[3] = va.z; cv[4] = va.w; cv[5] = b[4];
+                cp[0] = c[-1]; cp[1] = pa.x; cp[2] = pa.y; cp[3] = pa.z; cp[4] = pa.w; cp[5] = c[4];
+                const float4 us = *reinterpret_cast<const float4*>(slot(j - 1, 0) + 4 + lane * 4);
+                const float4 un = *reinterpret_cast<const float4*>(slot(j + 1, 0) + 4 + lane * 4);
+                const float4 vs = *reinterpret_cast<const float4*>(slot(j - 1, 1) + 4 + lane * 4);
+                const float4 vn = *reinterpret_cast<const float4*>(slot(j + 1, 1) + 4 + lane * 4);
+                const float4 ps = *reinterpret_cast<const float4*>(slot(j - 1, 2) + 4 + lane * 4);
+                const float4 pn = *reinterpret_cast<const float4*>(slot(j + 1, 2) + 4 + lane * 4);
+                uS[0] = us.x; uS[1] = us.y; uS[2] = us.z; uS[3] = us.w;
+                uN[0] = un.x; uN[1] = un.y; uN[2] = un.z; uN[3] = un.w;
+                vS[0] = vs.x; vS[1] = vs.y; vS[2] = vs.z; vS[3] = vs.w;
+                vN[0] = vn.x; vN[1] = vn.y; vN[2] = vn.z; vN[3] = vn.w;
+                pS[0] = ps.x; pS[1] = ps.y; pS[2] = ps.z; pS[3] = ps.w;
+                pN[0] = pn.x; pN[1] = pn.y; pN[2] = pn.z; pN[3] = pn.w;
+            }
+            float oru[4], orv[4], orc[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float uc = cu[e + 1], vc = cv[e + 1];
+                const float uW = cu[e], uE = cu[e + 2];
+                const float vW = cv[e], vE = cv[e + 2];
+                const float pW = cp[e], pE = cp[e + 2];
+                const float dudx = (uE - uW) * inv2h, dudy = (uN[e] - uS[e]) * inv2h;
+                const float dvdx = (vE - vW) * inv2h, dvdy = (vN[e] - vS[e]) * inv2h;
+                const float dpdx = (pE - pW) * inv2h, dpdy = (pN[e] - pS[e]) * inv2h;
+                const float lapu = (((uE - uc) + (uW - uc)) + ((uN[e] - uc) + (uS[e] - uc))) * invh2;
+                const float lapv = (((vE - vc) + (vW - vc)) + ((vN[e] - vc) + (vS[e] - vc))) * invh2;
+                const float ru = ((uc * dudx + vc * dudy) + dpdx) - nu * lapu;
+                const float rv = ((uc * dvdx + vc * dvdy) + dpdy) - nu * lapv;
+                const float rc = dudx + dvdy;
+                oru[e] = ru; orv[e] = rv; orc[e] = rc;
+                su = __fma_rn(double(ru), double(ru), su);
+                sv = __fma_rn(double(rv), double(rv), sv);
+                sc = __fma_rn(double(rc), double(rc), sc);
+            }
+            const int64_t ro = int64_t(j) * nx + c0;
+            st_f4(g.ru + ro, make_float4(oru[0], oru[1], oru[2], oru[3]));
+            st_f4(g.rv + ro, make_float4(orv[0], orv[1], orv[2], orv[3]));
+            st_f4(g.rc + ro, make_float4(orc[0], orc[1], orc[2], orc[3]));
+        }
+        __syncwarp();  // every lane is done with row j-1's slot before the next iteration refills it
+    }
+    nsi_wait<0>();
+    __syncwarp();
+}
+
 // Block b (of nblocks) of one residual: its 8 warps take items 8b .. 8b+7. Its norm partial goes to part[b]; the last
 // block to finish (counter `done`) sums the partials in block order.
 template <typename T, int VEC>
-__device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done) {
+__device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done,
+                                          float* ring = nullptr) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t item = b * kNsiWarps + warp;
     double su = 0.0, sv = 0.0, sc = 0.0;
-    if (item < g.items) {  // warp-uniform
+    if constexpr (sizeof(T) == 4 && VEC == 4) {
+        if (item < g.items) nsi_rows_ring(g, item, ring + size_t(warp) * kNsiRing * 3 * kNsiSlot, su, sv, sc);
+    } else if (item < g.items) {  // warp-uniform
         const int seg = int(item % g.segs);
         const int strip = int(item / g.segs);
         const int c0 = seg * 32 * VEC + lane * VEC;
@@ -208,7 +332,8 @@ __device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblo
 
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
-    nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
+    extern __shared__ __align__(16) float nsi_ring[];
+    nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_ring);
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
@@ -256,6 +381,7 @@ __global__ void k_nsi_plan(NsiTasksK g) {
 
 template <typename T>
 __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
+    extern __shared__ __align__(16) float nsi_ring[];
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = __ldcg(g.boff + g.count) <= g.cap_blocks && !status_bad(g.ctrl);
     __syncthreads();
@@ -265,14 +391,29 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
     }
     const uint64_t total = __ldcg(g.boff + g.count);
     constexpr int vfast = 4;
-    for (;;) {
-        const uint32_t v = grab_work(g.ctrl, kWork0);
-        if (uint64_t(v) >= total) break;
-        int64_t lo = 0, hi = g.count;  // boff[lo] <= v < boff[hi]
+    int64_t hint = 0;
+    for (uint32_t v = grab_work(g.ctrl, kWork0); uint64_t(v) < total;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        // the task of block v: boff[lo] <= v < boff[lo + 1]; a block's items increase, so start from its last task
+        int64_t lo = 0, hi = g.count;
+        const uint64_t ha = __ldcg(g.boff + hint), hb = __ldcg(g.boff + hint + 1);
+        if (ha <= v && v < hb) {
+            lo = hint;
+            hi = hint + 1;
+        } else if (ha <= v) {
+            lo = hint;
+            for (int64_t step = 1;; step <<= 1) {
+                const int64_t t = lo + step;
+                if (t >= g.count) break;
+                if (__ldcg(g.boff + t) > v) { hi = t; break; }
+                lo = t;
+            }
+        }
         while (hi - lo > 1) {
             const int64_t mid = (lo + hi) >> 1;
             if (__ldcg(g.boff + mid) <= v) lo = mid; else hi = mid;
         }
+        hint = lo;
         const cspb_ns_incomp_task& t = g.tasks[lo];
         const bool fast = nsi_fast(t, vfast);
         NsiK k{};
@@ -289,8 +430,9 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
         k.part = g.part + 3 * __ldcg(g.boff + lo);
         k.ctrl = g.ctrl;
         const int64_t b = int64_t(v) - int64_t(__ldcg(g.boff + lo));
-        if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
+        if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo, nsi_ring);
         else nsi_block<T, 1>(k, b, blocks, g.done + lo);
+        v = share_work(next);
     }
 }
 
@@ -301,6 +443,11 @@ using cspb_host::align_up;
 using cspb_host::aligned;
 
 namespace {
+
+// The ring needs more than the default 48 KB of dynamic shared memory per block.
+bool ring_ready(const void* kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kNsiRingBytes)) == cudaSuccess;
+}
 
 struct NsiPlan {
     int vec = 4, H = 32, segs = 0;
@@ -385,9 +532,11 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     if (bf16) {
         if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
+    } else if (fast) {
+        if (!ring_ready(reinterpret_cast<const void*>(k_ns_incomp<float, 4>))) return CSPB_ERR_LAUNCH;
+        k_ns_incomp<float, 4><<<grid, block, kNsiRingBytes, st>>>(g);
     } else {
-        if (fast) k_ns_incomp<float, 4><<<grid, block, 0, st>>>(g);
-        else k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
+        k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
@@ -429,11 +578,13 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
     if (r != CSPB_OK) return r;
     const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16>)
                               : reinterpret_cast<const void*>(k_nsi_tasks<float>);
+    const size_t smem = g.bf16 ? 0 : kNsiRingBytes;
+    if (smem && !ring_ready(kern)) return CSPB_ERR_LAUNCH;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNsiThreads, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNsiThreads, smem) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;
     void* args[] = {&g};
-    if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(kNsiThreads), args, 0, st) != cudaSuccess)
+    if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(kNsiThreads), args, smem, st) != cudaSuccess)
         return CSPB_ERR_LAUNCH;
     return CSPB_OK;
 }
