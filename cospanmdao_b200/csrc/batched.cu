@@ -190,7 +190,7 @@ __device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, fl
 
 template <typename T, int WX>
 __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    pass_unit<T, WX, true, true, false, true, false, 16>(a, unit, vec_ok, smem);
+    pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(a, unit, vec_ok, smem);
 }
 // Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update.
 template <typename T, int WX>

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
     for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0);
-        pass_unit<T, kWX, true, true, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
+        pass_unit<T, kWX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(g.p1, u, vec_ok != 0, smem);
         u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;

@@ -124,6 +124,10 @@ __device__ __forceinline__ void store_vec(float* row, int64_t c0, int ncols, boo
     }
 }
 
+// 16-bit storage carries twice the elements per byte: its column sums take 8 products in f32 before each f64
+// addition, so that the f32 -> f64 conversions do not bound the pass (f32 storage converts every product).
+template <typename LT> inline constexpr bool kF32Part = sizeof(LT) == 2;
+
 // Shared memory a pass needs (bytes).
 template <typename T, int WX>
 __host__ __device__ constexpr size_t pass_smem_bytes() {
@@ -261,6 +265,9 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
     double accA[VEC], accB[VEC];
 #pragma unroll
     for (int e = 0; e < VEC; ++e) { accA[e] = 0.0; accB[e] = 0.0; }
+    float pA[VEC], pB[VEC];  // f32 partials of 8 rows (16-bit storage only)
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) { pA[e] = 0.f; pB[e] = 0.f; }
     float racc[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) racc[k] = 0.f;
@@ -292,13 +299,34 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
                         b[e] = RANK2 ? __fadd_rn(__fadd_rn(val[e], __fmul_rn(u1k, v1c[e])), __fmul_rn(u2k, v2c[e]))
                                      : val[e];
                     if (store && ncols > 0) store_vec<VEC>(a.dst + (r0 + kk) * a.ldd, c0, ncols, vec_ok, b);
-                    if (CSA) {
+                    if constexpr (kF32Part<LT>) {
+                        // 16-bit storage: 8 products of a column in f32, then into the f64 sum (one conversion per 8 rows)
+                        const bool flush = (kk & 7) == 7 || kk == nrows - 1;
+                        if (CSA) {
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) accA[e] = __fma_rn(double(val[e]), double(cyak), accA[e]);
-                    }
-                    if (CSB) {
+                            for (int e = 0; e < VEC; ++e) pA[e] = fmaf(val[e], cyak, pA[e]);
+                            if (flush) {
 #pragma unroll
-                        for (int e = 0; e < VEC; ++e) accB[e] = __fma_rn(double(b[e]), double(cybk), accB[e]);
+                                for (int e = 0; e < VEC; ++e) { accA[e] += double(pA[e]); pA[e] = 0.f; }
+                            }
+                        }
+                        if (CSB) {
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) pB[e] = fmaf(b[e], cybk, pB[e]);
+                            if (flush) {
+#pragma unroll
+                                for (int e = 0; e < VEC; ++e) { accB[e] += double(pB[e]); pB[e] = 0.f; }
+                            }
+                        }
+                    } else {
+                        if (CSA) {
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) accA[e] = __fma_rn(double(val[e]), double(cyak), accA[e]);
+                        }
+                        if (CSB) {
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) accB[e] = __fma_rn(double(b[e]), double(cybk), accB[e]);
+                        }
                     }
                     if (RDOT) {
                         float d = 0.f;
