@@ -128,13 +128,20 @@ __device__ __forceinline__ void store_vec(float* row, int64_t c0, int ncols, boo
 // addition, so that the f32 -> f64 conversions do not bound the pass (f32 storage converts every product).
 template <typename LT> inline constexpr bool kF32Part = sizeof(LT) == 2;
 
+// 16-bit storage also keeps its unit loop rolled (8 rows of 8 elements per lane and batch make a fully unrolled unit
+// too large for the instruction cache); its row dots then wait in shared memory, one float per (warp, row, lane),
+// in the same region the epilogue uses afterwards.
+template <typename LT> inline constexpr bool kRolled = sizeof(LT) == 2;
+constexpr size_t kRolledDotBytes = size_t(kPassThreads) * 32 * sizeof(float);
+
 // Shared memory a pass needs (bytes).
 template <typename T, int WX>
 __host__ __device__ constexpr size_t pass_smem_bytes() {
     using G = PassGeo<T, WX>;
     const size_t cs = size_t(G::WY) * G::CW * sizeof(double);
     const size_t rd = size_t(WX) * G::S * sizeof(float);
-    return cs > rd ? cs : rd;
+    const size_t m = cs > rd ? cs : rd;
+    return kRolled<T> && kRolledDotBytes > m ? kRolledDotBytes : m;
 }
 
 // Synchronisation of the threads that run a unit's epilogue: the whole block (pass_unit) or, in a kernel with a
@@ -274,9 +281,9 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
 
     const LT* src = static_cast<const LT*>(a.src);
     const bool store = a.dst != nullptr;
+    float* rdot = reinterpret_cast<float*>(smem) + size_t(warp) * 32 * 32;  // rolled loop: [row][lane] of the warp
 
-#pragma unroll
-    for (int kb = 0; kb < 32; kb += RB) {
+    auto batch = [&](int kb) {
         if (kb < nrows) {  // warp-uniform
             uint4 raw[RB];
 #pragma unroll
@@ -332,11 +339,23 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
                         float d = 0.f;
 #pragma unroll
                         for (int e = 0; e < VEC; ++e) d = fmaf(b[e], xc[e], d);
-                        racc[kk] = d;
+                        if constexpr (kRolled<LT>) rdot[kk * 32 + lane] = d;
+                        else racc[kk] = d;
                     }
                 }
             }
         }
+    };
+    if constexpr (kRolled<LT>) {
+#pragma unroll 1
+        for (int kb = 0; kb < 32; kb += RB) batch(kb);
+        if (RDOT) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) racc[k] = k < nrows ? rdot[k * 32 + lane] : 0.f;  // this lane's own values
+        }
+    } else {
+#pragma unroll
+        for (int kb = 0; kb < 32; kb += RB) batch(kb);
     }
 
     unit_epilogue<LT, WX, CSA, CSB, RDOT, BlockSync, DEFER>(a, strip, chunk, accA, accB, racc, smem, BlockSync{});
