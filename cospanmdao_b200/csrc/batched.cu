@@ -22,6 +22,7 @@ namespace cspb {
 namespace batch {
 
 constexpr int kThreads = kPassThreads;
+constexpr uint32_t kGroup = 4;  // consecutive work items a block takes at once
 constexpr int kSets = 6;  // a, v, p, w, s, u
 enum { SA = 0, SV = 1, SP = 2, SW = 3, SS = 4, SU = 5 };
 
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     const uint64_t U1 = __ldcg(g.off[SU] + g.count);
     __shared__ int s_go;
     if (threadIdx.x == 0) {
-        bool fits = 2 * U1 < 0xffffffffull && U1 <= g.cap_units;
+        bool fits = 2 * U1 < 0xffffffffull - (1ull << 24) && U1 <= g.cap_units;  // room for the counter's overshoot
         for (int s = 0; s < kSets - 1; ++s)  // task mode has no packed matrix / vector offsets
             if (g.off[s] != nullptr) fits = fits && __ldcg(g.off[s] + g.count) <= g.cap[s];
         if (!fits) set_status(g.ctrl, CSPB_DEV_CAPACITY);
@@ -225,62 +226,79 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     __syncthreads();
     if (!s_go) return;
     __shared__ int s_last;
-    int64_t hint = 0;
-    for (uint32_t item32 = grab_work(g.ctrl, kWork0);;) {
-        const uint64_t item = item32;
-        if (item >= 2 * U1) break;
-        const uint32_t next = prefetch_work(g.ctrl, kWork0);
-        const bool pass2 = item >= U1;
-        const uint64_t u = pass2 ? item - U1 : item;
-        const int64_t k = find_instance_from(g.off[SU], g.count, u, hint);
-        hint = k;
-        const int64_t unit = int64_t(u - __ldcg(g.off[SU] + k));
-        const int wx = g.wx[k];
-        bool vec_ok;
-        const float* z;
-        float beta;
-        float* x;
-        const PassArgs a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
-        if (!pass2) {
-            switch (wx) {
-                case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
-                case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
-                default: unit1<T, 2>(a, unit, vec_ok, smem); break;
+    __shared__ int s_ok;
+    // A block takes kGroup consecutive items at a time (usually units of one instance), so the lookup of the instance
+    // and of its arguments is paid once per group rather than once per unit.
+    int64_t hint = 0, cur = -1;
+    PassArgs a{};
+    bool vec_ok = false;
+    const float* z = nullptr;
+    float beta = 0.f;
+    float* x = nullptr;
+    int wx = 2;
+    uint64_t ubase = 0;
+    for (uint32_t base = grab_work(g.ctrl, kWork0, kGroup); uint64_t(base) < 2 * U1;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0, kGroup);
+        bool stop = false;
+        for (uint32_t q = 0; q < kGroup; ++q) {
+            const uint64_t item = uint64_t(base) + q;
+            if (item >= 2 * U1) break;
+            const bool pass2 = item >= U1;
+            const uint64_t u = pass2 ? item - U1 : item;
+            const int64_t k = find_instance_from(g.off[SU], g.count, u, hint);
+            hint = k;
+            if (k != cur) {
+                cur = k;
+                wx = g.wx[k];
+                ubase = __ldcg(g.off[SU] + k);
+                a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
             }
-            // the chunk's counter; one thread fences for the block after the barrier (the cooperative grid-sync
-            // pattern). The last strip of the chunk forms x over the chunk's columns.
-            const int64_t c = unit % a.chunks;
-            const uint64_t slot = __ldcg(g.off[SU] + k) + uint64_t(c);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                __threadfence();
-                s_last = atomicAdd(g.chunk_done + slot, 1u) == uint32_t(a.strips - 1);
-                if (s_last) __threadfence();
-            }
-            __syncthreads();
-            if (s_last) {
-                const int64_t CW = cols_of(wx, bf16);
-                const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
-                instance_x(a, z, beta, x, c * CW, c1);
+            const int64_t unit = int64_t(u - ubase);
+            const uint64_t slot = ubase + uint64_t(unit % a.chunks);  // the unit's column chunk
+            if (!pass2) {
+                switch (wx) {
+                    case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
+                    case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
+                    default: unit1<T, 2>(a, unit, vec_ok, smem); break;
+                }
+                // the chunk's counter; one thread fences for the block after the barrier (the cooperative grid-sync
+                // pattern). The last strip of the chunk forms x over the chunk's columns.
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     __threadfence();
-                    st_release(g.x_ready + slot, 1u);
+                    s_last = atomicAdd(g.chunk_done + slot, 1u) == uint32_t(a.strips - 1);
+                    if (s_last) __threadfence();
+                }
+                __syncthreads();
+                if (s_last) {
+                    const int64_t c = unit % a.chunks;
+                    const int64_t CW = cols_of(wx, bf16);
+                    const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
+                    instance_x(a, z, beta, x, c * CW, c1);
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        __threadfence();
+                        st_release(g.x_ready + slot, 1u);
+                    }
+                }
+            } else {
+                if (threadIdx.x == 0)
+                    s_ok = ld_acquire(g.x_ready + slot) != 0u || wait_change(g.x_ready + slot, 0u, g.ctrl);
+                __syncthreads();
+                if (!s_ok) {
+                    stop = true;
+                    break;
+                }
+                switch (wx) {
+                    case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
+                    case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
+                    default: unit2<T, 2>(a, unit, vec_ok, smem); break;
                 }
             }
-        } else {
-            __shared__ int s_ok;
-            const uint64_t slot = __ldcg(g.off[SU] + k) + uint64_t(unit % a.chunks);
-            if (threadIdx.x == 0) s_ok = ld_acquire(g.x_ready + slot) != 0u || wait_change(g.x_ready + slot, 0u, g.ctrl);
-            __syncthreads();
-            if (!s_ok) break;
-            switch (wx) {
-                case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
-                case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
-                default: unit2<T, 2>(a, unit, vec_ok, smem); break;
-            }
+            __syncthreads();  // s_last / s_ok and the unit's shared memory are reused by the next item
         }
-        item32 = share_work(next);
+        if (stop) break;
+        base = share_work(next);
     }
 }
 

@@ -118,18 +118,18 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* ctrl) {
 }
 
 // One dynamic work item for the whole block from counter `word`.
-__device__ __forceinline__ uint32_t grab_work(uint32_t* ctrl, int word) {
+__device__ __forceinline__ uint32_t grab_work(uint32_t* ctrl, int word, uint32_t amount = 1u) {
     __shared__ uint32_t s_item;
     __syncthreads();
-    if (threadIdx.x == 0) s_item = atomicAdd(ctrl + word, 1u);
+    if (threadIdx.x == 0) s_item = atomicAdd(ctrl + word, amount);
     __syncthreads();
     return s_item;
 }
 
 // The next work item, fetched while the current one runs: thread 0 issues the atomic before the item's work and the
 // block reads the value after it (the atomic's latency is hidden behind the item instead of preceding it).
-__device__ __forceinline__ uint32_t prefetch_work(uint32_t* ctrl, int word) {
-    return threadIdx.x == 0 ? atomicAdd(ctrl + word, 1u) : 0u;
+__device__ __forceinline__ uint32_t prefetch_work(uint32_t* ctrl, int word, uint32_t amount = 1u) {
+    return threadIdx.x == 0 ? atomicAdd(ctrl + word, amount) : 0u;
 }
 __device__ __forceinline__ uint32_t share_work(uint32_t v) {
     __shared__ uint32_t s_next;

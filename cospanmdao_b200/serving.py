@@ -110,6 +110,25 @@ def make_workload(n_req: int = 20000, *, rate: float | None = None, seed: int = 
 
 
 # ---- resident models --------------------------------------------------------------------------------------------
+def model_matrix(n: int, dtype, seed: int, device):
+    """A GEMVER model's matrix: the seeded generator's n×n values (element (i, j) from index i·n + j), stored with its
+    rows padded to a multiple of 8 elements so that every row starts on 16 bytes (the kernels' vector loads need it;
+    an unpadded odd n would leave most rows misaligned). Returns the (n, n) view; its stride(0) is the padded pitch."""
+    import cospanmdao_b200 as cb
+    torch = _torch()
+    ld = (n + 7) // 8 * 8
+    buf = torch.empty((n, ld), dtype=dtype, device=device)
+    if ld == n:
+        cb.fill_hash(buf, seed, 0)
+    else:
+        tmp = torch.empty((n, n), dtype=dtype, device=device)
+        cb.fill_hash(tmp, seed, 0)
+        buf[:, :n].copy_(tmp)
+        del tmp
+    return buf[:, :n]
+
+
+
 @dataclass
 class Model:
     id: int
@@ -142,7 +161,9 @@ class ModelStore:
         kind, size = self.wl.model_size[mid]
         dt = self.dtype if kind == KIND_GEMVER else self.ns_dtype
         es = 2 if dt == _torch().bfloat16 else 4
-        return size * size * es * (1 if kind == KIND_GEMVER else 3)
+        if kind == KIND_GEMVER:
+            return size * ((size + 7) // 8 * 8) * es  # rows padded to 8 elements (model_matrix)
+        return size * size * es * 3
 
     def _load(self, mid: int) -> Model:
         import cospanmdao_b200 as cb
@@ -150,9 +171,7 @@ class ModelStore:
         torch = _torch()
         kind, size = self.wl.model_size[mid]
         if kind == KIND_GEMVER:
-            A = torch.empty((size, size), dtype=self.dtype, device=self.device)
-            cb.fill_hash(A, 16 * (1000 + mid) + 1, 0)
-            t = {"A": A}
+            t = {"A": model_matrix(size, self.dtype, 16 * (1000 + mid) + 1, self.device)}
         else:
             u, v, p, h = workloads.ns_fields(size, seed=1000 + mid, dtype=self.ns_dtype, device=self.device)
             t = {"u": u, "v": v, "p": p, "h": h}
@@ -267,10 +286,11 @@ class Server:
                 n = wl.size[gi]
                 base_in = int(slot.dev_in.data_ptr()) + 4 * (wl.in_off[gi] - in0)
                 base_out = int(slot.dev_out.data_ptr()) + 4 * (wl.out_off[gi] - o0)
+                mats = [self.store.models[int(m)].tensors["A"] for m in wl.model[gi]]
                 t["n"] = n
-                t["lda"] = n
+                t["lda"] = [a.stride(0) for a in mats]
                 t["ldb"] = n
-                t["A"] = [self.store.models[int(m)].tensors["A"].data_ptr() for m in wl.model[gi]]
+                t["A"] = [a.data_ptr() for a in mats]
                 for k, name in enumerate(("u1", "v1", "u2", "v2", "y", "z")):
                     t[name] = base_in + 4 * k * n
                 t["x"] = base_out
@@ -374,9 +394,7 @@ def plain(wl: Workload, *, device=None, stream=None) -> dict:
     models = {}
     for m, (kind, size) in wl.model_size.items():
         if kind == KIND_GEMVER:
-            A = torch.empty((size, size), dtype=torch.float32, device=dev)
-            cb.fill_hash(A, 16 * (1000 + m) + 1, 0)
-            models[m] = {"A": A}
+            models[m] = {"A": model_matrix(size, torch.float32, 16 * (1000 + m) + 1, dev)}
         else:
             u, v, p, h = workloads.ns_fields(size, seed=1000 + m, dtype=torch.float32, device=dev)
             models[m] = {"u": u, "v": v, "p": p, "h": h}

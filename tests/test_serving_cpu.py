@@ -19,11 +19,11 @@ class FakeWl:
 
 def test_store_budget_and_lru():
     import torch
-    wl = FakeWl([100, 100, 100, 100])  # 100*100*2 = 20000 bytes each in bf16
+    wl = FakeWl([96, 96, 96, 96])  # 96*96*2 = 18432 bytes each in bf16 (rows already a multiple of 8)
     st = FakeStore(wl, dtype=torch.bfloat16, budget_bytes=50000, device="cpu")
     assert st.acquire([0, 1])
     st.release([0, 1])
-    assert st.used == 40000 and st.loads == 2
+    assert st.used == 36864 and st.loads == 2
     assert st.acquire([2])          # evicts the least recently used (0)
     assert 0 not in st.models and {1, 2} <= set(st.models) and st.evictions == 1
     assert not st.acquire([0, 3])   # 2 is in use and 1 + two new ones do not fit
@@ -33,6 +33,12 @@ def test_store_budget_and_lru():
     # a model in use is never evicted
     assert not st.acquire([1, 2])
     st.release([0, 3])
+
+
+def test_store_counts_padded_rows():
+    import torch
+    st = FakeStore(FakeWl([100]), dtype=torch.bfloat16, budget_bytes=1e9, device="cpu")
+    assert st.bytes_of(0) == 100 * 104 * 2  # rows padded to 8 elements
 
 
 def test_store_repeated_model_counts_once():
