@@ -86,12 +86,14 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
 }
 
 // ---- f32 rows through a shared-memory ring (cp.async) -------------------------------------------------------------
-// A warp keeps kNsiRing rows of u, v, p in flight in its own ring of shared-memory slots instead of registers: each
+// A warp streams the rows of u, v, p through its own ring of kNsiRing shared-memory slots instead of registers: each
 // lane copies its 16-byte cells of a row (cp.async, no register held while the copy is in flight), lane 0 and the
 // last active lane copy the two wrapped halo cells of the strip, and the warp computes row j from the slots of rows
 // j-1, j, j+1 while rows j+2 .. j+kNsiRing-2 are still arriving. A slot is one row of one field: [3] the cell left of
-// the strip, [4 .. 4+128) the strip's cells, [4 + cells] the cell right of it.
-constexpr int kNsiRing = 8;
+// the strip, [4 .. 4+128) the strip's cells, [4 + cells] the cell right of it. Measured on B200 at 4096², a ring of 4
+// slots (26 KB per warp row set, 4 blocks of 8 warps per SM) runs a little faster than rings of 5 or 8 slots with
+// fewer blocks: the warps, not the depth of each warp's ring, keep the memory system busy.
+constexpr int kNsiRing = 4;
 constexpr int kNsiSlot = 136;  // floats
 constexpr size_t kNsiRingBytes = size_t(kNsiWarps) * kNsiRing * 3 * kNsiSlot * sizeof(float);
 
@@ -107,7 +109,8 @@ template <int N>
 __device__ __forceinline__ void nsi_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // One warp item (a strip of 128 columns × H rows) of an f32 residual with nx % 4 == 0 and 16-byte aligned fields.
-// The arithmetic per cell is the register path's, operation for operation.
+// The residuals are the register path's, operation for operation; the squares of a lane's 4 cells are summed in f32
+// before each f64 addition (a quarter of the conversions).
 __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float* ring, double& su, double& sv,
                                               double& sc) {
     const int lane = threadIdx.x & 31;
@@ -121,53 +124,70 @@ __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float
     const int j0 = strip * g.H;
     const int j1 = min(g.ny, j0 + g.H);
     const int64_t nx = g.nx;
-    const float* F[3] = {static_cast<const float*>(g.u), static_cast<const float*>(g.v),
-                         static_cast<const float*>(g.p)};
+    const float* U = static_cast<const float*>(g.u);
+    const float* V = static_cast<const float*>(g.v);
+    const float* P = static_cast<const float*>(g.p);
     const int lcol = sc0 == 0 ? g.nx - 1 : sc0 - 1;
     const int rcol = (sc0 + scols) % g.nx;
-    auto wrapj = [&](int j) { return j < 0 ? j + g.ny : (j >= g.ny ? j - g.ny : j); };
-    auto slot = [&](int r, int f) { return ring + ((r - (j0 - 1)) % kNsiRing * 3 + f) * kNsiSlot; };
-    // rows j0-1 .. j1 are read; one commit group per row, empty past j1
-    auto issue = [&](int r) {
-        if (r <= j1) {
-            const int64_t ro = int64_t(wrapj(r)) * nx;
-#pragma unroll
-            for (int f = 0; f < 3; ++f) {
-                float* sl = slot(r, f);
-                if (active) nsi_cp16(sl + 4 + lane * 4, F[f] + ro + c0);
-                if (lane == 0) nsi_cp4(sl + 3, F[f] + ro + lcol);
-                if (last) nsi_cp4(sl + 4 + scols, F[f] + ro + rcol);
+    constexpr int kField = kNsiSlot, kRow = 3 * kNsiSlot;  // floats between the fields of a slot, between slots
+    float* const mine = ring + 4 + lane * 4;                 // this lane's cells in slot 0, field 0
+    // rows j0-1 .. j1 are read; one commit group per row (empty past j1); row r goes to slot (r - j0 + 1) % kNsiRing
+    int s_next = 0, r_next = j0 - 1;
+    auto issue = [&]() {
+        if (r_next <= j1) {
+            const int rr = r_next < 0 ? r_next + g.ny : (r_next >= g.ny ? r_next - g.ny : r_next);
+            const int64_t ro = int64_t(rr) * nx;
+            float* sl = ring + s_next * kRow;
+            if (active) {
+                nsi_cp16(sl + 4 + lane * 4, U + ro + c0);
+                nsi_cp16(sl + kField + 4 + lane * 4, V + ro + c0);
+                nsi_cp16(sl + 2 * kField + 4 + lane * 4, P + ro + c0);
+            }
+            if (lane == 0) {
+                nsi_cp4(sl + 3, U + ro + lcol);
+                nsi_cp4(sl + kField + 3, V + ro + lcol);
+                nsi_cp4(sl + 2 * kField + 3, P + ro + lcol);
+            }
+            if (last) {
+                nsi_cp4(sl + 4 + scols, U + ro + rcol);
+                nsi_cp4(sl + kField + 4 + scols, V + ro + rcol);
+                nsi_cp4(sl + 2 * kField + 4 + scols, P + ro + rcol);
             }
         }
         nsi_commit();
+        ++r_next;
+        s_next = s_next + 1 == kNsiRing ? 0 : s_next + 1;
     };
 #pragma unroll 1
-    for (int q = 0; q < kNsiRing - 1; ++q) issue(j0 - 1 + q);
+    for (int q = 0; q < kNsiRing - 1; ++q) issue();
     const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
+    int sS = 0, sC = 1, sN = 2;  // the slots of rows j-1, j, j+1
 #pragma unroll 1
     for (int j = j0; j < j1; ++j) {
-        issue(j + kNsiRing - 2);  // into the slot row j-2 left (free since the last iteration's __syncwarp)
+        issue();  // row j+kNsiRing-2, into the slot row j-2 left (free since the last iteration's __syncwarp)
         // issued: rows j0-1 .. j+kNsiRing-2, one group each; rows up to j+1 must have landed (for this lane)
         nsi_wait<kNsiRing - 3>();
-        __syncwarp();              // and every lane's copies are visible to the warp
+        __syncwarp();  // and every lane's copies are visible to the warp
         if (active) {
+            const float* a = mine + sC * kRow;
+            const float* mS = mine + sS * kRow;
+            const float* mN = mine + sN * kRow;
             float cu[6], cv[6], cp[6];  // W, 4 cells, E of row j
             float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
             {
-                const float* a = slot(j, 0) + 4 + lane * 4;
-                const float* b = slot(j, 1) + 4 + lane * 4;
-                const float* c = slot(j, 2) + 4 + lane * 4;
-                const float4 ua = *reinterpret_cast<const float4*>(a), va = *reinterpret_cast<const float4*>(b),
-                             pa = *reinterpret_cast<const float4*>(c);
+                const float4 ua = *reinterpret_cast<const float4*>(a);
+                const float4 va = *reinterpret_cast<const float4*>(a + kField);
+                const float4 pa = *reinterpret_cast<const float4*>(a + 2 * kField);
                 cu[0] = a[-1]; cu[1] = ua.x; cu[2] = ua.y; cu[3] = ua.z; cu[4] = ua.w; cu[5] = a[4];
-                cv[0] = b[-1]; cv[1] = va.x; cv[2] = va.y; cv[3] = va.z; cv[4] = va.w; cv[5] = b[4];
-                cp[0] = c[-1]; cp[1] = pa.x; cp[2] = pa.y; cp[3] = pa.z; cp[4] = pa.w; cp[5] = c[4];
-                const float4 us = *reinterpret_cast<const float4*>(slot(j - 1, 0) + 4 + lane * 4);
-                const float4 un = *reinterpret_cast<const float4*>(slot(j + 1, 0) + 4 + lane * 4);
-                const float4 vs = *reinterpret_cast<const float4*>(slot(j - 1, 1) + 4 + lane * 4);
-                const float4 vn = *reinterpret_cast<const float4*>(slot(j + 1, 1) + 4 + lane * 4);
-                const float4 ps = *reinterpret_cast<const float4*>(slot(j - 1, 2) + 4 + lane * 4);
-                const float4 pn = *reinterpret_cast<const float4*>(slot(j + 1, 2) + 4 + lane * 4);
+                cv[0] = a[kField - 1]; cv[1] = va.x; cv[2] = va.y; cv[3] = va.z; cv[4] = va.w; cv[5] = a[kField + 4];
+                cp[0] = a[2 * kField - 1]; cp[1] = pa.x; cp[2] = pa.y; cp[3] = pa.z; cp[4] = pa.w;
+                cp[5] = a[2 * kField + 4];
+                const float4 us = *reinterpret_cast<const float4*>(mS);
+                const float4 un = *reinterpret_cast<const float4*>(mN);
+                const float4 vs = *reinterpret_cast<const float4*>(mS + kField);
+                const float4 vn = *reinterpret_cast<const float4*>(mN + kField);
+                const float4 ps = *reinterpret_cast<const float4*>(mS + 2 * kField);
+                const float4 pn = *reinterpret_cast<const float4*>(mN + 2 * kField);
                 uS[0] = us.x; uS[1] = us.y; uS[2] = us.z; uS[3] = us.w;
                 uN[0] = un.x; uN[1] = un.y; uN[2] = un.z; uN[3] = un.w;
                 vS[0] = vs.x; vS[1] = vs.y; vS[2] = vs.z; vS[3] = vs.w;
@@ -176,6 +196,7 @@ __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float
                 pN[0] = pn.x; pN[1] = pn.y; pN[2] = pn.z; pN[3] = pn.w;
             }
             float oru[4], orv[4], orc[4];
+            float qu = 0.f, qv = 0.f, qc = 0.f;  // the lane's 4 squares in f32, then one f64 addition per norm
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const float uc = cu[e + 1], vc = cv[e + 1];
@@ -191,16 +212,22 @@ __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float
                 const float rv = ((uc * dvdx + vc * dvdy) + dpdy) - nu * lapv;
                 const float rc = dudx + dvdy;
                 oru[e] = ru; orv[e] = rv; orc[e] = rc;
-                su = __fma_rn(double(ru), double(ru), su);
-                sv = __fma_rn(double(rv), double(rv), sv);
-                sc = __fma_rn(double(rc), double(rc), sc);
+                qu = fmaf(ru, ru, qu);
+                qv = fmaf(rv, rv, qv);
+                qc = fmaf(rc, rc, qc);
             }
+            su += double(qu);
+            sv += double(qv);
+            sc += double(qc);
             const int64_t ro = int64_t(j) * nx + c0;
             st_f4(g.ru + ro, make_float4(oru[0], oru[1], oru[2], oru[3]));
             st_f4(g.rv + ro, make_float4(orv[0], orv[1], orv[2], orv[3]));
             st_f4(g.rc + ro, make_float4(orc[0], orc[1], orc[2], orc[3]));
         }
         __syncwarp();  // every lane is done with row j-1's slot before the next iteration refills it
+        sS = sC;
+        sC = sN;
+        sN = sN + 1 == kNsiRing ? 0 : sN + 1;
     }
     nsi_wait<0>();
     __syncwarp();
@@ -337,10 +364,23 @@ __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
+// The row-strip height H of a grid: the one whose block count best fills whole waves of kNsiWave blocks (4 per SM on
+// the 148 SMs of a B200; a constant, so that the decomposition and hence every sum depends on (nx, ny) alone), the
+// taller one on a tie. Small grids take the shortest strips (the most blocks).
+constexpr int64_t kNsiWave = 4 * 148;
 __host__ __device__ inline void nsi_shape(int nx, int ny, int vec, int& H, int& segs, int64_t& items, int64_t& blocks) {
     segs = (nx + 32 * vec - 1) / (32 * vec);
+    int64_t best_b = 0, best_w = 1;
     H = 32;
-    while (H > 4 && int64_t(segs) * ((ny + H - 1) / H) < 4096) H /= 2;
+    for (int h = 32; h >= 4; h -= 4) {
+        const int64_t b = (int64_t(segs) * ((ny + h - 1) / h) + kNsiWarps - 1) / kNsiWarps;
+        const int64_t w = (b + kNsiWave - 1) / kNsiWave;
+        if (b * best_w > best_b * w) {  // a higher fill b / (w · wave)
+            best_b = b;
+            best_w = w;
+            H = h;
+        }
+    }
     items = int64_t(segs) * ((ny + H - 1) / H);
     blocks = (items + kNsiWarps - 1) / kNsiWarps;
 }
