@@ -22,6 +22,8 @@ from .build import ARCH, nvcc
 PKG = Path(__file__).resolve().parent
 # a host-only function called from device code (nvcc's diagnostic 20011) would run nothing on the GPU: make it an error
 STRICT = ["--diag-error=20011,20014"]
+# the runtime's fast paths call libcspb through include/cspb.h; the binaries find the library next to _examples/
+LINK = ["-I", str(PKG.parent / "include"), "-L", str(PKG), "-lcspb", "-Xlinker", "-rpath", "-Xlinker", "$ORIGIN/.."]
 OUT = PKG / "_examples"
 PROGRAMS = {
     "gemver-chain": ("examples/gemver-chain", "main.cpp"),
@@ -41,7 +43,7 @@ def build_examples(reference: str | os.PathLike | None = None, verbose: bool = F
         annotate_tree(ref / sub, src)
         exe = OUT / name
         cmd = [nvcc(), "-std=c++20", "-O2", *ARCH, "-I", str(PKG / "include"), "--extended-lambda",
-               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src / main), "-o", str(exe)]
+               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src / main), *LINK, "-o", str(exe)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         procs.append((name, exe, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
@@ -68,7 +70,7 @@ def build_runtime_tests(verbose: bool = False) -> dict[str, Path]:
     for name, src in RUNTIME_TESTS.items():
         exe = OUT / name
         cmd = [nvcc(), "-std=c++20", "-O2", *ARCH, "-I", str(PKG / "include"), "--extended-lambda",
-               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src_dir / src), "-o", str(exe)]
+               "--expt-relaxed-constexpr", *STRICT, "-x", "cu", str(src_dir / src), *LINK, "-o", str(exe)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

@@ -57,6 +57,7 @@ struct Var {
     std::optional<InitSpec> init;
     bool stale = false;
     bool produced = false;
+    std::uint64_t version = 0;        // incremented whenever an initializer writes the variable
     std::size_t elements() const {
         std::size_t n = 1;
         for (int d = 0; d < rank; ++d) n *= shape[d];
@@ -84,7 +85,8 @@ public:
     std::map<std::string, std::string> tie_keys;  // system path + "/" + alias -> tie key
     std::vector<std::function<bool(Runtime&, std::size_t&)>> pattern_runs;  // per leaf index: a fast path
     std::vector<int> pattern_at;             // leaf index -> pattern index or -1 (-2: covered, skip)
-    std::vector<struct PatternRec*> pattern_recs;
+    std::vector<std::size_t> pattern_hi;     // per pattern: the last leaf it covers
+    std::vector<std::shared_ptr<void>> pattern_state;  // what the fast paths keep between runs (workspaces, scales)
     int sms = 0;
     bool trace = false;  // NAGA_COSPAN_TRACE set: every launch and initializer is printed to stderr
 
@@ -99,6 +101,8 @@ public:
     }
     ~Runtime() {
         cudaStreamSynchronize(stream);
+        pattern_runs.clear();
+        pattern_state.clear();
         for (auto& v : vars)
             if (v.data) cudaFree(v.data);
         if (ctrl) cudaFree(ctrl);
@@ -177,6 +181,7 @@ public:
             InitTarget t{*this, v};
             v.init->run(t);
             v.stale = false;
+            ++v.version;
             if (trace) std::fprintf(stderr, "[cospan] init var %d '%s' at %p (%zu elements)\n", v.id, v.name.c_str(), v.data,
                                     v.elements());
         }
@@ -627,16 +632,24 @@ public:
     void run() {
         finalize();
         auto& rt = *rt_;
+        auto run_leaf = [&](std::size_t i) {
+            Node* n = rt.leaves[i];
+            if (n->kind == Node::Kind::component) rt.run_component(static_cast<ComponentBase*>(n));
+            else static_cast<FusedGroupBase*>(n)->launch(rt);
+        };
         for (std::size_t i = 0; i < rt.leaves.size(); ++i) {
             const int pat = rt.pattern_at.empty() ? -1 : rt.pattern_at[i];
             if (pat == -2) continue;
             if (pat >= 0) {
                 std::size_t next = i;
                 if (rt.pattern_runs[std::size_t(pat)](rt, next)) continue;
+                // the fast path declined this run: the leaves it covers run their own bodies
+                const std::size_t hi = rt.pattern_hi[std::size_t(pat)];
+                for (std::size_t k = i; k <= hi; ++k) run_leaf(k);
+                i = hi;
+                continue;
             }
-            Node* n = rt.leaves[i];
-            if (n->kind == Node::Kind::component) rt.run_component(static_cast<ComponentBase*>(n));
-            else static_cast<FusedGroupBase*>(n)->launch(rt);
+            run_leaf(i);
         }
         for (auto& v : rt.views) push(*v);
     }

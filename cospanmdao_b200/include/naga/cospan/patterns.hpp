@@ -1,8 +1,300 @@
-// naga/cospan/patterns.hpp — leaves that run as one cspb kernel (filled in below the generic path).
+// naga/cospan/patterns.hpp — leaves that run as one cspb kernel instead of their own component bodies.
+//
+// At finalize, the runtime looks through its leaves (solo components and fused groups, in run order) for runs of
+// components that together compute something a cspb kernel computes in fewer passes over memory, and registers a fast
+// path for them: the first leaf of the run calls the kernel through the C ABI (include/cspb.h), the others are
+// skipped. Everything else still runs its own bodies. A run is recognised by its component types and by its wiring
+// (which ports share a variable), never by names or paths, so every style that the reference's gemver-chain example
+// builds (unfused, parallel, fused, naive, onepass, crafted) lands on the same kernel:
+//
+//   GEMVER   Rank2Update | Rank2UpdateLocal → GemvTPartial | GemvTPartialLocal → ColReduce<true> → Gemv
+//            (examples/gemver-chain/components.hpp:85-265, :366-470)             → cspb_gemver_fused
+//   BiCGK    BicgkOnePass → RowReduce → ColReduce<false>   (components.hpp:277-358) → cspb_bicgk_fused
+//            Gemv → GemvTPartial → ColReduce<false>        (the unfused / parallel / fused BiCGK)
+//
+// The kernel writes the run's outputs (B, x, w; q, s); the partial-sum variables between the run's components (P, Pq,
+// Ps) are not written, so a run whose partials something else reads, or whose scale is itself computed, is left to
+// the generic path. The scales (the reference's `scale` inputs: α = β = 1/√n in the chain) are read from their device
+// variables once per initialisation. NAGA_COSPAN_GENERIC set in the environment turns every fast path off.
 #pragma once
 
+#include <cstdlib>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cspb.h"
 #include "model.hpp"
 
 namespace naga::cospan::detail {
-inline void register_patterns(Runtime& rt) { rt.pattern_at.assign(rt.leaves.size(), -1); }
+
+// "gc::ColReduce<true>" -> "ColReduce<true>"
+inline std::string short_type(const ComponentBase* c) {
+    const std::string& t = c->type_name_;
+    const std::size_t lt = t.find('<');
+    const std::size_t cut = t.rfind("::", lt == std::string::npos ? std::string::npos : lt);
+    return cut == std::string::npos ? t : t.substr(cut + 2);
+}
+
+inline bool has_port(const ComponentBase* c, const char* name) {
+    for (auto& p : c->ports_)
+        if (p.name == name) return true;
+    return false;
+}
+
+struct PatternLeaves {
+    std::vector<ComponentBase*> comps;  // the components of every leaf, in run order
+    std::vector<std::size_t> leaf_of;   // comps[i] runs in leaf leaf_of[i]
+    std::vector<std::size_t> first;     // the first component of each leaf (leaves.size() + 1 entries)
+};
+
+inline PatternLeaves pattern_leaves(Runtime& rt) {
+    PatternLeaves L;
+    for (std::size_t i = 0; i < rt.leaves.size(); ++i) {
+        L.first.push_back(L.comps.size());
+        Node* n = rt.leaves[i];
+        if (n->kind == Node::Kind::component) {
+            L.comps.push_back(static_cast<ComponentBase*>(n));
+            L.leaf_of.push_back(i);
+        } else {
+            for (ComponentBase* c : static_cast<FusedGroupBase*>(n)->stages_) {
+                L.comps.push_back(c);
+                L.leaf_of.push_back(i);
+            }
+        }
+    }
+    L.first.push_back(L.comps.size());
+    return L;
+}
+
+// The state a fast path keeps: its workspace and the host copies of its scales.
+struct FastState {
+    std::vector<int> internal;  // the run's partial-sum variables (not written by the kernel)
+    void* ws = nullptr;
+    std::size_t ws_bytes = 0;
+    std::vector<int> scale_vars;
+    std::vector<std::uint64_t> scale_version;
+    std::vector<float> scale;
+    ~FastState() {
+        if (ws) cudaFree(ws);
+    }
+    // false when the host now views one of the partials (the generic path writes them)
+    bool partials_unviewed(const Runtime& rt) const {
+        for (auto& v : rt.views)
+            for (int iv : internal)
+                if (v->var == iv) return false;
+        return true;
+    }
+    void* workspace(std::size_t bytes) {
+        if (bytes > ws_bytes) {
+            if (ws) cudaFree(ws);
+            ws = nullptr;
+            cuda_check(cudaMalloc(&ws, bytes), "fast-path workspace");
+            ws_bytes = bytes;
+        }
+        return ws;
+    }
+    // the current value of every scale variable (a device read only after an initializer wrote it again)
+    void refresh(Runtime& rt) {
+        for (std::size_t k = 0; k < scale_vars.size(); ++k) {
+            Var& v = rt.vars[std::size_t(scale_vars[k])];
+            if (v.version == scale_version[k]) continue;
+            float h = 0.f;
+            cuda_check(cudaStreamSynchronize(rt.stream), "scale");
+            cuda_check(cudaMemcpy(&h, v.data, sizeof(float), cudaMemcpyDeviceToHost), "scale");
+            scale[k] = h;
+            scale_version[k] = v.version;
+        }
+    }
+};
+
+inline int var_id(Runtime& rt, ComponentBase* c, const char* port) {
+    auto it = rt.key_var.find(c->path() + "." + port);
+    return it == rt.key_var.end() ? -1 : it->second;
+}
+
+// Whether a component outside `run` touches one of the `internal` variables (host views are checked at run time).
+inline bool internal_escapes(Runtime& rt, const std::vector<ComponentBase*>& run, const std::vector<int>& internal) {
+    for (ComponentBase* c : rt.components) {
+        bool inside = false;
+        for (ComponentBase* r : run) inside = inside || r == c;
+        if (inside) continue;
+        for (auto& p : c->ports_)
+            for (int v : internal)
+                if (p.var == v) return true;
+    }
+    return false;
+}
+
+// The leaves [lo, hi] must hold exactly the components comps[a .. a + k).
+inline bool whole_leaves(const PatternLeaves& L, std::size_t a, std::size_t k, std::size_t& lo, std::size_t& hi) {
+    lo = L.leaf_of[a];
+    hi = L.leaf_of[a + k - 1];
+    return L.first[lo] == a && L.first[hi + 1] == a + k;
+}
+
+inline void fast_fail(int st, const std::string& what) {
+    if (st == CSPB_OK) return;
+    const std::string m = "naga::cospan: " + what + ": " + cspb_status_string(st);
+    if (st == CSPB_ERR_ARGUMENT || st == CSPB_ERR_UNSUPPORTED || st == CSPB_ERR_WORKSPACE) throw std::invalid_argument(m);
+    throw std::runtime_error(m);
+}
+
+inline bool scale_is_input(Runtime& rt, int v) {
+    return v >= 0 && !rt.vars[std::size_t(v)].produced && rt.vars[std::size_t(v)].dtype == DType::f32;
+}
+
+// ---- GEMVER --------------------------------------------------------------------------------------------------------
+inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    if (a + 4 > L.comps.size()) return false;
+    ComponentBase *r2u = L.comps[a], *gtp = L.comps[a + 1], *cred = L.comps[a + 2], *gemv = L.comps[a + 3];
+    const std::string t0 = short_type(r2u), t1 = short_type(gtp);
+    if (!(t0 == "Rank2Update" || t0 == "Rank2UpdateLocal") || !(t1 == "GemvTPartial" || t1 == "GemvTPartialLocal") ||
+        short_type(cred) != "ColReduce<true>" || short_type(gemv) != "Gemv")
+        return false;
+    const int vB = var_id(rt, r2u, "B"), vP = var_id(rt, gtp, "P");
+    if (vB < 0 || var_id(rt, gemv, "B") != vB || var_id(rt, cred, "P") != vP || var_id(rt, cred, "x") != var_id(rt, gemv, "x"))
+        return false;
+    if (has_port(gtp, "B") && var_id(rt, gtp, "B") != vB) return false;  // the local variant takes B from its tile
+    const int vbeta = var_id(rt, cred, "scale"), valpha = var_id(rt, gemv, "scale");
+    if (!scale_is_input(rt, vbeta) || !scale_is_input(rt, valpha)) return false;
+    std::size_t lo, hi;
+    if (!whole_leaves(L, a, 4, lo, hi)) return false;
+    if (internal_escapes(rt, {r2u, gtp, cred, gemv}, {vP})) return false;
+
+    auto st = std::make_shared<FastState>();
+    st->internal = {vP};
+    st->scale_vars = {vbeta, valpha};
+    st->scale_version = {~0ull, ~0ull};
+    st->scale = {0.f, 0.f};
+    rt.pattern_state.push_back(st);
+    const int pat = int(rt.pattern_runs.size());
+    rt.pattern_runs.push_back([st, r2u, gtp, cred, gemv](Runtime& rt, std::size_t&) {
+        if (!st->partials_unviewed(rt)) return false;
+        for (ComponentBase* c : {r2u, gtp, cred, gemv}) rt.prepare(c);
+        Var& A = rt.var_of_port(r2u, "A");
+        if (A.rank != 2 || A.shape[0] != A.shape[1]) return false;
+        const std::int64_t n = std::int64_t(A.shape[0]);
+        st->refresh(rt);
+        cspb_gemver_desc d{};
+        d.n = n;
+        d.lda = n;
+        d.ldb = n;
+        d.a_dtype = CSPB_F32;
+        d.A = A.data;
+        d.u1 = static_cast<const float*>(rt.var_of_port(r2u, "u1").data);
+        d.v1 = static_cast<const float*>(rt.var_of_port(r2u, "v1").data);
+        d.u2 = static_cast<const float*>(rt.var_of_port(r2u, "u2").data);
+        d.v2 = static_cast<const float*>(rt.var_of_port(r2u, "v2").data);
+        d.y = static_cast<const float*>(rt.var_of_port(gtp, "y").data);
+        d.z = static_cast<const float*>(rt.var_of_port(cred, "z").data);
+        d.beta = st->scale[0];
+        d.alpha = st->scale[1];
+        d.B = static_cast<float*>(rt.var_of_port(r2u, "B").data);
+        d.x = static_cast<float*>(rt.var_of_port(cred, "x").data);
+        d.w = static_cast<float*>(rt.var_of_port(gemv, "y").data);
+        d.workspace_bytes = cspb_gemver_workspace_bytes(n);
+        d.workspace = st->workspace(d.workspace_bytes);
+        if (rt.trace)
+            std::fprintf(stderr, "[cospan] fast path cspb_gemver_fused n=%lld for '%s' .. '%s'\n", (long long)n,
+                         r2u->path().c_str(), gemv->path().c_str());
+        fast_fail(cspb_gemver_fused(&d, rt.stream), "'" + r2u->path() + "' (GEMVER fast path)");
+        return true;
+    });
+    rt.pattern_hi.push_back(hi);
+    rt.pattern_at[lo] = pat;
+    for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+    return true;
+}
+
+// ---- BiCGK ---------------------------------------------------------------------------------------------------------
+inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    if (a + 3 > L.comps.size()) return false;
+    ComponentBase *c0 = L.comps[a], *c1 = L.comps[a + 1], *c2 = L.comps[a + 2];
+    if (short_type(c2) != "ColReduce<false>") return false;
+    const std::string t0 = short_type(c0), t1 = short_type(c1);
+    int vB, vp, vr, vq, vs, vscale_q = -1;
+    std::vector<int> internal;
+    if (t0 == "BicgkOnePass" && t1 == "RowReduce") {
+        vB = var_id(rt, c0, "B");
+        vp = var_id(rt, c0, "p");
+        vr = var_id(rt, c0, "r");
+        if (var_id(rt, c1, "Pq") != var_id(rt, c0, "Pq") || var_id(rt, c2, "P") != var_id(rt, c0, "Ps")) return false;
+        vq = var_id(rt, c1, "q");
+        internal = {var_id(rt, c0, "Pq"), var_id(rt, c0, "Ps")};
+    } else if (t0 == "Gemv" && t1 == "GemvTPartial") {
+        vB = var_id(rt, c0, "B");
+        if (var_id(rt, c1, "B") != vB || var_id(rt, c2, "P") != var_id(rt, c1, "P")) return false;
+        vp = var_id(rt, c0, "x");
+        vr = var_id(rt, c1, "y");
+        vq = var_id(rt, c0, "y");
+        vscale_q = var_id(rt, c0, "scale");
+        internal = {var_id(rt, c1, "P")};
+        if (!scale_is_input(rt, vscale_q)) return false;
+    } else {
+        return false;
+    }
+    vs = var_id(rt, c2, "x");
+    const int vscale_s = var_id(rt, c2, "scale");
+    if (vB < 0 || vp < 0 || vr < 0 || vq < 0 || vs < 0 || !scale_is_input(rt, vscale_s)) return false;
+    std::size_t lo, hi;
+    if (!whole_leaves(L, a, 3, lo, hi)) return false;
+    if (internal_escapes(rt, {c0, c1, c2}, internal)) return false;
+
+    auto st = std::make_shared<FastState>();
+    st->internal = internal;
+    st->scale_vars = {vscale_s};
+    if (vscale_q >= 0) st->scale_vars.push_back(vscale_q);
+    st->scale_version.assign(st->scale_vars.size(), ~0ull);
+    st->scale.assign(st->scale_vars.size(), 0.f);
+    rt.pattern_state.push_back(st);
+    const int pat = int(rt.pattern_runs.size());
+    rt.pattern_runs.push_back([st, c0, c1, c2, vB, vp, vr, vq, vs](Runtime& rt, std::size_t&) {
+        if (!st->partials_unviewed(rt)) return false;
+        for (ComponentBase* c : {c0, c1, c2}) rt.prepare(c);
+        st->refresh(rt);
+        for (float s : st->scale)
+            if (s != 1.0f) return false;  // the kernel forms q = B·p and s = Bᵀ·r unscaled
+        Var& B = rt.vars[std::size_t(vB)];
+        if (B.rank != 2 || B.shape[0] != B.shape[1]) return false;
+        const std::int64_t n = std::int64_t(B.shape[0]);
+        cspb_bicgk_desc d{};
+        d.n = n;
+        d.ldb = n;
+        d.b_dtype = CSPB_F32;
+        d.B = B.data;
+        d.p = static_cast<const float*>(rt.vars[std::size_t(vp)].data);
+        d.r = static_cast<const float*>(rt.vars[std::size_t(vr)].data);
+        d.q = static_cast<float*>(rt.vars[std::size_t(vq)].data);
+        d.s = static_cast<float*>(rt.vars[std::size_t(vs)].data);
+        d.workspace_bytes = cspb_bicgk_workspace_bytes(n);
+        d.workspace = st->workspace(d.workspace_bytes);
+        if (rt.trace)
+            std::fprintf(stderr, "[cospan] fast path cspb_bicgk_fused n=%lld for '%s' .. '%s'\n", (long long)n,
+                         c0->path().c_str(), c2->path().c_str());
+        fast_fail(cspb_bicgk_fused(&d, rt.stream), "'" + c0->path() + "' (BiCGK fast path)");
+        return true;
+    });
+    rt.pattern_hi.push_back(hi);
+    rt.pattern_at[lo] = pat;
+    for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+    return true;
+}
+
+inline void register_patterns(Runtime& rt) {
+    rt.pattern_at.assign(rt.leaves.size(), -1);
+    rt.pattern_hi.clear();
+    if (std::getenv("NAGA_COSPAN_GENERIC")) return;
+    const PatternLeaves L = pattern_leaves(rt);
+    for (std::size_t a = 0; a < L.comps.size();) {
+        if (L.first[L.leaf_of[a]] != a || rt.pattern_at[L.leaf_of[a]] != -1) {  // runs start on a leaf boundary
+            ++a;
+            continue;
+        }
+        if (try_gemver(rt, L, a)) a += 4;
+        else if (try_bicgk(rt, L, a)) a += 3;
+        else ++a;
+    }
+}
+
 }  // namespace naga::cospan::detail

@@ -2,6 +2,7 @@
 this package's cs:: runtime (cospanmdao_b200.examples) and run with their own --check: every variant must report
 ALL OK against the reference's host FP64 oracles (and, for gemver-chain, the variants must agree with each other the
 way the reference requires: bitwise for unfused / parallel / fused)."""
+import os
 import subprocess
 from pathlib import Path
 
@@ -12,13 +13,19 @@ pytestmark = pytest.mark.gpu
 EX = Path(__file__).resolve().parents[1] / "cospanmdao_b200" / "_examples"
 
 
-def _run(args, timeout=300):
+def _run(args, timeout=300, env=None):
     exe = EX / args[0]
     if not exe.exists():
         pytest.fail(f"{exe} was not built (python -m cospanmdao_b200.examples)")
+    full_env = dict(os.environ, **(env or {}))
     r = subprocess.run([str(exe), *args[1:]], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
-                       timeout=timeout)
+                       timeout=timeout, env=full_env)
     return r.returncode, r.stdout
+
+
+# "fast": the runtime's registered fast paths (patterns.hpp) run the GEMVER and BiCGK stages as cspb kernels;
+# "generic": every component runs its own body (NAGA_COSPAN_GENERIC)
+MODES = {"fast": {}, "generic": {"NAGA_COSPAN_GENERIC": "1"}}
 
 
 def test_runtime_fused_groups(cuda):
@@ -34,17 +41,35 @@ def test_getting_started(cuda):
     assert out.split() == ["3", "5", "7", "9"], out
 
 
+@pytest.mark.parametrize("mode", sorted(MODES))
 @pytest.mark.parametrize("variant", ["unfused", "parallel", "fused", "onepass", "naive", "crafted"])
-def test_gemver_chain_variant(cuda, variant):
+def test_gemver_chain_variant(cuda, variant, mode):
     rc, out = _run(["gemver-chain", "--n", "1024", "--R", "64", "--iters", "2", "--warmup", "1", "--variant", variant,
-                    "--check"])
+                    "--check"], env=MODES[mode])
     assert rc == 0 and "ALL OK" in out, out
 
 
-def test_gemver_chain_all_variants_agree(cuda):
-    rc, out = _run(["gemver-chain", "--n", "512", "--R", "64", "--iters", "1", "--warmup", "1", "--check"])
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_gemver_chain_all_variants_agree(cuda, mode):
+    rc, out = _run(["gemver-chain", "--n", "512", "--R", "64", "--iters", "1", "--warmup", "1", "--check"],
+                   env=MODES[mode])
     assert rc == 0 and "ALL OK" in out, out
     assert out.count("bitwise equal") >= 2, out
+
+
+def test_gemver_chain_fast_paths_engage(cuda):
+    """Every style's GEMVERs and BiCGK run as cspb kernels (the crafted chain's middle group and G2 keep their own
+    bodies: their stages split a GEMVER across groups)."""
+    for variant, want_g, want_b in (("unfused", 2, 1), ("parallel", 2, 1), ("fused", 2, 1), ("onepass", 2, 1),
+                                    ("naive", 2, 1), ("crafted", 1, 0)):
+        rc, out = _run(["gemver-chain", "--n", "512", "--R", "64", "--iters", "1", "--warmup", "1", "--variant",
+                        variant], env={"NAGA_COSPAN_TRACE": "1"})
+        assert rc == 0, out
+        assert out.count("fast path cspb_gemver_fused") >= want_g, (variant, out[-2000:])
+        if want_b:
+            assert out.count("fast path cspb_bicgk_fused") >= want_b, (variant, out[-2000:])
+        else:
+            assert "fast path cspb_bicgk_fused" not in out, (variant, out[-2000:])
 
 
 @pytest.mark.parametrize("bc", ["walls", "periodic"])
