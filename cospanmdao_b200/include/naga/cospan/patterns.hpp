@@ -11,6 +11,9 @@
 //            (examples/gemver-chain/components.hpp:85-265, :366-470)             → cspb_gemver_fused
 //   BiCGK    BicgkOnePass → RowReduce → ColReduce<false>   (components.hpp:277-358) → cspb_bicgk_fused
 //            Gemv → GemvTPartial → ColReduce<false>        (the unfused / parallel / fused BiCGK)
+//   NS       the 19 stages of NsFused or the 18 components of NsUnfused (examples/ns-residual/systems.hpp:31-140,
+//            components.hpp:100-852), either limiter and boundary  → cspb_ns_compressible, whose 18 diagnostics
+//            are then copied into the Dt, Ws, Sq, Det and Err variables
 //
 // The kernel writes the run's outputs (B, x, w; q, s); the partial-sum variables between the run's components (P, Pq,
 // Ps) are not written, so a run whose partials something else reads, or whose scale is itself computed, is left to
@@ -18,6 +21,7 @@
 // variables once per initialisation. NAGA_COSPAN_GENERIC set in the environment turns every fast path off.
 #pragma once
 
+#include <algorithm>
 #include <cstdlib>
 #include <memory>
 #include <string>
@@ -281,6 +285,125 @@ inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
     return true;
 }
 
+
+// ---- NS residual (compressible) ------------------------------------------------------------------------------------
+// A stage's role: its type with the limiter / boundary argument dropped ("Reconstruct<nsr::MinMod>" -> "Reconstruct<>").
+inline std::string ns_role(const ComponentBase* c, int& lim, int& walls) {
+    std::string t = short_type(c);
+    const std::size_t lt = t.find('<');
+    if (lt != std::string::npos) {
+        const std::string arg = t.substr(lt + 1);
+        if (arg.find("MinMod") != std::string::npos) { lim = 0; return t.substr(0, lt) + "<>"; }
+        if (arg.find("VanLeer") != std::string::npos) { lim = 1; return t.substr(0, lt) + "<>"; }
+        if (arg.find("BcWalls") != std::string::npos) { walls = 1; return t.substr(0, lt) + "<>"; }
+        if (arg.find("BcPeriodic") != std::string::npos) { walls = 0; return t.substr(0, lt) + "<>"; }
+    }
+    return t;
+}
+
+inline bool try_ns(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    static const std::vector<std::string> fused = {
+        "InitDiagnostics", "LoadTile", "ApplyBoundary<>", "ToPrimitive", "Gradients", "Reconstruct<>", "ConvFlux<0>",
+        "ConvFlux<1>", "ViscFlux<0>", "ViscFlux<1>", "ConvDivergence<true>", "ViscDivergence", "LocalTimestep<true>",
+        "WaveSpeed<true>", "ResidualSquares<true>", "DetNorm", "DetExtreme<true>", "DetExtreme<false>",
+        "ErrorStage<true>"};
+    static const std::vector<std::string> unfused = {
+        "InitDiagnostics", "PadBoundary<>", "ToPrimitiveG", "GradientsG", "ReconstructG<>", "ConvFluxG<0>",
+        "ConvFluxG<1>", "ViscFluxG<0>", "ViscFluxG<1>", "ConvDivergence<false>", "ViscDivergenceChained",
+        "LocalTimestep<false>", "WaveSpeed<false>", "ResidualSquares<false>", "DetNorm", "DetExtreme<true>",
+        "DetExtreme<false>", "ErrorStage<false>"};
+    int lim = -1, walls = -1;
+    for (const auto* fam : {&fused, &unfused}) {
+        const std::size_t k = fam->size();
+        if (a + k > L.comps.size()) continue;
+        std::vector<std::string> got;
+        std::vector<ComponentBase*> run(L.comps.begin() + std::ptrdiff_t(a), L.comps.begin() + std::ptrdiff_t(a + k));
+        for (ComponentBase* c : run) got.push_back(ns_role(c, lim, walls));
+        std::vector<std::string> want = *fam;
+        std::sort(got.begin(), got.end());
+        std::sort(want.begin(), want.end());
+        if (got != want || lim < 0 || walls < 0) continue;
+        std::size_t lo, hi;
+        if (!whole_leaves(L, a, k, lo, hi)) return false;
+        auto find = [&](const std::string& role) -> ComponentBase* {
+            int l2 = lim, w2 = walls;
+            for (ComponentBase* c : run)
+                if (ns_role(c, l2, w2) == role) return c;
+            return nullptr;
+        };
+        ComponentBase* init = find("InitDiagnostics");
+        ComponentBase* load = find(fam == &fused ? "LoadTile" : "PadBoundary<>");
+        ComponentBase* vdiv = find(fam == &fused ? "ViscDivergence" : "ViscDivergenceChained");
+        ComponentBase* detn = find("DetNorm");
+        ComponentBase* detd = find("DetExtreme<true>");
+        ComponentBase* detw = find("DetExtreme<false>");
+        ComponentBase* err = find(fam == &fused ? "ErrorStage<true>" : "ErrorStage<false>");
+        const int vU = var_id(rt, load, "U"), vR = var_id(rt, vdiv, "R");
+        const std::vector<int> outs = {var_id(rt, init, "Dt"), var_id(rt, init, "Ws"), var_id(rt, init, "Sq"),
+                                       var_id(rt, detn, "Det"), var_id(rt, detd, "Det"), var_id(rt, detw, "Det"),
+                                       var_id(rt, err, "Err")};
+        if (vU < 0 || vR < 0) return false;
+        for (int v : outs)
+            if (v < 0) return false;
+        // every other variable the run touches is internal (fluxes, primitives, partials): nothing else may use it
+        std::vector<int> internal;
+        for (ComponentBase* c : run)
+            for (auto& pr : c->ports_) {
+                const int v = pr.var;
+                bool keep = v == vU || v == vR || var_id(rt, c, "geo") == v;
+                for (int o : outs) keep = keep || o == v;
+                if (!keep && std::find(internal.begin(), internal.end(), v) == internal.end()) internal.push_back(v);
+            }
+        if (internal_escapes(rt, run, internal)) return false;
+
+        auto st = std::make_shared<FastState>();
+        st->internal = internal;
+        rt.pattern_state.push_back(st);
+        const int pat = int(rt.pattern_runs.size());
+        rt.pattern_runs.push_back([st, run, vU, vR, outs, lim, walls](Runtime& rt, std::size_t&) {
+            if (!st->partials_unviewed(rt)) return false;
+            for (ComponentBase* c : run) rt.prepare(c);
+            Var& U = rt.vars[std::size_t(vU)];
+            Var& R = rt.vars[std::size_t(vR)];
+            if (U.rank != 3 || U.shape[0] != 4 || R.rank != 3 || R.shape != U.shape) return false;
+            const int ny = int(U.shape[1]), nx = int(U.shape[2]);
+            const std::size_t wsb = cspb_ns_comp_workspace_bytes(nx, ny);
+            // the kernel's workspace, then its 18 diagnostics
+            char* ws = static_cast<char*>(st->workspace((wsb + 255) / 256 * 256 + 256));
+            float* diag = reinterpret_cast<float*>(ws + (wsb + 255) / 256 * 256);
+            cspb_ns_comp_desc d{};
+            d.nx = nx;
+            d.ny = ny;
+            d.limiter = lim;
+            d.walls = walls;
+            d.U = static_cast<const float*>(U.data);
+            d.R = static_cast<float*>(R.data);
+            d.diag = diag;
+            d.det_sq64 = nullptr;
+            d.workspace = ws;
+            d.workspace_bytes = wsb;
+            if (rt.trace)
+                std::fprintf(stderr, "[cospan] fast path cspb_ns_compressible %dx%d for '%s' .. '%s'\n", nx, ny,
+                             run.front()->path().c_str(), run.back()->path().c_str());
+            fast_fail(cspb_ns_compressible(&d, rt.stream), "'" + run.front()->path() + "' (NS fast path)");
+            // diag: [0] Dt [1] Ws [2..5] Sq | [6..9] detn [10] detd [11] detw | [12..17] Err
+            const int at[7] = {0, 1, 2, 6, 10, 11, 12}, len[7] = {1, 1, 4, 4, 1, 1, 6};
+            for (int k = 0; k < 7; ++k) {
+                Var& o = rt.vars[std::size_t(outs[std::size_t(k)])];
+                if (o.elements() != std::size_t(len[k])) throw std::logic_error("naga::cospan: NS fast path: '" + o.name + "' has an unexpected size");
+                cuda_check(cudaMemcpyAsync(o.data, diag + at[k], std::size_t(len[k]) * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, rt.stream), "NS diagnostics");
+            }
+            return true;
+        });
+        rt.pattern_hi.push_back(hi);
+        rt.pattern_at[lo] = pat;
+        for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+        return true;
+    }
+    return false;
+}
+
 inline void register_patterns(Runtime& rt) {
     rt.pattern_at.assign(rt.leaves.size(), -1);
     rt.pattern_hi.clear();
@@ -293,6 +416,7 @@ inline void register_patterns(Runtime& rt) {
         }
         if (try_gemver(rt, L, a)) a += 4;
         else if (try_bicgk(rt, L, a)) a += 3;
+        else if (try_ns(rt, L, a)) a = L.first[std::size_t(rt.pattern_hi.back()) + 1];
         else ++a;
     }
 }

@@ -72,15 +72,25 @@ def test_gemver_chain_fast_paths_engage(cuda):
             assert "fast path cspb_bicgk_fused" not in out, (variant, out[-2000:])
 
 
+@pytest.mark.parametrize("mode", sorted(MODES))
 @pytest.mark.parametrize("bc", ["walls", "periodic"])
 @pytest.mark.parametrize("variant", ["unfused", "fused"])
-def test_ns_residual_variant(cuda, variant, bc):
+def test_ns_residual_variant(cuda, variant, bc, mode):
     rc, out = _run(["ns-residual", "--nx", "128", "--ny", "96", "--iters", "2", "--warmup", "1", "--variant", variant,
-                    "--bc", bc, "--check"])
+                    "--bc", bc, "--check"], env=MODES[mode])
     assert rc == 0 and "ALL OK" in out, out
 
 
-def test_ns_residual_vanleer_fused(cuda):
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_ns_residual_vanleer_fused(cuda, mode):
     rc, out = _run(["ns-residual", "--nx", "64", "--ny", "64", "--iters", "1", "--warmup", "1", "--variant", "fused",
-                    "--limiter", "vanleer", "--range-split", "all", "--check"])
+                    "--limiter", "vanleer", "--range-split", "all", "--check"], env=MODES[mode])
     assert rc == 0 and "ALL OK" in out, out
+
+
+def test_ns_residual_fast_path_engages(cuda):
+    for variant in ("unfused", "fused"):
+        rc, out = _run(["ns-residual", "--nx", "128", "--ny", "128", "--iters", "1", "--warmup", "1", "--variant",
+                        variant], env={"NAGA_COSPAN_TRACE": "1"})
+        assert rc == 0, out
+        assert "fast path cspb_ns_compressible 128x128" in out, (variant, out[-2000:])
