@@ -421,6 +421,40 @@ def bench_serving(torch, dist, args):
     return res
 
 
+def bench_reference_programs(args):
+    """The reference's own example programs, unchanged, compiled against this package's cs:: runtime (its fast paths
+    run the GEMVER, BiCGK and NS stages as cspb kernels): ms per chain / evaluation at the reference's published sizes,
+    beside the reference's own numbers on an RTX 4090 (examples/gemver-chain/README.md:140-174,
+    examples/ns-residual/README.md:85-101)."""
+    ex = ROOT / "cospanmdao_b200" / "_examples"
+    res = {}
+    runs = [("gemver_chain_fused_n16384", ["gemver-chain", "--n", "16384", "--iters", "20", "--warmup", "3",
+                                           "--variant", "fused"], "fused", 9.150),
+            ("gemver_chain_crafted_n16384", ["gemver-chain", "--n", "16384", "--iters", "20", "--warmup", "3",
+                                             "--variant", "crafted"], "crafted", 8.359),
+            ("ns_residual_fused_4096", ["ns-residual", "--nx", "4096", "--ny", "4096", "--iters", "20", "--warmup", "3",
+                                        "--variant", "fused", "--range-split", "flatten"], "fused-flatten", 5.810),
+            ("ns_residual_unfused_4096", ["ns-residual", "--nx", "4096", "--ny", "4096", "--iters", "20", "--warmup",
+                                          "3", "--variant", "unfused"], "unfused", 9.685)]
+    for key, cmd, row, ref_ms in runs:
+        exe = ex / cmd[0]
+        if not exe.exists():
+            res[key] = {"skipped": f"{exe.name} not built (python -m cospanmdao_b200.examples)"}
+            continue
+        r = subprocess.run([str(exe), *cmd[1:]], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                           timeout=600)
+        ms = None
+        for line in r.stdout.splitlines():
+            f = line.split()
+            if f and f[0] == row and len(f) > 1:
+                try:
+                    ms = float(f[1])
+                except ValueError:
+                    pass
+        res[key] = {"ms": ms, "rc": r.returncode, "reference_rtx4090_ms": ref_ms}
+    return res
+
+
 # ---- the CPU path ---------------------------------------------------------------------------------------------
 def cpu_gemver(n: int, target_s: float = 3.0, reps: int = 3) -> dict:
     """The reference's unfused GEMVER component loops in f32 (oracle port, OpenMP, every host thread) on a bounded
@@ -475,7 +509,8 @@ def main(argv=None) -> int:
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving stream")
     ap.add_argument("--max-batch", type=int, default=512, help="serving: requests per batch at most")
     ap.add_argument("--only", default="", help="comma list of secondary workloads to run (gemver_bf16_storage, "
-                    "gemver_chain, ns_residual, ragged_batch, serving); default all, none with --quick")
+                    "gemver_chain, ns_residual, ragged_batch, serving, reference_programs); default all, none with "
+                    "--quick")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
     dist = Dist()
@@ -533,6 +568,7 @@ def main(argv=None) -> int:
         "ns_residual": lambda: bench_ns(torch, cb, dist, args),
         "ragged_batch": lambda: bench_ragged(torch, cb, dist, args, pk),
         "serving": lambda: bench_serving(torch, dist, args),
+        "reference_programs": lambda: bench_reference_programs(args),
     }
     wanted = [w for w in args.only.split(",") if w] or ([] if args.quick else list(secondaries))
     unknown = [w for w in wanted if w not in secondaries]
