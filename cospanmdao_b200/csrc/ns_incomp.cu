@@ -359,8 +359,12 @@ __device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblo
 
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
+    nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
+}
+// The f32 ring path: 4 blocks per SM (the waves nsi_shape fills), so at most 64 registers a thread.
+__global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_ring(NsiK g) {
     extern __shared__ __align__(16) float nsi_ring[];
-    nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_ring);
+    nsi_block<float, 4>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_ring);
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
@@ -573,8 +577,8 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
         if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
     } else if (fast) {
-        if (!ring_ready(reinterpret_cast<const void*>(k_ns_incomp<float, 4>))) return CSPB_ERR_LAUNCH;
-        k_ns_incomp<float, 4><<<grid, block, kNsiRingBytes, st>>>(g);
+        if (!ring_ready(reinterpret_cast<const void*>(k_ns_incomp_ring))) return CSPB_ERR_LAUNCH;
+        k_ns_incomp_ring<<<grid, block, kNsiRingBytes, st>>>(g);
     } else {
         k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
