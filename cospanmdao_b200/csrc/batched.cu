@@ -23,8 +23,8 @@ namespace batch {
 
 constexpr int kThreads = kPassThreads;
 constexpr uint32_t kGroup = 4;  // consecutive work items a block takes at once
-constexpr int kSets = 6;  // a, v, p, w, s, u
-enum { SA = 0, SV = 1, SP = 2, SW = 3, SS = 4, SU = 5 };
+constexpr int kSets = 7;  // a, v, p, w, s, u, c
+enum { SA = 0, SV = 1, SP = 2, SW = 3, SS = 4, SU = 5, SC = 6 };
 
 // tuning word: 2 bits per size bucket (n < 512, < 1024, < 2048, >= 2048): 0 -> WX 2, 1 -> WX 1, 2 -> WX 4
 __host__ __device__ inline int bucket_of(uint32_t n) { return n < 512 ? 0 : (n < 1024 ? 1 : (n < 2048 ? 2 : 3)); }
@@ -65,6 +65,7 @@ __global__ void k_plan(PlanK g) {
         g.sizes[SW * g.count + k] = chunks * n;
         g.sizes[SS * g.count + k] = strips;
         g.sizes[SU * g.count + k] = strips * chunks;
+        g.sizes[SC * g.count + k] = chunks;
     }
 }
 
@@ -74,7 +75,7 @@ struct RunK {
     const cspb_gemver_task* tasks;  // task mode when not NULL
     const uint8_t* wx;
     const uint64_t* off[kSets];  // each count + 1
-    uint64_t cap[kSets - 1];     // capacities of a, v, p, w, s (elements)
+    uint64_t cap[SS + 1];        // capacities of a, v, p, w, s (elements)
     const void* A;
     const float *u1, *v1, *u2, *v2, *y, *z, *alpha, *beta;
     float *B, *x, *w;
@@ -200,9 +201,10 @@ __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_
         PassArgs b = a;
         b.src = a.dst;
         b.lds = a.ldd;
-        pass_unit<float, WX, false, false, false, false, true, 16>(b, unit, vec_ok, smem);
+        b.dst = nullptr;  // pass 2 only reads Â
+        pass_unit<float, WX, false, false, false, false, true, 16, true>(b, unit, vec_ok, smem);
     } else {
-        pass_unit<T, WX, true, true, false, false, true>(a, unit, vec_ok, smem);
+        pass_unit<T, WX, true, true, false, false, true, 0, true>(a, unit, vec_ok, smem);
     }
 }
 
@@ -217,85 +219,113 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     const uint64_t U1 = __ldcg(g.off[SU] + g.count);
     __shared__ int s_go;
     if (threadIdx.x == 0) {
-        bool fits = 2 * U1 < 0xffffffffull - (1ull << 24) && U1 <= g.cap_units;  // room for the counter's overshoot
-        for (int s = 0; s < kSets - 1; ++s)  // task mode has no packed matrix / vector offsets
+        // the work list (at most 4·U1 items) must fit the 32-bit counter with room for its overshoot
+        bool fits = 4 * U1 < 0xffffffffull - (1ull << 24) && U1 <= g.cap_units;
+        for (int s = 0; s <= SS; ++s)  // task mode has no packed matrix / vector offsets
             if (g.off[s] != nullptr) fits = fits && __ldcg(g.off[s] + g.count) <= g.cap[s];
         if (!fits) set_status(g.ctrl, CSPB_DEV_CAPACITY);
         s_go = fits && !status_bad(g.ctrl);  // status set by the plan: an invalid size
     }
     __syncthreads();
     if (!s_go) return;
-    __shared__ int s_last;
+    // The work list, one counter: [pass-1 units][x finishes, one per (instance, chunk)][pass-2 units]
+    // [w finishes, one per (instance, strip)]. A unit only counts itself done (a release reduction, no wait); a
+    // finish waits (bounded) for the counter it needs and then forms x over a chunk or w over a strip, in the fixed
+    // orders of the single-instance kernels. Everything an item waits for sits earlier in the list, taken by blocks
+    // that are running and never wait on later items.
+    const uint64_t C1 = __ldcg(g.off[SC] + g.count), S1 = __ldcg(g.off[SS] + g.count);
+    const uint64_t e1 = U1, e2 = U1 + C1, e3 = 2 * U1 + C1, e4 = 2 * U1 + C1 + S1;
     __shared__ int s_ok;
-    // A block takes kGroup consecutive items at a time (usually units of one instance), so the lookup of the instance
-    // and of its arguments is paid once per group rather than once per unit.
-    int64_t hint = 0, cur = -1;
+    int64_t cur = -1;
     PassArgs a{};
     bool vec_ok = false;
     const float* z = nullptr;
     float beta = 0.f;
     float* x = nullptr;
     int wx = 2;
-    uint64_t ubase = 0;
-    for (uint32_t base = grab_work(g.ctrl, kWork0, kGroup); uint64_t(base) < 2 * U1;) {
+    uint64_t ubase = 0, sbase = 0;
+    auto instance = [&](int64_t k) {
+        if (k == cur) return;
+        cur = k;
+        wx = g.wx[k];
+        ubase = __ldcg(g.off[SU] + k);
+        sbase = __ldcg(g.off[SS] + k);
+        a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
+    };
+    auto count_done = [&](uint32_t* counter) {  // this block's unit is complete
+        __syncthreads();
+        if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
+    };
+    auto wait_for = [&](const uint32_t* counter, uint32_t target) {  // bounded; false when it gave up
+        if (threadIdx.x == 0) s_ok = ld_acquire(counter) >= target || wait_at_least(counter, target, g.ctrl);
+        __syncthreads();
+        return s_ok != 0;
+    };
+    for (uint32_t base = grab_work(g.ctrl, kWork0, kGroup); uint64_t(base) < e4;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0, kGroup);
         bool stop = false;
-        for (uint32_t q = 0; q < kGroup; ++q) {
+        for (uint32_t q = 0; q < kGroup && !stop; ++q) {
             const uint64_t item = uint64_t(base) + q;
-            if (item >= 2 * U1) break;
-            const bool pass2 = item >= U1;
-            const uint64_t u = pass2 ? item - U1 : item;
-            const int64_t k = find_instance_from(g.off[SU], g.count, u, hint);
-            hint = k;
-            if (k != cur) {
-                cur = k;
-                wx = g.wx[k];
-                ubase = __ldcg(g.off[SU] + k);
-                a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
-            }
-            const int64_t unit = int64_t(u - ubase);
-            const uint64_t slot = ubase + uint64_t(unit % a.chunks);  // the unit's column chunk
-            if (!pass2) {
-                switch (wx) {
-                    case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
-                    case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
-                    default: unit1<T, 2>(a, unit, vec_ok, smem); break;
+            if (item >= e4) break;
+            if (item < e1 || (item >= e2 && item < e3)) {  // a unit of pass 1 or pass 2
+                const bool pass2 = item >= e2;
+                const uint64_t u = pass2 ? item - e2 : item;
+                const int64_t k = find_instance_from(g.off[SU], g.count, u, cur);
+                instance(k);
+                const int64_t unit = int64_t(u - ubase);
+                const int64_t c = unit % a.chunks, strip = unit / a.chunks;
+                if (!pass2) {
+                    switch (wx) {
+                        case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
+                        case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
+                        default: unit1<T, 2>(a, unit, vec_ok, smem); break;
+                    }
+                    count_done(g.chunk_done + ubase + uint64_t(c));
+                } else {
+                    if (!wait_for(g.x_ready + ubase + uint64_t(c), 1u)) { stop = true; break; }
+                    switch (wx) {
+                        case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
+                        case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
+                        default: unit2<T, 2>(a, unit, vec_ok, smem); break;
+                    }
+                    count_done(g.strip_done + sbase + uint64_t(strip));
                 }
-                // the chunk's counter; one thread fences for the block after the barrier (the cooperative grid-sync
-                // pattern). The last strip of the chunk forms x over the chunk's columns.
+            } else if (item < e2) {  // x over one chunk of an instance
+                const uint64_t f = item - e1;
+                const int64_t k = find_instance_from(g.off[SC], g.count, f, cur);
+                instance(k);
+                const int64_t c = int64_t(f - __ldcg(g.off[SC] + k));
+                if (!wait_for(g.chunk_done + ubase + uint64_t(c), uint32_t(a.strips))) { stop = true; break; }
+                const int64_t CW = cols_of(wx, bf16);
+                const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
+                instance_x(a, z, beta, x, c * CW, c1);
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     __threadfence();
-                    s_last = atomicAdd(g.chunk_done + slot, 1u) == uint32_t(a.strips - 1);
-                    if (s_last) __threadfence();
+                    st_release(g.x_ready + ubase + uint64_t(c), 1u);
                 }
-                __syncthreads();
-                if (s_last) {
-                    const int64_t c = unit % a.chunks;
-                    const int64_t CW = cols_of(wx, bf16);
-                    const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
-                    instance_x(a, z, beta, x, c * CW, c1);
-                    __syncthreads();
-                    if (threadIdx.x == 0) {
-                        __threadfence();
-                        st_release(g.x_ready + slot, 1u);
+            } else {  // w over one strip of an instance: the row-dot partials of its chunks, in chunk order
+                const uint64_t f = item - e3;
+                const int64_t k = find_instance_from(g.off[SS], g.count, f, cur);
+                instance(k);
+                const int64_t strip = int64_t(f - sbase);
+                if (!wait_for(g.strip_done + sbase + uint64_t(strip), uint32_t(a.chunks))) { stop = true; break; }
+                const int64_t S = rows_of(wx);
+                for (int64_t row = strip * S + threadIdx.x; row < (strip + 1) * S && row < a.n; row += blockDim.x) {
+                    float sum = 0.f;
+                    int64_t cc = 0;
+                    for (; cc + 16 <= a.chunks; cc += 16) {
+                        float v[16];
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) v[t] = __ldcg(a.Wp + (cc + t) * a.n + row);
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) sum += v[t];
                     }
-                }
-            } else {
-                if (threadIdx.x == 0)
-                    s_ok = ld_acquire(g.x_ready + slot) != 0u || wait_change(g.x_ready + slot, 0u, g.ctrl);
-                __syncthreads();
-                if (!s_ok) {
-                    stop = true;
-                    break;
-                }
-                switch (wx) {
-                    case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
-                    case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
-                    default: unit2<T, 2>(a, unit, vec_ok, smem); break;
+                    for (; cc < a.chunks; ++cc) sum += __ldcg(a.Wp + cc * a.n + row);
+                    a.rout1[row] = a.rscale1 * sum;
                 }
             }
-            __syncthreads();  // s_last / s_ok and the unit's shared memory are reused by the next item
+            __syncthreads();  // s_ok and the unit's shared memory are reused by the next item
         }
         if (stop) break;
         base = share_work(next);
@@ -328,8 +358,8 @@ BatchLayout batch_layout(int64_t count, int64_t max_elems, int64_t max_vec) {
     size_t o = kCtrlBytes;
     L.off_sizes = o;
     o = align_up(o + size_t(batch::kSets) * size_t(count) * 8, 256);
-    L.off_offs = o;  // p, w, s, u offsets (a and v go to the caller)
-    o = align_up(o + 4 * size_t(count + 1) * 8, 256);
+    L.off_offs = o;  // p, w, s, u, c offsets (a and v go to the caller)
+    o = align_up(o + 5 * size_t(count + 1) * 8, 256);
     L.off_wx = o;
     o = align_up(o + size_t(count), 256);
     L.off_p1 = o;  // chunk counters then chunk flags, zeroed together with the strip counters
@@ -399,7 +429,7 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
 
     uint64_t* offs = reinterpret_cast<uint64_t*>(ws + L.off_offs);
     uint64_t* outs[batch::kSets] = {a_off, v_off, offs, offs + (count + 1), offs + 2 * (count + 1),
-                                    offs + 3 * (count + 1)};
+                                    offs + 3 * (count + 1), offs + 4 * (count + 1)};
     for (int s = 0; s < batch::kSets; ++s) {
         if (!outs[s]) continue;  // task mode: no packed matrix / vector offsets
         const int r = cspb_exclusive_scan_u64(pk.sizes + size_t(s) * size_t(count), outs[s], count, ws + L.off_scan,
