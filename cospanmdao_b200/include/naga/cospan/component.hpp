@@ -64,7 +64,18 @@ struct PortRec {
     std::function<void(void*, const std::size_t*)> bind;
     const void* wrapper = nullptr;
     int var = -1;
+    // a ragged port: declared counts (cs::counts / cs::offsets) and how to point its wrapper at a variable (data, N,
+    // block offsets and per-index extents on the device, or nullptr and the row length for a dense variable)
+    bool ragged = false;
+    std::optional<std::vector<std::size_t>> counts;
+    std::function<void(void*, std::size_t, const std::uint32_t*, const std::uint32_t*, std::size_t)> bind_ragged;
 };
+
+inline std::string list_of(const std::vector<std::size_t>& v) {
+    std::string s = "[";
+    for (std::size_t i = 0; i < v.size(); ++i) s += (i ? "," : "") + std::to_string(v[i]);
+    return s + "]";
+}
 
 template <class S>
 inline void spec_from(ShapeSpec& s, int& d, const S& v) {
@@ -206,11 +217,61 @@ protected:
             set_dims<R>(w.shape_, w.stride_, s);
         }, &w);
     }
+    // ragged ports (component.hpp:220-260 of the reference): (m, name) both dimensions unspecified; (m, name, n) N
+    // given; (m, name, cs::counts(v)) host counts, which give N too; (m, name, cs::offsets(v)) the same as offsets
+    template <DType DT, int R>
+    void declare_input(RaggedInput<DT, R>& w, std::string name) { add_ragged_port(w, std::move(name), false, {}, {}); }
+    template <DType DT, int R, class N, std::enable_if_t<std::is_integral_v<N>, int> = 0>
+    void declare_input(RaggedInput<DT, R>& w, std::string name, N n) {
+        add_ragged_port(w, std::move(name), false, leading(n), {});
+    }
+    template <DType DT, int R>
+    void declare_input(RaggedInput<DT, R>& w, std::string name, Counts c) {
+        add_ragged_port(w, std::move(name), false, {}, std::move(c.v));
+    }
+    template <DType DT, int R>
+    void declare_input(RaggedInput<DT, R>& w, std::string name, const Offsets& o) {
+        add_ragged_port(w, std::move(name), false, {}, counts_of(o).v);
+    }
+    template <DType DT, int R>
+    void declare_output(RaggedOutput<DT, R>& w, std::string name) { add_ragged_port(w, std::move(name), true, {}, {}); }
+    template <DType DT, int R, class N, std::enable_if_t<std::is_integral_v<N>, int> = 0>
+    void declare_output(RaggedOutput<DT, R>& w, std::string name, N n) {
+        add_ragged_port(w, std::move(name), true, leading(n), {});
+    }
+    template <DType DT, int R>
+    void declare_output(RaggedOutput<DT, R>& w, std::string name, Counts c) {
+        add_ragged_port(w, std::move(name), true, {}, std::move(c.v));
+    }
+    template <DType DT, int R>
+    void declare_output(RaggedOutput<DT, R>& w, std::string name, const Offsets& o) {
+        add_ragged_port(w, std::move(name), true, {}, counts_of(o).v);
+    }
     void init_input(std::string name, InitSpec init) { own_inits_.emplace_back(std::move(name), std::move(init)); }
     template <DType DT, int R>
     sycl::range<R> shape_of(const Input<DT, R>& w) const;
     template <DType DT, int R, class... E>
     void set_shape(Output<DT, R>& w, E... e);
+    // a ragged port's shape: N, the total and the counts (on the device for a hooked or copied column)
+    template <DType DT, int R>
+    RaggedShape shape_of(const RaggedInput<DT, R>& w) const { return ragged_shape_of(&w); }
+    template <DType DT, int R>
+    RaggedShape shape_of(const RaggedOutput<DT, R>& w) const { return ragged_shape_of(&w); }
+    /// A ragged output takes a RaggedShape (another port's, read with shape_of): N and the counts, device ones shared.
+    template <DType DT, int R>
+    void set_shape(RaggedOutput<DT, R>& w, const RaggedShape& s) { set_ragged_shape(&w, s); }
+    /// A ragged output takes N and host counts (counts.size() == n).
+    template <DType DT, int R, class N, std::enable_if_t<std::is_integral_v<N>, int> = 0>
+    void set_shape(RaggedOutput<DT, R>& w, N n, std::vector<std::size_t> counts) {
+        if (std::size_t(leading(n)) != counts.size())
+            throw std::invalid_argument("naga::cospan: set_shape on '" + path() + "': N is " + std::to_string(n) + " but " +
+                                        std::to_string(counts.size()) + " counts were given");
+        RaggedShape s;
+        s.n = counts.size();
+        for (auto c : counts) s.total += c;
+        s.counts = std::move(counts);
+        set_ragged_shape(&w, s);
+    }
     template <class... D>
     std::unique_ptr<LaunchDescription> create_launch_config(const D&... descs) const {
         auto L = std::make_unique<LaunchDescription>();
@@ -219,6 +280,36 @@ protected:
     }
 
 private:
+    RaggedShape ragged_shape_of(const void* wrapper) const;               // model.hpp
+    void set_ragged_shape(const void* wrapper, const RaggedShape& s);     // model.hpp
+    template <class N>
+    static std::size_t leading(N n) {
+        if constexpr (std::is_signed_v<N>)
+            if (n < 0) throw std::invalid_argument("naga::cospan: a ragged port's N cannot be negative");
+        return static_cast<std::size_t>(n);
+    }
+    template <class W>
+    void add_ragged_port(W& w, std::string name, bool out, std::optional<std::size_t> n,
+                         std::optional<std::vector<std::size_t>> counts) {
+        ShapeSpec sp;
+        sp.rank = 2;
+        if (counts) n = counts->size();
+        if (n) {
+            sp.ext[0] = *n;
+            sp.known[0] = true;
+        }
+        add_port(std::move(name), out, W::dtype, 2, sp, nullptr, &w);
+        detail::PortRec& p = ports_.back();
+        p.ragged = true;
+        p.counts = std::move(counts);
+        p.bind_ragged = [&w](void* d, std::size_t nb, const std::uint32_t* offs, const std::uint32_t* ext, std::size_t row) {
+            w.data_ = static_cast<std::remove_reference_t<decltype(*w.data_)>*>(d);
+            w.n_ = nb;
+            w.offs_ = offs;
+            w.ext_ = ext;
+            w.row_ = row;
+        };
+    }
     template <int R>
     static void set_dims(sycl::range<R>& shape, sycl::range<R>& stride, const std::size_t* s) {
         std::size_t st = 1;

@@ -184,6 +184,127 @@ struct Initializer {
     value_type* data_ = nullptr;
 };
 
+// ---- ragged ports (wrappers.hpp:236-347 of the reference) -------------------------------------------------------
+// A ragged port is rank 2: N blocks, block i holding count(i) elements, the blocks stored end to end. The runtime
+// keeps per-index extents and the N + 1 block offsets (u32, so a ragged total is below 2^32) on the device. A
+// RaggedInput also reads a DENSE rank-2 variable, whose block i is row i.
+
+/// Per-index counts given on the host, in a declaration: declare_output(m, "m", cs::counts({1, 0, 3})).
+struct Counts {
+    std::vector<std::size_t> v;
+};
+inline Counts counts(std::vector<std::size_t> v) { return Counts{std::move(v)}; }
+/// The same as N + 1 block offsets (offsets[0] == 0, never decreasing).
+struct Offsets {
+    std::vector<std::size_t> v;
+};
+inline Offsets offsets(std::vector<std::size_t> v) {
+    if (v.empty() || v[0] != 0)
+        throw std::invalid_argument("naga::cospan: cs::offsets needs N + 1 >= 1 entries starting at 0");
+    for (std::size_t i = 1; i < v.size(); ++i)
+        if (v[i] < v[i - 1]) throw std::invalid_argument("naga::cospan: cs::offsets must not decrease");
+    return Offsets{std::move(v)};
+}
+inline Counts counts_of(const Offsets& o) {
+    Counts c;
+    for (std::size_t i = 0; i + 1 < o.v.size(); ++i) c.v.push_back(o.v[i + 1] - o.v[i]);
+    return c;
+}
+
+/// One block of a ragged port: a dense rank-1 view (`T` is const for an input).
+template <class T, int R = 1>
+struct Block {
+    static_assert(R == 1, "naga::cospan: a ragged block has rank 1");
+    CS_HD T& operator[](const sycl::id<1>& i) const { return data_[i[0]]; }
+    CS_HD T& operator[](std::size_t f) const { return data_[f]; }
+    CS_HD sycl::range<1> shape() const { return sycl::range<1>{n_}; }
+    CS_HD std::size_t size() const { return n_; }
+    T* data_ = nullptr;
+    std::size_t n_ = 0;
+};
+/// The block of an atomic ragged output: indexing gives a relaxed device-scope atomic_ref.
+template <class T, int R = 1>
+struct AtomicBlock {
+    CS_HD sycl::atomic_ref<T> operator[](const sycl::id<1>& i) const { return sycl::atomic_ref<T>(b_.data_[i[0]]); }
+    CS_HD sycl::atomic_ref<T> operator[](std::size_t f) const { return sycl::atomic_ref<T>(b_.data_[f]); }
+    CS_HD sycl::range<1> shape() const { return b_.shape(); }
+    CS_HD std::size_t size() const { return b_.size(); }
+    Block<T, R> b_;
+};
+
+namespace detail {
+/// Block i: extents from the per-index array (a ragged variable) or the row length (a dense one); the start from the
+/// block offsets, or i rows in.
+template <class T>
+CS_HD inline Block<T> ragged_block(T* data, const std::uint32_t* offs, const std::uint32_t* ext, std::size_t row,
+                                   std::size_t i) {
+    Block<T> b;
+    b.n_ = ext ? std::size_t(ext[i]) : row;
+    b.data_ = data + (offs ? std::size_t(offs[i]) : i * row);
+    return b;
+}
+}  // namespace detail
+
+/// RaggedInput<DT, 2>: a read-only ragged port. size() is N; block(i) is block i.
+template <DType DT, int Rank>
+struct RaggedInput {
+    static_assert(Rank == 2, "naga::cospan: a ragged port is rank 2");
+    static_assert(!is_atomic_v<DT>, "naga::cospan: a ragged input is not atomic");
+    using value_type = cpp_type_t<DT>;
+    static constexpr DType dtype = DT;
+    static constexpr int rank = Rank;
+    static constexpr bool ragged = true;
+    CS_HD std::size_t size() const { return n_; }
+    CS_HD Block<const value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, ext_, row_, i); }
+
+    std::size_t n_ = 0;
+    const value_type* data_ = nullptr;
+    const std::uint32_t* offs_ = nullptr;
+    const std::uint32_t* ext_ = nullptr;
+    std::size_t row_ = 0;
+};
+
+/// RaggedOutput<DT, 2>: the writable twin; with an atomic dtype, block(i) is an AtomicBlock.
+template <DType DT, int Rank>
+struct RaggedOutput {
+    static_assert(Rank == 2, "naga::cospan: a ragged port is rank 2");
+    using value_type = cpp_type_t<DT>;
+    static constexpr DType dtype = DT;
+    static constexpr int rank = Rank;
+    static constexpr bool ragged = true;
+    CS_HD std::size_t size() const { return n_; }
+    template <DType Q = DT, std::enable_if_t<!is_atomic_v<Q>, int> = 0>
+    CS_HD Block<value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, ext_, row_, i); }
+    template <DType Q = DT, std::enable_if_t<is_atomic_v<Q>, int> = 0>
+    CS_HD AtomicBlock<value_type> block(std::size_t i) const {
+        return AtomicBlock<value_type>{detail::ragged_block(data_, offs_, ext_, row_, i)};
+    }
+
+    std::size_t n_ = 0;
+    value_type* data_ = nullptr;
+    const std::uint32_t* offs_ = nullptr;
+    const std::uint32_t* ext_ = nullptr;
+    std::size_t row_ = 0;
+};
+
+static_assert(std::is_trivially_copyable_v<RaggedInput<DType::f32, 2>>);
+static_assert(std::is_trivially_copyable_v<RaggedOutput<DType::atomic_f32, 2>>);
+
+namespace detail {
+struct Column;  // the device counts and offsets of a ragged variable (model.hpp)
+}
+
+/// The shape of a ragged port, as a component's shape_of returns it and its set_shape takes it (component.hpp:
+/// 130-160 of the reference): N, the total, and the counts — on the host (`counts`) or on the device (`column`).
+struct RaggedShape {
+    std::size_t n = 0;
+    std::uint64_t total = 0;
+    std::vector<std::size_t> counts;
+    std::shared_ptr<const detail::Column> column;
+    std::uint64_t column_version = 0;
+    bool on_device() const noexcept { return column != nullptr; }
+};
+
 // ---- work-group items -------------------------------------------------------------------------------------------
 template <int R>
 struct Group {

@@ -148,9 +148,27 @@ inline void Model::finalize() {
         }
         if (is_atomic(pr.p->dtype)) v.dtype = pr.p->dtype;
         if (pr.p->output) v.produced = true;
+        if (pr.p->ragged) {
+            v.ragged_port = true;
+            if (pr.p->output) v.ragged_out = true;
+            if (pr.p->counts) {
+                if (v.declared_counts && *v.declared_counts != *pr.p->counts)
+                    throw std::invalid_argument("naga::cospan: '" + k + "' declares the counts " + detail::list_of(*pr.p->counts) +
+                                                " but '" + v.name + "' has " + detail::list_of(*v.declared_counts) +
+                                                "; the counts must match");
+                v.declared_counts = pr.p->counts;
+            }
+        }
         merge_spec(v, pr.p->declared, k);
         pr.p->var = v.id;
         rt.key_var[k] = v.id;
+    }
+    // a ragged output's variable is read by ragged ports only (a dense one cannot see per-index extents)
+    for (auto& [k, pr] : port_of_key) {
+        const detail::Var& v = rt.vars[pr.p->var];
+        if (v.ragged_out && !pr.p->ragged)
+            throw std::invalid_argument("naga::cospan: '" + k + "' reads the ragged variable '" + v.name +
+                                        "'; a dense Input cannot see per-index extents (declare it as a RaggedInput)");
     }
     for (auto& [k, tr] : tie_of_key) {
         detail::Var& v = var_for(k);
@@ -186,6 +204,7 @@ inline void Model::finalize() {
             detail::Var& v = rt.var_of_path(s, h.path);
             v.hook = h.dims;
             v.hook_sys = s;
+            v.hook_path = s->path().empty() ? h.path : s->path() + "." + h.path;
         }
     detail::register_patterns(rt);
     finalized_ = true;

@@ -18,6 +18,7 @@
 #include <numeric>
 #include <set>
 
+#include "cspb.h"
 #include "naga/slabkit/slabkit.hpp"
 #include "system.hpp"
 
@@ -35,9 +36,59 @@ struct ViewState {
     std::size_t bytes = 0;
     std::array<std::size_t, 4> shape{};
     cudaEvent_t ev = nullptr;
+    // a ragged view: N, and the block offsets (a copy of the device column's, or the rows of a dense variable)
+    bool ragged = false, per = false;
+    std::size_t n = 0, row = 0;
+    std::uint32_t* host_offs = nullptr;
+    std::size_t offs_cap = 0;
     ~ViewState() {
         if (host) cudaFreeHost(host);
+        if (host_offs) cudaFreeHost(host_offs);
         if (ev) cudaEventDestroy(ev);
+    }
+};
+
+/// A ragged variable's device counts and block offsets (shape_hook.hpp:215-348 and variable.hpp:252-300 of the
+/// reference): N extents and N + 1 offsets, u32, so that a ragged total is below 2^32. A counts_from / offsets_from
+/// hook builds one with cspb_build_column (one launch; [total, flag] comes back through mapped pinned memory); host
+/// counts (a declaration, or a producer's set_shape) are uploaded into one. Shared between variables by set_shape(out,
+/// shape_of(in)): the wrappers read the pointers at every bind, so a column that grows is seen by all of them.
+struct Column {
+    std::uint32_t* ext = nullptr;
+    std::uint32_t* offs = nullptr;
+    std::size_t cap = 0;  // entries of offs (ext has at least cap - 1)
+    std::size_t n = 0;
+    std::uint64_t total = 0;
+    std::uint64_t version = 0;
+    std::uint32_t* tf = nullptr;  // mapped pinned [total, flag]
+    std::uint32_t* tf_dev = nullptr;
+    std::vector<std::size_t> uploaded;  // the host counts in the column (a host column)
+    bool has_upload = false;
+    std::vector<std::uint32_t> staging;
+    Column() = default;
+    Column(const Column&) = delete;
+    Column& operator=(const Column&) = delete;
+    ~Column() {
+        if (ext) cudaFree(ext);
+        if (offs) cudaFree(offs);
+        if (tf) cudaFreeHost(tf);
+    }
+    /// Room for n blocks. A reallocation waits for the stream first (kernels in flight may read the old arrays).
+    void reserve(std::size_t nb, cudaStream_t s) {
+        if (!tf) {
+            if (cudaHostAlloc(reinterpret_cast<void**>(&tf), 8, cudaHostAllocMapped) != cudaSuccess ||
+                cudaHostGetDevicePointer(reinterpret_cast<void**>(&tf_dev), tf, 0) != cudaSuccess)
+                throw std::runtime_error("naga::cospan: a ragged column's host word");
+        }
+        if (nb + 1 <= cap) return;
+        const std::size_t want = std::max(nb + 1, cap * 2);
+        if (ext || offs) cudaStreamSynchronize(s);
+        if (ext) cudaFree(ext);
+        if (offs) cudaFree(offs);
+        ext = offs = nullptr;
+        if (cudaMalloc(&ext, std::max<std::size_t>(want - 1, 1) * 4) != cudaSuccess || cudaMalloc(&offs, want * 4) != cudaSuccess)
+            throw std::runtime_error("naga::cospan: allocating a ragged column of " + std::to_string(nb) + " blocks");
+        cap = want;
     }
 };
 
@@ -49,6 +100,7 @@ struct Var {
     ShapeSpec spec;                   // what declarations and ties fix
     std::vector<HookDim> hook;        // a shape hook on it
     System* hook_sys = nullptr;
+    std::string hook_path;            // the hook's target as its System named it (for messages)
     std::array<std::size_t, 4> shape{};
     bool shape_known = false;
     bool shape_from_prepare = false;  // set by a producer's prepare_forward (re-derived every run)
@@ -58,7 +110,18 @@ struct Var {
     bool stale = false;
     bool produced = false;
     std::uint64_t version = 0;        // incremented whenever an initializer writes the variable
+    // ragged (rank 2): N = shape[0], the per-index counts in `column`, `total` elements
+    bool ragged_port = false;         // some port on it is a RaggedInput / RaggedOutput
+    bool ragged_out = false;          // its producer's port is a RaggedOutput
+    bool per = false;                 // its current shape is ragged
+    std::uint64_t total = 0;
+    std::optional<std::vector<std::size_t>> declared_counts;  // cs::counts / cs::offsets in a declaration
+    std::vector<std::size_t> host_counts;                     // counts given on the host (empty for a hooked column)
+    std::shared_ptr<Column> column;                           // what its ragged wrappers read
+    std::shared_ptr<Column> own_column;                       // where its host counts are uploaded
+    std::shared_ptr<Column> hook_column;                      // what its ragged hook builds
     std::size_t elements() const {
+        if (per) return std::size_t(total);
         std::size_t n = 1;
         for (int d = 0; d < rank; ++d) n *= shape[d];
         return n;
@@ -89,6 +152,9 @@ public:
     std::vector<std::shared_ptr<void>> pattern_state;  // what the fast paths keep between runs (workspaces, scales)
     int sms = 0;
     bool trace = false;  // NAGA_COSPAN_TRACE set: every launch and initializer is printed to stderr
+    void* scan_ws = nullptr;  // cspb_build_column's workspace (ragged hooks), grown as needed
+    std::size_t scan_ws_bytes = 0;
+    void* value_buf = nullptr;  // pinned: one element read down by a from_value hook
 
     Runtime() {
         trace = std::getenv("NAGA_COSPAN_TRACE") != nullptr;
@@ -106,33 +172,203 @@ public:
         for (auto& v : vars)
             if (v.data) cudaFree(v.data);
         if (ctrl) cudaFree(ctrl);
+        if (scan_ws) cudaFree(scan_ws);
+        if (value_buf) cudaFreeHost(value_buf);
         views.clear();
         uq.reset();
         if (stream) cudaStreamDestroy(stream);
     }
 
     // ---- shapes and memory ----
+    /// A shape hook (shape_hook.hpp:404-527 of the reference): one descriptor per dimension, or one ragged descriptor.
+    /// It runs once per forward, when the variable's shape is first needed (Model::run forgets hooked shapes).
     void shape_from_hook(Var& v) {
         if (v.hook.empty()) return;
+        const std::string who = "the shape hook on '" + (v.hook_path.empty() ? v.name : v.hook_path) + "'";
+        if (v.hook.size() == 1 && (std::holds_alternative<ragged::CountsFrom>(v.hook[0]) ||
+                                   std::holds_alternative<ragged::OffsetsFrom>(v.hook[0]))) {
+            ragged_hook(v, who);
+            return;
+        }
         if (int(v.hook.size()) != v.rank)
-            throw std::invalid_argument("naga::cospan: the shape hook of '" + v.name + "' has " + std::to_string(v.hook.size()) +
+            throw std::invalid_argument("naga::cospan: " + who + " has " + std::to_string(v.hook.size()) +
                                         " dimensions, the variable has rank " + std::to_string(v.rank));
+        if (v.per) v.shape_known = false;  // a dense hook on a variable that was ragged: it is dense now
+        v.per = false;
         for (int d = 0; d < v.rank; ++d) {
             const HookDim& h = v.hook[d];
             if (auto f = std::get_if<dim::FixedAtRun>(&h)) v.shape[d] = f->v;
-            else if (auto s = std::get_if<dim::FromShape>(&h)) {
-                Var& o = var_of_path(v.hook_sys, s->path);
+            else if (auto sh = std::get_if<dim::FromShape>(&h)) {
+                Var& o = var_of_path(v.hook_sys, sh->path);
                 ensure_shape(o);
-                v.shape[d] = o.shape[s->d];
-            } else if (!v.shape_known)
-                throw std::invalid_argument("naga::cospan: '" + v.name + "': as_is on a dimension with no shape");
+                if (int(sh->d) >= o.rank)
+                    throw std::out_of_range("naga::cospan: " + who + ": '" + sh->path + "' has rank " + std::to_string(o.rank) +
+                                            ", no dimension " + std::to_string(sh->d));
+                if (o.per && sh->d == 1)
+                    throw std::invalid_argument("naga::cospan: " + who + ": dimension 1 of '" + sh->path +
+                                                "' is per-index and cannot become a dense dimension (use cs::ragged::counts_from)");
+                v.shape[d] = o.shape[sh->d];
+            } else if (auto fv = std::get_if<dim::FromValue>(&h)) {
+                v.shape[d] = value_of(var_of_path(v.hook_sys, fv->path), fv->path, fv->index, who);
+            } else if (auto cu = std::get_if<dim::Custom>(&h)) {
+                v.shape[d] = custom_dim(v, *cu);
+            } else if (std::holds_alternative<dim::AsIs>(h)) {
+                if (!v.shape_known && !(v.spec.rank > d && v.spec.known[d]))
+                    throw std::invalid_argument("naga::cospan: '" + v.name + "': as_is on a dimension with no shape");
+                if (!v.shape_known) v.shape[d] = v.spec.ext[d];
+            } else {
+                throw std::invalid_argument("naga::cospan: " + who + ": a ragged descriptor is for a ragged target, as its "
+                                            "only descriptor");
+            }
         }
+        v.shape_known = true;
+    }
+    std::size_t custom_dim(Var& v, const dim::Custom& c);  // after ShapeHookCtx
+    /// The value of element `index` of the integer variable `o`, read down from the device (one small copy, one wait).
+    std::size_t value_of(Var& o, const std::string& path, std::size_t index, const std::string& who) {
+        const DType dt = value_dtype(o.dtype);
+        if (dt == DType::f32 || dt == DType::f64)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' drives a size by value and must have an "
+                                        "integer dtype");
+        if (!o.produced) materialize(o);
+        ensure_shape(o);
+        if (index >= o.elements())
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' drives a size from element " +
+                                        std::to_string(index) + " but has only " + std::to_string(o.elements()) + " elements");
+        if (!o.data) throw std::logic_error("naga::cospan: " + who + ": '" + path + "' has no data");
+        if (!value_buf) cuda_check(cudaMallocHost(&value_buf, 8), "a hook's value buffer");
+        const std::size_t es = dtype_size(dt);
+        cuda_check(cudaMemcpyAsync(value_buf, static_cast<const unsigned char*>(o.data) + index * es, es,
+                                   cudaMemcpyDeviceToHost, stream), "a hook's value read");
+        cuda_check(cudaStreamSynchronize(stream), "a hook's value read");
+        std::int64_t val = 0;
+        switch (dt) {
+            case DType::i32: val = *static_cast<const std::int32_t*>(value_buf); break;
+            case DType::u32: val = std::int64_t(*static_cast<const std::uint32_t*>(value_buf)); break;
+            case DType::i64: val = *static_cast<const std::int64_t*>(value_buf); break;
+            case DType::u64: val = std::int64_t(*static_cast<const std::uint64_t*>(value_buf)); break;
+            default: val = *static_cast<const std::uint8_t*>(value_buf); break;
+        }
+        if (val < 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": element " + std::to_string(index) + " of '" + path +
+                                        "' is " + std::to_string(val) + "; a size cannot be negative");
+        return std::size_t(val);
+    }
+    /// counts_from / offsets_from: the column is built on the device by cspb_build_column from the source's values
+    /// (shape_hook.hpp:215-348 of the reference); only [total, flag] comes back to the host.
+    void ragged_hook(Var& v, const std::string& who) {
+        if (v.rank != 2) throw std::invalid_argument("naga::cospan: " + who + ": a ragged hook needs a rank-2 target");
+        const bool offsets_mode = std::holds_alternative<ragged::OffsetsFrom>(v.hook[0]);
+        const std::string path = offsets_mode ? std::get<ragged::OffsetsFrom>(v.hook[0]).path
+                                              : std::get<ragged::CountsFrom>(v.hook[0]).path;
+        Var& src = var_of_path(v.hook_sys, path);
+        int code = -1;
+        switch (value_dtype(src.dtype)) {
+            case DType::i32: code = CSPB_I32; break;
+            case DType::u32: code = CSPB_U32; break;
+            case DType::i64: code = CSPB_I64; break;
+            case DType::u64: code = CSPB_U64; break;
+            default: break;
+        }
+        if (code < 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' drives per-index extents by value and must "
+                                        "have a 32- or 64-bit integer dtype");
+        if (!src.produced) materialize(src);
+        ensure_shape(src);
+        if (offsets_mode ? src.rank != 1 : src.rank > 2)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' drives per-index extents by value and must "
+                                        "be rank 1" + std::string(offsets_mode ? " (N + 1 offsets)" : " [N] or rank 2 [N, k]"));
+        const std::size_t count = src.shape[0];
+        const std::size_t k = src.rank == 2 ? src.shape[1] : 1;
+        if (offsets_mode && count == 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds no offsets (it needs N + 1 >= 1 entries)");
+        if (!offsets_mode && src.rank == 2 && k == 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' has no column 0");
+        if (!src.data) throw std::logic_error("naga::cospan: " + who + ": '" + path + "' has no data");
+        const std::size_t n = offsets_mode ? count - 1 : count;
+        if (!v.hook_column) v.hook_column = std::make_shared<Column>();
+        Column& c = *v.hook_column;
+        c.reserve(n, stream);
+        const std::size_t need = std::size_t(cspb_scan_workspace_bytes(std::int64_t(n)));
+        if (need > scan_ws_bytes) {
+            if (scan_ws) {
+                cuda_check(cudaStreamSynchronize(stream), "a ragged hook's workspace");
+                cudaFree(scan_ws);
+                scan_ws = nullptr;
+            }
+            cuda_check(cudaMalloc(&scan_ws, need), "a ragged hook's workspace");
+            scan_ws_bytes = need;
+        }
+        const int rc = cspb_build_column(src.data, code, std::int64_t(count), std::int64_t(k), offsets_mode ? 1 : 0, c.ext,
+                                         c.offs, c.tf_dev, scan_ws, std::int64_t(scan_ws_bytes), stream);
+        if (rc != 0) throw std::runtime_error("naga::cospan: " + who + ": cspb_build_column: " + cspb_status_string(rc));
+        cuda_check(cudaStreamSynchronize(stream), who);
+        const std::uint32_t total = c.tf[0], flag = c.tf[1];
+        if ((flag & 1u) == 0 && (flag & 2u) != 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds a value or a total past 2^32 - 1; "
+                                        "ragged totals are limited to 2^32 - 1 elements");
+        if (flag != 0)
+            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds " +
+                                        std::string(offsets_mode ? "offsets that are negative, do not start at 0, or decrease"
+                                                                 : "a negative value") + "; a size cannot be negative");
+        c.n = n;
+        c.total = total;
+        ++c.version;
+        c.has_upload = false;
+        v.per = true;
+        v.shape[0] = n;
+        v.shape[1] = 0;
+        v.total = total;
+        v.host_counts.clear();
+        v.column = v.hook_column;
+        v.shape_known = true;
+    }
+    /// A ragged shape from host counts: uploaded into the variable's own column when they changed.
+    void set_host_counts(Var& v, const std::vector<std::size_t>& counts, const std::string& who) {
+        std::uint64_t total = 0;
+        for (auto c : counts) total += c;
+        if (total > 0xFFFFFFFFull)
+            throw std::invalid_argument("naga::cospan: " + who + ": a ragged shape has " + std::to_string(total) +
+                                        " elements; ragged totals are limited to 2^32 - 1 elements");
+        if (!v.own_column) v.own_column = std::make_shared<Column>();
+        Column& c = *v.own_column;
+        if (!c.has_upload || c.uploaded != counts) {
+            c.reserve(counts.size(), stream);
+            c.staging.assign(2 * counts.size() + 1, 0u);
+            std::uint32_t run = 0;
+            for (std::size_t i = 0; i < counts.size(); ++i) {
+                c.staging[i] = std::uint32_t(counts[i]);
+                c.staging[counts.size() + i] = run;
+                run += std::uint32_t(counts[i]);
+            }
+            c.staging[2 * counts.size()] = run;
+            // staging is pageable: each copy has consumed it when the call returns
+            if (!counts.empty())
+                cuda_check(cudaMemcpyAsync(c.ext, c.staging.data(), counts.size() * 4, cudaMemcpyHostToDevice, stream), who);
+            cuda_check(cudaMemcpyAsync(c.offs, c.staging.data() + counts.size(), (counts.size() + 1) * 4,
+                                       cudaMemcpyHostToDevice, stream), who);
+            c.uploaded = counts;
+            c.has_upload = true;
+            c.n = counts.size();
+            c.total = total;
+            ++c.version;
+        }
+        v.per = true;
+        v.shape[0] = counts.size();
+        v.shape[1] = 0;
+        v.total = total;
+        v.host_counts = counts;
+        v.column = v.own_column;
         v.shape_known = true;
     }
     void ensure_shape(Var& v) {
         if (v.shape_known) return;
         if (!v.hook.empty()) {
             shape_from_hook(v);
+            return;
+        }
+        if (v.declared_counts) {
+            set_host_counts(v, *v.declared_counts, "'" + v.name + "'");
             return;
         }
         if (!v.spec.empty()) {
@@ -165,6 +401,8 @@ public:
             cudaFree(v.data);
         }
         cuda_check(cudaMalloc(&v.data, b), "allocating '" + v.name + "'");
+        // zeroed, so that a variable nothing has written yet (a hooked free input) reads the same on every run
+        cuda_check(cudaMemsetAsync(v.data, 0, b, stream), "allocating '" + v.name + "'");
         v.capacity = b;
     }
     void materialize(Var& v) {
@@ -219,16 +457,37 @@ public:
     Var& var_of_port(ComponentBase* c, const std::string& port) { return vars[key_var.at(c->path() + "." + port)]; }
 
     // ---- running one component (a solo leaf, or a stage of a fused group) ----
+    /// A variable whose declaration fixes zero elements needs no initializer (N = 0 stays valid).
+    static bool declared_empty(const Var& v) {
+        if (v.declared_counts) return v.declared_counts->empty();
+        if (v.spec.empty() || v.spec.rank != v.rank) return false;
+        for (int d = 0; d < v.rank; ++d)
+            if (v.spec.known[d] && v.spec.ext[d] == 0) return true;
+        return false;
+    }
+    /// Points a port's wrapper at its variable: a dense port gets the data and shape; a ragged one the data, N and
+    /// the device column (or, on a dense rank-2 variable, the row length).
+    void bind(ComponentBase* c, detail::PortRec& p, Var& v) {
+        if (p.ragged) {
+            if (v.per) p.bind_ragged(v.data, v.shape[0], v.column->offs, v.column->ext, 0);
+            else p.bind_ragged(v.data, v.shape[0], nullptr, nullptr, v.shape[1]);
+            return;
+        }
+        if (v.per)
+            throw std::logic_error("naga::cospan: '" + c->path() + "." + p.name + "' is ragged; declare it with RaggedInput / "
+                                   "RaggedOutput (a dense Input / Output cannot see per-index extents)");
+        p.bind(v.data, v.shape.data());
+    }
     void prepare(ComponentBase* c) {
         c->rt_ = this;
         for (auto& p : c->ports_) {
             if (p.output) continue;
             Var& v = vars[p.var];
-            if (!v.produced && !v.init && !v.data)
+            if (!v.produced && !v.init && !v.data && v.hook.empty() && !declared_empty(v))
                 throw std::invalid_argument("naga::cospan: the input '" + c->path() + "." + p.name + "' (variable '" +
                                             v.name + "') is never initialized");
             materialize(v);
-            p.bind(v.data, v.shape.data());
+            bind(c, p, v);
         }
         for (auto& p : c->ports_)
             if (p.output) {
@@ -240,7 +499,7 @@ public:
             if (!p.output) continue;
             Var& v = vars[p.var];
             materialize(v);
-            p.bind(v.data, v.shape.data());
+            bind(c, p, v);
         }
     }
     void trace_ports(ComponentBase* c) {
@@ -249,6 +508,7 @@ public:
             std::fprintf(stderr, "[cospan]   %s %-8s var %3d %-28s %p shape", p.output ? "out" : "in ", p.name.c_str(), v.id,
                          v.name.c_str(), v.data);
             for (int d = 0; d < v.rank; ++d) std::fprintf(stderr, " %zu", v.shape[d]);
+            if (v.per) std::fprintf(stderr, " (ragged, %llu elements)", (unsigned long long)v.total);
             std::fprintf(stderr, "\n");
         }
     }
@@ -377,6 +637,8 @@ sycl::range<R> ComponentBase::shape_of(const Input<DT, R>& w) const {
         if (p.wrapper == static_cast<const void*>(&w)) {
             detail::Var& v = rt_->vars[p.var];
             rt_->ensure_shape(v);
+            if (v.per)
+                throw std::logic_error("naga::cospan: '" + path() + "." + p.name + "' is ragged; declare it with RaggedInput");
             sycl::range<R> r;
             for (int d = 0; d < R; ++d) r[d] = v.shape[d];
             return r;
@@ -396,6 +658,92 @@ void ComponentBase::set_shape(Output<DT, R>& w, E... e) {
             return;
         }
     throw std::logic_error("naga::cospan: '" + path() + "': set_shape on a port it does not own");
+}
+
+inline RaggedShape ComponentBase::ragged_shape_of(const void* w) const {
+    for (const auto& p : ports_)
+        if (p.wrapper == w) {
+            detail::Var& v = rt_->vars[p.var];
+            rt_->ensure_shape(v);
+            RaggedShape r;
+            r.n = v.shape[0];
+            if (v.per) {
+                r.total = v.total;
+                r.counts = v.host_counts;
+                r.column = v.column;
+                r.column_version = v.column ? v.column->version : 0;
+            } else {  // a dense variable reads as constant rows
+                r.counts.assign(r.n, v.shape[1]);
+                r.total = std::uint64_t(r.n) * v.shape[1];
+            }
+            return r;
+        }
+    throw std::logic_error("naga::cospan: '" + path() + "': shape_of on a port it does not own");
+}
+inline void ComponentBase::set_ragged_shape(const void* w, const RaggedShape& s) {
+    for (auto& p : ports_)
+        if (p.wrapper == w) {
+            if (!p.output) throw std::logic_error("naga::cospan: '" + path() + "': set_shape on an input");
+            detail::Var& v = rt_->vars[p.var];
+            const std::string who = "set_shape('" + path() + "." + p.name + "')";
+            if (v.declared_counts && !s.on_device() && *v.declared_counts != s.counts)
+                throw std::invalid_argument("naga::cospan: " + who + ": the counts " + detail::list_of(s.counts) +
+                                            " differ from the declared " + detail::list_of(*v.declared_counts));
+            if (s.on_device()) {
+                v.per = true;
+                v.shape[0] = s.n;
+                v.shape[1] = 0;
+                v.total = s.total;
+                v.host_counts = s.counts;
+                v.column = std::const_pointer_cast<detail::Column>(s.column);
+                v.shape_known = true;
+            } else {
+                if (s.counts.size() != s.n)
+                    throw std::invalid_argument("naga::cospan: " + who + ": N is " + std::to_string(s.n) + " but " +
+                                                std::to_string(s.counts.size()) + " counts were given");
+                rt_->set_host_counts(v, s.counts, who);
+            }
+            v.shape_from_prepare = true;
+            return;
+        }
+    throw std::logic_error("naga::cospan: '" + path() + "': set_shape on a port it does not own");
+}
+
+/// What a cs::dim::custom function reads (shape_hook.hpp:352-390 of the reference): shapes and values of variables
+/// by path, in the namespace of the System that declared the hook.
+class ShapeHookCtx {
+public:
+    struct Shape {
+        int rank = 0;
+        std::array<std::size_t, 4> extents{};
+        bool ragged = false;
+        std::uint64_t total = 0;
+    };
+    ShapeHookCtx(detail::Runtime& rt, System* sys, std::string target) : rt_(&rt), sys_(sys), target_(std::move(target)) {}
+    Shape shape_of(std::string_view path) {
+        detail::Var& v = rt_->var_of_path(sys_, std::string(path));
+        if (!v.produced) rt_->materialize(v);
+        rt_->ensure_shape(v);
+        Shape r;
+        r.rank = v.rank;
+        r.extents = v.shape;
+        r.ragged = v.per;
+        r.total = v.per ? v.total : std::uint64_t(v.elements());
+        return r;
+    }
+    std::size_t value_of(std::string_view path, std::size_t index) {
+        detail::Var& v = rt_->var_of_path(sys_, std::string(path));
+        return rt_->value_of(v, std::string(path), index, "the shape hook on '" + target_ + "'");
+    }
+
+private:
+    detail::Runtime* rt_;
+    System* sys_;
+    std::string target_;
+};
+inline std::size_t detail::Runtime::custom_dim(Var& v, const dim::Custom& c) {
+    ShapeHookCtx ctx(*this, v.hook_sys, v.hook_path.empty() ? v.name : v.hook_path);
+    return c.fn(ctx);
 }
 
 namespace detail {
@@ -510,23 +858,47 @@ void FusedGroup<Opts, Items...>::launch(detail::Runtime& rt) {
     if (nseg > detail::kMaxSegments) throw std::invalid_argument("naga::cospan: '" + path() + "': too many segments");
     std::vector<std::size_t> seg_base(nseg, 0), seg_bytes(nseg, 0);
     std::size_t threads = 0;
+    std::vector<std::unique_ptr<LaunchDescription>> descs(stages_.size());
     for (std::size_t i = 0; i < stages_.size(); ++i) {
         ComponentBase* c = stages_[i];
-        if (!kinds[i])
-            throw std::invalid_argument("naga::cospan: '" + c->path() + "': index-range stages in a fused group are not "
-                                        "provided by this backend (give the stage a work-group body)");
         rt.prepare(c);
-        std::unique_ptr<LaunchDescription> d = c->define_forward();
-        if (!d) throw std::invalid_argument("naga::cospan: '" + c->path() + "' describes no launch");
-        detail::StageGeom& g = p.st[i];
-        const int s = stage_segment_[i];
-        g.segment = std::uint32_t(s);
-        g.whole = std::uint32_t(segment_whole_[s]);
-        detail::group_geometry(*d, ranks[i], g.groups, g.local, g.count, c->path());
-        std::size_t th = g.local[0] * g.local[1] * g.local[2];
+        descs[i] = c->define_forward();
+        if (!descs[i]) throw std::invalid_argument("naga::cospan: '" + c->path() + "' describes no launch");
+    }
+    // the work-group size: the group stages' (they must agree); 256 work-items when every stage is index-range
+    for (std::size_t i = 0; i < stages_.size(); ++i) {
+        if (!kinds[i]) continue;
+        std::array<std::size_t, 3> g3{1, 1, 1}, l3{1, 1, 1};
+        std::uint64_t cnt = 0;
+        detail::group_geometry(*descs[i], ranks[i], g3, l3, cnt, stages_[i]->path());
+        const std::size_t th = l3[0] * l3[1] * l3[2];
         if (threads == 0) threads = th;
         else if (threads != th)
             throw std::invalid_argument("naga::cospan: '" + path() + "': its stages have different work-group sizes");
+    }
+    if (threads == 0) threads = 256;
+    for (std::size_t i = 0; i < stages_.size(); ++i) {
+        ComponentBase* c = stages_[i];
+        const LaunchDescription* d = descs[i].get();
+        detail::StageGeom& g = p.st[i];
+        const int s = stage_segment_[i];
+        g.segment = std::uint32_t(s);
+        if (!kinds[i]) {
+            // an index-range stage: its range, flattened, in groups of `threads` work-items
+            if (d->rank != ranks[i])
+                throw std::invalid_argument("naga::cospan: '" + c->path() + "': launch range of the wrong rank");
+            g.whole = 0;
+            g.items = 1;
+            for (int k = 0; k < ranks[i]; ++k) {
+                g.groups[k] = d->range[k];
+                g.items *= d->range[k];
+            }
+            g.count = (g.items + threads - 1) / threads;
+            p.seg[s].count = std::max<std::uint64_t>(p.seg[s].count, g.count);
+            continue;
+        }
+        g.whole = std::uint32_t(segment_whole_[s]);
+        detail::group_geometry(*d, ranks[i], g.groups, g.local, g.count, c->path());
         std::size_t bytes = 0;
         const std::uint32_t base = segment_local_shared_[s] ? 0u : std::uint32_t(seg_bytes[s]);
         g.local_mem = detail::local_layout(elems[i], *d, base, bytes, c->path());
@@ -599,6 +971,40 @@ private:
     std::shared_ptr<detail::ViewState> s_;
 };
 
+/// HostRagged<DT, 2>: a host view of a ragged variable (host_view.hpp:154-200 of the reference): the blocks end to
+/// end, N, and the N + 1 block offsets. Also taken of a dense rank-2 variable, whose blocks are its rows.
+template <DType DT, int R>
+class HostRagged {
+public:
+    static_assert(R == 2, "naga::cospan: a ragged host view is rank 2");
+    using value_type = cpp_type_t<value_dtype(DT)>;
+    explicit HostRagged(std::shared_ptr<detail::ViewState> s) : s_(std::move(s)) {}
+    void sync() const {
+        if (s_->ev) detail::cuda_check(cudaEventSynchronize(s_->ev), "view sync");
+    }
+    std::size_t size() const { return s_->bytes / sizeof(value_type); }
+    const value_type* data() const { return static_cast<const value_type*>(s_->host); }
+    std::span<const value_type> span() const { return std::span<const value_type>(data(), size()); }
+    const value_type& operator[](std::size_t f) const { return data()[f]; }
+    /// N, the number of blocks.
+    std::size_t n() const { return s_->n; }
+    /// Block i is data()[offsets[i], offsets[i + 1]).
+    std::vector<std::uint64_t> block_offsets() const {
+        std::vector<std::uint64_t> o(s_->n + 1, 0);
+        for (std::size_t i = 0; i <= s_->n; ++i) o[i] = s_->per ? std::uint64_t(s_->host_offs[i]) : std::uint64_t(i) * s_->row;
+        return o;
+    }
+    std::span<const value_type> block(std::size_t i) const {
+        if (i >= s_->n) throw std::out_of_range("naga::cospan: HostRagged::block past the last block");
+        const std::uint64_t a = s_->per ? s_->host_offs[i] : std::uint64_t(i) * s_->row;
+        const std::uint64_t b = s_->per ? s_->host_offs[i + 1] : std::uint64_t(i + 1) * s_->row;
+        return std::span<const value_type>(data() + a, std::size_t(b - a));
+    }
+
+private:
+    std::shared_ptr<detail::ViewState> s_;
+};
+
 // ---- the model --------------------------------------------------------------------------------------------------------
 namespace detail {
 void register_patterns(Runtime& rt);  // patterns.hpp
@@ -627,11 +1033,17 @@ public:
             throw std::invalid_argument("naga::cospan: update_input('" + path + "'): the variable is an output of a component");
         v.init = std::move(init);
         v.stale = true;
-        if (!v.hook.empty() || v.spec.empty()) v.shape_known = false;
+        // the new initializer may bring another shape, unless the declaration fixes every dimension
+        bool fixed = !v.spec.empty() && v.hook.empty();
+        for (int d = 0; fixed && d < v.rank; ++d) fixed = v.spec.known[d];
+        if (!fixed) v.shape_known = false;
     }
     void run() {
         finalize();
         auto& rt = *rt_;
+        // shape hooks run once per forward, when their target's shape is first needed
+        for (auto& v : rt.vars)
+            if (!v.hook.empty()) v.shape_known = false;
         auto run_leaf = [&](std::size_t i) {
             Node* n = rt.leaves[i];
             if (n->kind == Node::Kind::component) rt.run_component(static_cast<ComponentBase*>(n));
@@ -663,18 +1075,14 @@ public:
         }
     }
     template <DType DT, int R>
-    HostView<DT, R> view_output(const std::string& path) {
-        finalize();
-        detail::Var& v = rt_->var_of_path(root_.get(), path);
-        if (v.rank != R || !dtype_compatible(v.dtype, DT))
-            throw std::invalid_argument("naga::cospan: view_output('" + path + "'): the variable is " +
-                                        std::string(dtype_name(v.dtype)) + " of rank " + std::to_string(v.rank));
-        auto s = std::make_shared<detail::ViewState>();
-        s->var = v.id;
-        rt_->views.push_back(s);
-        push(*s);
-        return HostView<DT, R>(s);
-    }
+    HostView<DT, R> view_output(const std::string& path) { return dense_view<DT, R>("view_output", path); }
+    template <DType DT, int R>
+    HostView<DT, R> view_input(const std::string& path) { return dense_view<DT, R>("view_input", path); }
+    /// A host view of a ragged variable (or of a dense rank-2 one, as rows), pushed after every run while it lives.
+    template <DType DT, int R>
+    HostRagged<DT, R> view_ragged_output(const std::string& path) { return ragged_view<DT, R>("view_ragged_output", path); }
+    template <DType DT, int R>
+    HostRagged<DT, R> view_ragged_input(const std::string& path) { return ragged_view<DT, R>("view_ragged_input", path); }
     System& root() { return *root_; }
     detail::Runtime& runtime() { return *rt_; }
     /// device bytes held by the model's variables (Model::memory_report's total)
@@ -689,18 +1097,63 @@ private:
     std::unique_ptr<detail::Runtime> rt_;
     bool setup_done_ = false, finalized_ = false;
 
+    template <DType DT, int R>
+    HostView<DT, R> dense_view(const char* what, const std::string& path) {
+        finalize();
+        detail::Var& v = rt_->var_of_path(root_.get(), path);
+        if (v.per || v.ragged_out)
+            throw std::invalid_argument("naga::cospan: " + std::string(what) + "('" + path + "'): the variable is ragged; "
+                                        "read it with view_ragged_" + std::string(what + 5));
+        if (v.rank != R || !dtype_compatible(v.dtype, DT))
+            throw std::invalid_argument("naga::cospan: " + std::string(what) + "('" + path + "'): wrong dtype or rank (the "
+                                        "variable is " + std::string(dtype_name(v.dtype)) + " of rank " +
+                                        std::to_string(v.rank) + ")");
+        auto s = std::make_shared<detail::ViewState>();
+        s->var = v.id;
+        rt_->views.push_back(s);
+        push(*s);
+        return HostView<DT, R>(s);
+    }
+    template <DType DT, int R>
+    HostRagged<DT, R> ragged_view(const char* what, const std::string& path) {
+        finalize();
+        detail::Var& v = rt_->var_of_path(root_.get(), path);
+        if (v.rank != R || R != 2 || !dtype_compatible(v.dtype, DT))
+            throw std::invalid_argument("naga::cospan: " + std::string(what) + "('" + path + "'): wrong dtype or rank (the "
+                                        "variable is " + std::string(dtype_name(v.dtype)) + " of rank " +
+                                        std::to_string(v.rank) + ")");
+        auto s = std::make_shared<detail::ViewState>();
+        s->var = v.id;
+        s->ragged = true;
+        rt_->views.push_back(s);
+        push(*s);
+        return HostRagged<DT, R>(s);
+    }
     void push(detail::ViewState& s) {
         detail::Var& v = rt_->vars[s.var];
         if (!v.data) return;
         const std::size_t b = v.bytes();
-        if (b != s.bytes) {
+        if (b != s.bytes || !s.host) {
             if (s.host) cudaFreeHost(s.host);
             detail::cuda_check(cudaMallocHost(&s.host, std::max<std::size_t>(b, 16)), "host view");
             s.bytes = b;
         }
         s.shape = v.shape;
+        s.per = v.per;
+        s.n = v.shape[0];
+        s.row = v.rank == 2 && !v.per ? v.shape[1] : 0;
         if (!s.ev) detail::cuda_check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "view event");
-        detail::cuda_check(cudaMemcpyAsync(s.host, v.data, b, cudaMemcpyDeviceToHost, rt_->stream), "view push");
+        if (b) detail::cuda_check(cudaMemcpyAsync(s.host, v.data, b, cudaMemcpyDeviceToHost, rt_->stream), "view push");
+        if (s.ragged && v.per) {
+            if (s.offs_cap < s.n + 1) {
+                if (s.host_offs) cudaFreeHost(s.host_offs);
+                s.host_offs = nullptr;
+                detail::cuda_check(cudaMallocHost(reinterpret_cast<void**>(&s.host_offs), (s.n + 1) * 4), "host view");
+                s.offs_cap = s.n + 1;
+            }
+            detail::cuda_check(cudaMemcpyAsync(s.host_offs, v.column->offs, (s.n + 1) * 4, cudaMemcpyDeviceToHost, rt_->stream),
+                               "view push");
+        }
         detail::cuda_check(cudaEventRecord(s.ev, rt_->stream), "view event");
     }
 

@@ -15,16 +15,32 @@
 
 namespace naga::cospan {
 
-// shape-hook descriptors (shape_hook.hpp:65-84)
+class ShapeHookCtx;  // what a custom descriptor reads through (model.hpp)
+
+// shape-hook descriptors (shape_hook.hpp:65-84): one per dimension, or one ragged descriptor for a rank-2 target
 namespace dim {
 struct AsIs {};
 struct FixedAtRun { std::size_t v = 0; };
 struct FromShape { std::string path; std::size_t d = 0; };
+struct FromValue { std::string path; std::size_t index = 0; };
+struct Custom { std::function<std::size_t(ShapeHookCtx&)> fn; };
 inline AsIs as_is() { return {}; }
 inline FixedAtRun fixed_at_run(std::size_t v) { return FixedAtRun{v}; }
 inline FromShape from_shape(std::string path, std::size_t d) { return FromShape{std::move(path), d}; }
+/// the VALUE of element `index` (flat) of an integer variable
+inline FromValue from_value(std::string path, std::size_t index) { return FromValue{std::move(path), index}; }
+inline Custom custom(std::function<std::size_t(ShapeHookCtx&)> fn) { return Custom{std::move(fn)}; }
 }  // namespace dim
-using HookDim = std::variant<dim::AsIs, dim::FixedAtRun, dim::FromShape>;
+namespace ragged {
+/// the per-index counts are the values of an integer variable (rank 1 [N], or column 0 of a rank-2 [N, k])
+struct CountsFrom { std::string path; };
+/// the N + 1 block offsets are the values of a rank-1 integer variable
+struct OffsetsFrom { std::string path; };
+inline CountsFrom counts_from(std::string path) { return CountsFrom{std::move(path)}; }
+inline OffsetsFrom offsets_from(std::string path) { return OffsetsFrom{std::move(path)}; }
+}  // namespace ragged
+using HookDim = std::variant<dim::AsIs, dim::FixedAtRun, dim::FromShape, dim::FromValue, dim::Custom, ragged::CountsFrom,
+                             ragged::OffsetsFrom>;
 
 class System : public Node {
 public:
@@ -41,7 +57,12 @@ public:
         adopt(d.build(), d.name);
     }
 
-    void connect(std::string_view src, std::string_view dst) { connects_.emplace_back(std::string(src), std::string(dst)); }
+    /// Records a connect. The ragged wiring rules are checked in the call, as the reference does (wiring.hpp): a dense
+    /// Input cannot read a ragged source, and two ragged ports that both declare N or counts must agree.
+    void connect(std::string_view src, std::string_view dst) {
+        check_ragged_connect(std::string(src), std::string(dst));
+        connects_.emplace_back(std::string(src), std::string(dst));
+    }
     template <DType DT, int R>
     void promote(std::string_view path, std::string alias) {
         if (aliases_.count(alias))
@@ -101,7 +122,41 @@ public:
         else static_cast<System*>(raw)->setup();
     }
 
+    /// The port a path names below this system, through child names (nullptr when it names none of them).
+    detail::PortRec* find_port(const std::string& path) const {
+        const auto dot = path.find('.');
+        if (dot == std::string::npos) return nullptr;
+        Node* c = child(path.substr(0, dot));
+        if (!c) return nullptr;
+        const std::string rest = path.substr(dot + 1);
+        if (c->kind == Kind::component) return static_cast<ComponentBase*>(c)->port(rest);
+        return static_cast<System*>(c)->find_port(rest);
+    }
+
 private:
+    void check_ragged_connect(const std::string& a, const std::string& b) const {
+        const detail::PortRec* pa = find_port(a);
+        const detail::PortRec* pb = find_port(b);
+        if (!pa || !pb) return;  // promoted or tied names: checked when the model finalizes
+        const std::string call = "naga::cospan: connect('" + a + "', '" + b + "')";
+        auto dense_reader = [&](const detail::PortRec* src, const std::string& sn, const detail::PortRec* dst,
+                                const std::string& dn) {
+            if (src->ragged && src->output && !dst->ragged && !dst->output)
+                throw std::invalid_argument(call + ": '" + sn + "' is ragged; a dense Input cannot see per-index extents "
+                                            "(declare '" + dn + "' as a RaggedInput)");
+        };
+        dense_reader(pa, a, pb, b);
+        dense_reader(pb, b, pa, a);
+        if (!pa->ragged || !pb->ragged) return;
+        if (pa->declared.known[0] && pb->declared.known[0] && pa->declared.ext[0] != pb->declared.ext[0])
+            throw std::invalid_argument(call + ": dimension 0: '" + a + "' declares " + std::to_string(pa->declared.ext[0]) +
+                                        ", '" + b + "' declares " + std::to_string(pb->declared.ext[0]) +
+                                        "; the extents must match");
+        if (pa->counts && pb->counts && *pa->counts != *pb->counts)
+            throw std::invalid_argument(call + ": dimension 1: the counts must match ('" + a + "' declares " +
+                                        detail::list_of(*pa->counts) + ", '" + b + "' declares " +
+                                        detail::list_of(*pb->counts) + ")");
+    }
     template <DType DT, int R>
     static TieEntry cs_tie_inputs(std::initializer_list<std::string_view> members, std::string name, ShapeSpec shape) {
         return naga::cospan::tie_inputs<DT, R>(members, std::move(name), shape);
@@ -165,6 +220,7 @@ struct StageGeom {
     std::uint32_t segment = 0;
     std::uint32_t whole = 0;  // range_mode::whole
     std::uint64_t count = 0;  // the stage's own work-groups
+    std::uint64_t items = 0;  // an index-range stage: its indices (groups holds its range)
     std::array<std::size_t, 3> groups{1, 1, 1};
     std::array<std::size_t, 3> local{1, 1, 1};
     LocalLayout local_mem;
@@ -221,23 +277,36 @@ __device__ inline bool fused_barrier(std::uint32_t* ctrl) {
 template <class X, int I, class P>
 __device__ inline void run_stage(const P& p, std::uint64_t lg, unsigned char* smem) {
     const StageGeom& g = p.st[I];
-    // own: the stage runs for its first `count` groups of the segment's block; whole: for every group of the block
-    const std::uint64_t cnt = g.whole ? p.seg[g.segment].count : g.count;
-    if (lg >= cnt) return;
-    constexpr int R = body_rank<X>;
-    GroupItem<R> it;
-    std::uint64_t rest = 1;
-    for (int d = 0; d < R; ++d) {
-        it.group_range[d] = g.groups[d];
-        it.local_range[d] = g.local[d];
-        if (d > 0) rest *= g.groups[d];
+    if constexpr (!is_group_body<X>) {
+        // an index-range stage: group lg of the segment runs indices [lg * threads, (lg + 1) * threads) of its
+        // flattened range, one per work-item
+        constexpr int R = body_rank<X>;
+        const std::uint64_t t = lg * blockDim.x + threadIdx.x;
+        if (lg >= g.count || t >= g.items) return;
+        sycl::range<R> r;
+        for (int d = 0; d < R; ++d) r[d] = g.groups[d];
+        const auto& io = std::get<I>(p.io);
+        X::compute_forward(delinear<R>(t, r), io.first, io.second);
+        return;
+    } else {
+        // own: the stage runs for its first `count` groups of the segment's block; whole: for every group of the block
+        const std::uint64_t cnt = g.whole ? p.seg[g.segment].count : g.count;
+        if (lg >= cnt) return;
+        constexpr int R = body_rank<X>;
+        GroupItem<R> it;
+        std::uint64_t rest = 1;
+        for (int d = 0; d < R; ++d) {
+            it.group_range[d] = g.groups[d];
+            it.local_range[d] = g.local[d];
+            if (d > 0) rest *= g.groups[d];
+        }
+        if (g.whole) it.group_range[0] = (cnt + rest - 1) / rest;
+        it.group_id = delinear<R>(lg, it.group_range);
+        it.segment = g.segment;
+        const auto& io = std::get<I>(p.io);
+        if constexpr (std::is_void_v<body_local_t<X>>) X::compute_forward(it, io.first, io.second);
+        else X::compute_forward(it, io.first, io.second, make_local<body_local_t<X>>(smem, g.local_mem));
     }
-    if (g.whole) it.group_range[0] = (cnt + rest - 1) / rest;
-    it.group_id = delinear<R>(lg, it.group_range);
-    it.segment = g.segment;
-    const auto& io = std::get<I>(p.io);
-    if constexpr (std::is_void_v<body_local_t<X>>) X::compute_forward(it, io.first, io.second);
-    else X::compute_forward(it, io.first, io.second, make_local<body_local_t<X>>(smem, g.local_mem));
 }
 
 template <class P, class... Xs, std::size_t... I>

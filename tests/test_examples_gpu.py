@@ -35,6 +35,14 @@ def test_runtime_fused_groups(cuda):
     assert rc == 0 and "ALL OK" in out, out
 
 
+def test_runtime_ragged(cuda):
+    """Ragged ports and counts_from / offsets_from hooks (tests/runtime/ragged.cu): device-built columns over forwards
+    with changing counts, declared counts at connects, dense rows read as blocks, the hook's error flags, host views,
+    and ragged stages inside a fused group (the reference refuses those)."""
+    rc, out = _run(["runtime-ragged"])
+    assert rc == 0 and "ALL OK" in out, out
+
+
 def test_getting_started(cuda):
     rc, out = _run(["getting-started"])
     assert rc == 0, out
