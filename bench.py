@@ -428,21 +428,33 @@ def bench_reference_programs(args):
     examples/ns-residual/README.md:85-101)."""
     ex = ROOT / "cospanmdao_b200" / "_examples"
     res = {}
+    eager = {"NAGA_COSPAN_NO_GRAPH": "1"}  # no CUDA-graph replay of steady forwards
     runs = [("gemver_chain_fused_n16384", ["gemver-chain", "--n", "16384", "--iters", "20", "--warmup", "3",
-                                           "--variant", "fused"], "fused", 9.150),
+                                           "--variant", "fused"], "fused", 9.150, {}),
             ("gemver_chain_crafted_n16384", ["gemver-chain", "--n", "16384", "--iters", "20", "--warmup", "3",
-                                             "--variant", "crafted"], "crafted", 8.359),
+                                             "--variant", "crafted"], "crafted", 8.359, {}),
             ("ns_residual_fused_4096", ["ns-residual", "--nx", "4096", "--ny", "4096", "--iters", "20", "--warmup", "3",
-                                        "--variant", "fused", "--range-split", "flatten"], "fused-flatten", 5.810),
+                                        "--variant", "fused", "--range-split", "flatten"], "fused-flatten", 5.810, {}),
             ("ns_residual_unfused_4096", ["ns-residual", "--nx", "4096", "--ny", "4096", "--iters", "20", "--warmup",
-                                          "3", "--variant", "unfused"], "unfused", 9.685)]
-    for key, cmd, row, ref_ms in runs:
+                                          "3", "--variant", "unfused"], "unfused", 9.685, {})]
+    # small sizes, where the reference's per-forward host work dominates: replayed forwards, and eager ones
+    for tag, env in (("", {}), ("_eager", eager)):
+        runs += [(f"gemver_chain_fused_n2048{tag}", ["gemver-chain", "--n", "2048", "--iters", "200", "--warmup", "3",
+                                                    "--variant", "fused"], "fused", 1.582, env),
+                 (f"gemver_chain_unfused_n2048{tag}", ["gemver-chain", "--n", "2048", "--iters", "200", "--warmup", "3",
+                                                      "--variant", "unfused"], "unfused", 1.925, env),
+                 (f"ns_residual_fused_1024{tag}", ["ns-residual", "--nx", "1024", "--ny", "1024", "--iters", "200",
+                                                  "--warmup", "3", "--variant", "fused", "--range-split", "flatten"],
+                  "fused-flatten", 1.532, env),
+                 (f"ns_residual_unfused_1024{tag}", ["ns-residual", "--nx", "1024", "--ny", "1024", "--iters", "200",
+                                                    "--warmup", "3", "--variant", "unfused"], "unfused", 3.260, env)]
+    for key, cmd, row, ref_ms, env in runs:
         exe = ex / cmd[0]
         if not exe.exists():
             res[key] = {"skipped": f"{exe.name} not built (python -m cospanmdao_b200.examples)"}
             continue
         r = subprocess.run([str(exe), *cmd[1:]], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
-                           timeout=600)
+                           timeout=600, env=dict(os.environ, **env))
         ms = None
         for line in r.stdout.splitlines():
             f = line.split()

@@ -155,9 +155,20 @@ public:
     void* scan_ws = nullptr;  // cspb_build_column's workspace (ragged hooks), grown as needed
     std::size_t scan_ws_bytes = 0;
     void* value_buf = nullptr;  // pinned: one element read down by a from_value hook
+    // CUDA-graph replay of steady runs (Model::run): a run that made no host wait and no allocation is a template
+    // for the next one, which is captured; later runs replay it until an update_input or a new view.
+    std::uint64_t host_syncs = 0;  // waits and device reads the host made (hooks, initializers, scale reads, uploads)
+    std::uint64_t allocs = 0;      // device allocations
+    std::uint64_t epoch = 0;       // bumped by update_input and by a new view
+    std::uint64_t steady_epoch = ~0ull;
+    std::uint64_t graph_epoch = ~0ull;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_allowed = true;     // NAGA_COSPAN_NO_GRAPH, NAGA_COSPAN_TRACE or a failed capture turn it off
+    std::uint64_t graph_captures = 0, graph_replays = 0;
 
     Runtime() {
         trace = std::getenv("NAGA_COSPAN_TRACE") != nullptr;
+        graph_allowed = !trace && std::getenv("NAGA_COSPAN_NO_GRAPH") == nullptr;
         cuda_check(cudaGetDevice(&device), "cudaGetDevice");
         cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
         cuda_check(cudaMalloc(&ctrl, 256), "control block");
@@ -167,6 +178,7 @@ public:
     }
     ~Runtime() {
         cudaStreamSynchronize(stream);
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
         pattern_runs.clear();
         pattern_state.clear();
         for (auto& v : vars)
@@ -236,6 +248,7 @@ public:
             throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' drives a size from element " +
                                         std::to_string(index) + " but has only " + std::to_string(o.elements()) + " elements");
         if (!o.data) throw std::logic_error("naga::cospan: " + who + ": '" + path + "' has no data");
+        ++host_syncs;
         if (!value_buf) cuda_check(cudaMallocHost(&value_buf, 8), "a hook's value buffer");
         const std::size_t es = dtype_size(dt);
         cuda_check(cudaMemcpyAsync(value_buf, static_cast<const unsigned char*>(o.data) + index * es, es,
@@ -258,6 +271,7 @@ public:
     /// (shape_hook.hpp:215-348 of the reference); only [total, flag] comes back to the host.
     void ragged_hook(Var& v, const std::string& who) {
         if (v.rank != 2) throw std::invalid_argument("naga::cospan: " + who + ": a ragged hook needs a rank-2 target");
+        ++host_syncs;
         const bool offsets_mode = std::holds_alternative<ragged::OffsetsFrom>(v.hook[0]);
         const std::string path = offsets_mode ? std::get<ragged::OffsetsFrom>(v.hook[0]).path
                                               : std::get<ragged::CountsFrom>(v.hook[0]).path;
@@ -291,6 +305,7 @@ public:
         c.reserve(n, stream);
         const std::size_t need = std::size_t(cspb_scan_workspace_bytes(std::int64_t(n)));
         if (need > scan_ws_bytes) {
+            ++allocs;
             if (scan_ws) {
                 cuda_check(cudaStreamSynchronize(stream), "a ragged hook's workspace");
                 cudaFree(scan_ws);
@@ -333,6 +348,7 @@ public:
         if (!v.own_column) v.own_column = std::make_shared<Column>();
         Column& c = *v.own_column;
         if (!c.has_upload || c.uploaded != counts) {
+            ++host_syncs;  // an upload from pageable memory: never part of a captured run
             c.reserve(counts.size(), stream);
             c.staging.assign(2 * counts.size() + 1, 0u);
             std::uint32_t run = 0;
@@ -396,6 +412,7 @@ public:
     void allocate(Var& v) {
         const std::size_t b = std::max<std::size_t>(v.bytes(), 16);
         if (v.data && v.capacity >= b) return;
+        ++allocs;
         if (v.data) {
             cuda_check(cudaStreamSynchronize(stream), "resize");
             cudaFree(v.data);
@@ -591,6 +608,7 @@ InitSpec from_host(std::vector<T> values) {
                                         "' has " + std::to_string(t.var.elements()) + " elements");
         if (sizeof(T) != dtype_size(t.var.dtype))
             throw std::invalid_argument("naga::cospan: init::from_host for '" + t.var.name + "' has the wrong element type");
+        ++t.rt.host_syncs;
         detail::cuda_check(cudaMemcpyAsync(t.var.data, data->data(), n * sizeof(T), cudaMemcpyHostToDevice, t.rt.stream),
                            "from_host");
         detail::cuda_check(cudaStreamSynchronize(t.rt.stream), "from_host");
@@ -742,6 +760,7 @@ private:
     std::string target_;
 };
 inline std::size_t detail::Runtime::custom_dim(Var& v, const dim::Custom& c) {
+    ++host_syncs;  // a custom function may give another size on every run: such a model is never replayed
     ShapeHookCtx ctx(*this, v.hook_sys, v.hook_path.empty() ? v.name : v.hook_path);
     return c.fn(ctx);
 }
@@ -1033,13 +1052,80 @@ public:
             throw std::invalid_argument("naga::cospan: update_input('" + path + "'): the variable is an output of a component");
         v.init = std::move(init);
         v.stale = true;
+        ++rt_->epoch;
         // the new initializer may bring another shape, unless the declaration fixes every dimension
         bool fixed = !v.spec.empty() && v.hook.empty();
         for (int d = 0; fixed && d < v.rank; ++d) fixed = v.spec.known[d];
         if (!fixed) v.shape_known = false;
     }
+    /// One forward (model.hpp:471-480 of the reference): enqueues the leaves on the model's stream and returns.
+    /// Steady runs replay a CUDA graph: once a run has made no host wait and no allocation (so every later run with
+    /// the same inputs enqueues the same work), the next run is captured and later ones replay it with one launch,
+    /// until update_input or a new host view. A capture that fails turns replay off for the model; the run is then
+    /// done eagerly. NAGA_COSPAN_NO_GRAPH=1 turns replay off.
     void run() {
         finalize();
+        auto& rt = *rt_;
+        if (rt.graph_exec && rt.graph_epoch == rt.epoch) {
+            detail::cuda_check(cudaGraphLaunch(rt.graph_exec, rt.stream), "replaying a forward");
+            ++rt.graph_replays;
+            for (auto& v : rt.views) push(*v);
+            return;
+        }
+        if (rt.graph_allowed && rt.steady_epoch == rt.epoch && capture()) {
+            for (auto& v : rt.views) push(*v);
+            return;
+        }
+        const std::uint64_t syncs = rt.host_syncs, allocs = rt.allocs;
+        run_leaves();
+        rt.steady_epoch = rt.host_syncs == syncs && rt.allocs == allocs ? rt.epoch : ~0ull;
+        for (auto& v : rt.views) push(*v);
+    }
+    /// How many forwards were captured into a graph, and how many replayed one.
+    std::pair<std::uint64_t, std::uint64_t> graph_counts() const { return {rt_->graph_captures, rt_->graph_replays}; }
+
+private:
+    /// Captures one forward into a graph and launches it. False (nothing enqueued, replay turned off) when the capture
+    /// failed or the forward waited on the host or allocated.
+    bool capture() {
+        auto& rt = *rt_;
+        if (rt.graph_exec) {
+            cudaGraphExecDestroy(rt.graph_exec);
+            rt.graph_exec = nullptr;
+        }
+        const std::uint64_t syncs = rt.host_syncs, allocs = rt.allocs;
+        if (cudaStreamBeginCapture(rt.stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+            cudaGetLastError();
+            rt.graph_allowed = false;
+            return false;
+        }
+        bool ok = true;
+        try {
+            run_leaves();
+        } catch (const std::exception&) {
+            ok = false;
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(rt.stream, &g);
+        ok = ok && e == cudaSuccess && g != nullptr && rt.host_syncs == syncs && rt.allocs == allocs;
+        if (ok) ok = cudaGraphInstantiate(&rt.graph_exec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            cudaGetLastError();
+            if (rt.graph_exec) cudaGraphExecDestroy(rt.graph_exec);
+            rt.graph_exec = nullptr;
+            rt.graph_allowed = false;
+            rt.steady_epoch = ~0ull;
+            if (rt.trace) std::fprintf(stderr, "[cospan] capture failed: forwards run eagerly\n");
+            run_leaves();  // the forward itself, eagerly
+            return true;
+        }
+        rt.graph_epoch = rt.epoch;
+        ++rt.graph_captures;
+        detail::cuda_check(cudaGraphLaunch(rt.graph_exec, rt.stream), "launching a captured forward");
+        return true;
+    }
+    void run_leaves() {
         auto& rt = *rt_;
         // shape hooks run once per forward, when their target's shape is first needed
         for (auto& v : rt.vars)
@@ -1063,8 +1149,9 @@ public:
             }
             run_leaf(i);
         }
-        for (auto& v : rt.views) push(*v);
     }
+
+public:
     void wait() {
         detail::cuda_check(cudaStreamSynchronize(rt_->stream), "wait");
         std::uint32_t status = 0;
@@ -1111,6 +1198,7 @@ private:
         auto s = std::make_shared<detail::ViewState>();
         s->var = v.id;
         rt_->views.push_back(s);
+        ++rt_->epoch;  // a viewed variable may change what the fast paths do
         push(*s);
         return HostView<DT, R>(s);
     }
@@ -1126,6 +1214,7 @@ private:
         s->var = v.id;
         s->ragged = true;
         rt_->views.push_back(s);
+        ++rt_->epoch;
         push(*s);
         return HostRagged<DT, R>(s);
     }

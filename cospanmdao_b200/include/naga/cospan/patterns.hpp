@@ -89,10 +89,11 @@ struct FastState {
                 if (v->var == iv) return false;
         return true;
     }
-    void* workspace(std::size_t bytes) {
+    void* workspace(Runtime& rt, std::size_t bytes) {
         if (bytes > ws_bytes) {
             if (ws) cudaFree(ws);
             ws = nullptr;
+            ++rt.allocs;
             cuda_check(cudaMalloc(&ws, bytes), "fast-path workspace");
             ws_bytes = bytes;
         }
@@ -104,6 +105,7 @@ struct FastState {
             Var& v = rt.vars[std::size_t(scale_vars[k])];
             if (v.version == scale_version[k]) continue;
             float h = 0.f;
+            ++rt.host_syncs;
             cuda_check(cudaStreamSynchronize(rt.stream), "scale");
             cuda_check(cudaMemcpy(&h, v.data, sizeof(float), cudaMemcpyDeviceToHost), "scale");
             scale[k] = h;
@@ -198,7 +200,7 @@ inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
         d.x = static_cast<float*>(rt.var_of_port(cred, "x").data);
         d.w = static_cast<float*>(rt.var_of_port(gemv, "y").data);
         d.workspace_bytes = cspb_gemver_workspace_bytes(n);
-        d.workspace = st->workspace(d.workspace_bytes);
+        d.workspace = st->workspace(rt, d.workspace_bytes);
         if (rt.trace)
             std::fprintf(stderr, "[cospan] fast path cspb_gemver_fused n=%lld for '%s' .. '%s'\n", (long long)n,
                          r2u->path().c_str(), gemv->path().c_str());
@@ -272,7 +274,7 @@ inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
         d.q = static_cast<float*>(rt.vars[std::size_t(vq)].data);
         d.s = static_cast<float*>(rt.vars[std::size_t(vs)].data);
         d.workspace_bytes = cspb_bicgk_workspace_bytes(n);
-        d.workspace = st->workspace(d.workspace_bytes);
+        d.workspace = st->workspace(rt, d.workspace_bytes);
         if (rt.trace)
             std::fprintf(stderr, "[cospan] fast path cspb_bicgk_fused n=%lld for '%s' .. '%s'\n", (long long)n,
                          c0->path().c_str(), c2->path().c_str());
@@ -369,7 +371,7 @@ inline bool try_ns(Runtime& rt, const PatternLeaves& L, std::size_t a) {
             const int ny = int(U.shape[1]), nx = int(U.shape[2]);
             const std::size_t wsb = cspb_ns_comp_workspace_bytes(nx, ny);
             // the kernel's workspace, then its 18 diagnostics
-            char* ws = static_cast<char*>(st->workspace((wsb + 255) / 256 * 256 + 256));
+            char* ws = static_cast<char*>(st->workspace(rt, (wsb + 255) / 256 * 256 + 256));
             float* diag = reinterpret_cast<float*>(ws + (wsb + 255) / 256 * 256);
             cspb_ns_comp_desc d{};
             d.nx = nx;

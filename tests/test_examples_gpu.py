@@ -24,8 +24,9 @@ def _run(args, timeout=300, env=None):
 
 
 # "fast": the runtime's registered fast paths (patterns.hpp) run the GEMVER and BiCGK stages as cspb kernels;
-# "generic": every component runs its own body (NAGA_COSPAN_GENERIC)
-MODES = {"fast": {}, "generic": {"NAGA_COSPAN_GENERIC": "1"}}
+# "generic": every component runs its own body (NAGA_COSPAN_GENERIC); "eager": the fast paths with no CUDA-graph
+# replay of steady forwards (NAGA_COSPAN_NO_GRAPH)
+MODES = {"fast": {}, "generic": {"NAGA_COSPAN_GENERIC": "1"}, "eager": {"NAGA_COSPAN_NO_GRAPH": "1"}}
 
 
 def test_runtime_fused_groups(cuda):
@@ -40,6 +41,13 @@ def test_runtime_ragged(cuda):
     with changing counts, declared counts at connects, dense rows read as blocks, the hook's error flags, host views,
     and ragged stages inside a fused group (the reference refuses those)."""
     rc, out = _run(["runtime-ragged"])
+    assert rc == 0 and "ALL OK" in out, out
+
+
+def test_runtime_replay(cuda):
+    """CUDA-graph replay of steady forwards (tests/runtime/replay.cu): captured after one steady forward, replayed
+    bit-identical to eager forwards, dropped by update_input, never used for a model whose hooks read the device."""
+    rc, out = _run(["runtime-replay"])
     assert rc == 0 and "ALL OK" in out, out
 
 
