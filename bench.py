@@ -264,10 +264,17 @@ def bench_gemver_bf16(torch, cb, dist, args):
         ms = timed(torch, dist, step, args.steps, args.warmup)
         nbytes = gemver_bytes(n, a_bytes=2, store_B=store, second_read_bytes=2)
         res["store_B" if store else "no_B"] = {"ms": ms, "gbs": nbytes / (ms * 1e-3) / 1e9, "bytes": nbytes}
+    # without Â the default schedule is the low-rank form (the rank-2 update as dot products): its own error check
+    xl = torch.empty_like(x)
+    wl = torch.empty_like(w)
+    cb.gemver(A16, d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2, want_B=False, x=xl, w=wl,
+              workspace=ws)
     cb.gemver(A16, d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2, B=B, x=x, w=w,
               workspace=ws)
     B64, x64, w64 = gemver_f64_reference(torch, d, 1.5, 1.2)  # the f32 matrix: storage error included
-    res["err_vs_f64_of_f32_A"] = {"B": relerr(torch, B, B64), "x": relerr(torch, x, x64), "w": relerr(torch, w, w64)}
+    res["err_vs_f64_of_f32_A"] = {"B": relerr(torch, B, B64), "x": relerr(torch, x, x64), "w": relerr(torch, w, w64),
+                                  "x_no_B": relerr(torch, xl, x64), "w_no_B": relerr(torch, wl, w64)}
+    res["no_B"]["schedule"] = "lowrank"
     del B64, x64, w64, B, A16, d
     torch.cuda.empty_cache()
     return res

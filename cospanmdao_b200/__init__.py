@@ -142,14 +142,16 @@ def _mat_dtype(t):
 
 # ---- GEMVER family ------------------------------------------------------------------------------------------------
 def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: bool = True, B=None, x=None, w=None,
-           schedule: str = "barrier", lag: int = 0, workspace: Workspace | None = None, stream=None):
+           schedule: str = "auto", lag: int = 0, workspace: Workspace | None = None, stream=None):
     """Â = A + u1·v1ᵀ + u2·v2ᵀ, x = β·Âᵀy + z, w = α·Â·x in one launch. A: (n, n) float32 or bfloat16 (a row
-    stride from A.stride(0) is honoured). schedule 'barrier' (three streaming passes, the default), 'bulk' (the same
-    passes fed through a shared-memory ring by bulk copies; used when n is a multiple of 4 (f32) / 8 (bf16) and the
-    operands are 16-byte aligned, else 'barrier') or 'panel' (column panels pipelined through L2); all give the same
-    bits. Returns (B or None, x, w)."""
-    if schedule not in ("panel", "barrier", "bulk"):
-        raise ValueError("schedule must be 'barrier', 'bulk' or 'panel'")
+    stride from A.stride(0) is honoured). schedule 'barrier' (three streaming passes), 'bulk' (the same passes fed
+    through a shared-memory ring by bulk copies; used when n is a multiple of 4 (f32) / 8 (bf16) and the operands are
+    16-byte aligned, else 'barrier') or 'panel' (column panels pipelined through L2) all give the same bits.
+    'lowrank' (only without Â: want_B False and no B) applies the rank-2 update as four dot products, so both passes
+    over A are plain GEMVs: other rounding, within the f64 tolerance. 'auto' (the default) is 'lowrank' for a bfloat16
+    matrix without Â and 'barrier' otherwise. Returns (B or None, x, w)."""
+    if schedule not in ("auto", "panel", "barrier", "bulk", "lowrank"):
+        raise ValueError("schedule must be 'auto', 'barrier', 'bulk', 'panel' or 'lowrank'")
     torch = _torch()
     if A is None or A.dim() != 2 or A.shape[0] != A.shape[1]:
         raise ValueError("'A' must be a square matrix")
@@ -175,7 +177,10 @@ def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: b
     wp, wb = ws.ptr(need)
     if not 0 <= int(lag) <= 255:
         raise ValueError("lag must be in [0, 255]")
-    flags = {"panel": _capi.GEMVER_PANEL, "bulk": _capi.GEMVER_BULK}.get(schedule, 0) | (int(lag) << 8)
+    if schedule == "auto":
+        schedule = "lowrank" if B is None and A.dtype == torch.bfloat16 else "barrier"
+    flags = {"panel": _capi.GEMVER_PANEL, "bulk": _capi.GEMVER_BULK,
+             "lowrank": _capi.GEMVER_LOWRANK}.get(schedule, 0) | (int(lag) << 8)
     d = _capi.GemverDesc(n, A.stride(0), B.stride(0) if B is not None else n, _mat_dtype(A), flags, _ptr(A), _ptr(u1),
                          _ptr(v1), _ptr(u2), _ptr(v2), _ptr(y), _ptr(z), float(alpha), float(beta), _ptr(B), _ptr(x),
                          _ptr(w), wp, wb)

@@ -68,6 +68,45 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
     rowsum_finish(g.p2);
 }
 
+// GEMVER without Â (flag CSPB_GEMVER_LOWRANK, B not requested): the rank-2 update is applied as four dot products,
+//   Âᵀy = Aᵀy + v1(u1·y) + v2(u2·y),   Â·x = A·x + u1(v1·x) + u2(v2·x),
+// so the two passes over A are plain streaming GEMVs (column sums of A·y, then row dots of A·x) with no per-element
+// update, and the finishes add the rank-2 terms. The dots are formed by every block in the same order (block_dot2),
+// in f64. Measured at n = 16384 with bf16 storage, forming Â per element made each pass issue-bound at 3.3 TB/s.
+// Other rounding than the schedules that form Â (closer to the f64 result, not the same bits).
+struct LowRankK {
+    PassArgs p1, p2;
+    uint32_t* ctrl;
+    int64_t units;
+    const float *u1, *v1, *u2, *v2, *y, *z;
+    float beta;
+    float* x;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kPassThreads, 2) k_gemver_lr(LowRankK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        pass_unit<T, kWX, true, false, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
+        u = share_work(next);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    double s1, s2;
+    block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
+    colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, s1, s2, g.x);
+    if (!grid_barrier(g.ctrl)) return;
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+        pass_unit<T, kWX, true, false, false, false, true, 16, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, smem);
+        u = share_work(next);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    double t1, t2;
+    block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
+    rowsum_finish_lr(g.p2, g.u1, g.u2, t1, t2);
+}
+
 // The same three passes with the matrix streamed through a shared-memory ring by bulk copies (bulkpass.cuh): one
 // CTA per SM, 8 consumer warps and a producer warp; the results are bit-identical to k_gemver's.
 template <typename T, bool P2_FROM_B, int NST>
@@ -387,7 +426,8 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     if (n > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y || !d->x || !d->w) return CSPB_ERR_ARGUMENT;
     if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
-    if ((d->flags & ~(CSPB_GEMVER_PANEL | CSPB_GEMVER_BULK | CSPB_GEMVER_LAG_MASK)) != 0) return CSPB_ERR_UNSUPPORTED;
+    if ((d->flags & ~(CSPB_GEMVER_PANEL | CSPB_GEMVER_BULK | CSPB_GEMVER_LOWRANK | CSPB_GEMVER_LAG_MASK)) != 0)
+        return CSPB_ERR_UNSUPPORTED;
     const bool bf16 = d->a_dtype == CSPB_BF16;
     const PassLayout L = pass_layout(n, kS, bf16 ? kCW16 : kCW32, 1, false);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
@@ -424,6 +464,24 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t zero = L.off_PA;  // ctrl, strip_done, chunk_done, x_ready
 
+    // without Â, the low-rank form (takes precedence over the schedule flags)
+    if ((d->flags & CSPB_GEMVER_LOWRANK) && d->B == nullptr) {
+        LowRankK g{};
+        g.p1 = p1;
+        g.p1.dst = nullptr;
+        g.p1.u1 = g.p1.v1 = g.p1.u2 = g.p1.v2 = nullptr;
+        g.p2 = p2;
+        g.ctrl = reinterpret_cast<uint32_t*>(ws);
+        g.units = L.units;
+        g.u1 = d->u1; g.v1 = d->v1; g.u2 = d->u2; g.v2 = d->v2;
+        g.y = d->y;
+        g.z = d->z;
+        g.beta = d->beta;
+        g.x = d->x;
+        void* args[] = {&g, const_cast<int*>(&vec_ok)};
+        if (bf16) return launch_coop(k_gemver_lr<__nv_bfloat16>, args, L.units, zero, ws, st);
+        return launch_coop(k_gemver_lr<float>, args, L.units, zero, ws, st);
+    }
     // the bulk-copy ring: every row segment and vector piece must start on 16 bytes and be a multiple of 16 bytes long
     const int vw = bf16 ? 8 : 4;
     const bool bulk_ok = vec_ok && n % vw == 0 && (d->lda * eb) % 16 == 0 && (!d->B || (d->ldb * 4) % 16 == 0) &&

@@ -440,4 +440,82 @@ __device__ __forceinline__ void colsum_finish_cols(const double* P, int64_t stri
     }
 }
 
+// a·b and c·b over [0, n) in f64, formed by ONE block in a fixed order (thread-strided sums, then a fixed tree), so
+// every block of a grid that calls it gets the same two values. For the low-rank GEMVER's finishes.
+__device__ __forceinline__ void block_dot2(const float* a, const float* c, const float* b, int64_t n, double& ab,
+                                           double& cb) {
+    __shared__ double s_red[2][kPassThreads / 32];
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const double bj = double(__ldcg(b + j));
+        s0 = __fma_rn(double(__ldcg(a + j)), bj, s0);
+        s1 = __fma_rn(double(__ldcg(c + j)), bj, s1);
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        s0 += __shfl_xor_sync(kFull, s0, off);
+        s1 += __shfl_xor_sync(kFull, s1, off);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) {
+        s_red[0][warp] = s0;
+        s_red[1][warp] = s1;
+    }
+    __syncthreads();
+    double t0 = 0.0, t1 = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+        t0 += s_red[0][w];
+        t1 += s_red[1][w];
+    }
+    ab = t0;
+    cb = t1;
+}
+
+// x[j] = float(z[j] + scale·(Σ_strips P[st][j] + v1[j]·s1 + v2[j]·s2)): colsum_finish with the low-rank terms of
+// Âᵀy = Aᵀy + v1(u1·y) + v2(u2·y) (s1 = u1·y, s2 = u2·y).
+__device__ __forceinline__ void colsum_finish_lr(const double* P, int64_t strips, int64_t n, const float* z, float scale,
+                                                 const float* v1, const float* v2, double s1, double s2, float* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t base = gtid - lane; base < 4 * n; base += gthreads) {
+        const int64_t item = base + lane;
+        const bool valid = item < 4 * n;
+        const int64_t j = item >> 2;
+        const int q = int(item & 3);
+        double s = valid ? strided_strip_sum(P, strips, n, j, q) : 0.0;
+        s += __shfl_xor_sync(kFull, s, 1);
+        s += __shfl_xor_sync(kFull, s, 2);
+        if (valid && q == 0) {
+            s = __fma_rn(double(__ldcg(v1 + j)), s1, s);
+            s = __fma_rn(double(__ldcg(v2 + j)), s2, s);
+            const double zz = z ? double(__ldcg(z + j)) : 0.0;
+            out[j] = float(zz + double(scale) * s);
+        }
+    }
+}
+
+// w[i] = float(scale·(Σ_c Wp[c][i] + u1[i]·t1 + u2[i]·t2)): rowsum_finish with the low-rank terms of Â·x = A·x +
+// u1(v1·x) + u2(v2·x) (t1 = v1·x, t2 = v2·x); the chunk sums in index order, in f32 as rowsum_finish, then f64.
+__device__ __forceinline__ void rowsum_finish_lr(const PassArgs& a, const float* u1, const float* u2, double t1, double t2) {
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t row = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < a.n; row += gthreads) {
+        float s = 0.f;
+        int64_t c = 0;
+        for (; c + 16 <= a.chunks; c += 16) {
+            float v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = __ldcg(a.Wp + (c + q) * a.n + row);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) s += v[q];
+        }
+        for (; c < a.chunks; ++c) s += __ldcg(a.Wp + c * a.n + row);
+        double d = double(s);
+        d = __fma_rn(double(__ldcg(u1 + row)), t1, d);
+        d = __fma_rn(double(__ldcg(u2 + row)), t2, d);
+        a.rout1[row] = float(double(a.rscale1) * d);
+    }
+}
+
 }  // namespace cspb

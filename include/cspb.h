@@ -83,6 +83,11 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
  * ================================================================================================================== */
 #define CSPB_GEMVER_PANEL 1
 #define CSPB_GEMVER_BULK 2
+/* flags = CSPB_GEMVER_LOWRANK with B == NULL: x and w are formed from A with the rank-2 update applied as four dot
+ * products, x = β·(Aᵀy + v1(u1·y) + v2(u2·y)) + z and w = α·(A·x + u1(v1·x) + u2(v2·x)), in two streaming passes with
+ * no per-element update. Other rounding than the schedules that form Â (within the f64 tolerance, not the same bits);
+ * ignored when B is requested. No counterpart in the reference, whose GEMVER always forms B. */
+#define CSPB_GEMVER_LOWRANK 4
 /* bits 8..15 of flags: the panel schedule's lag (pass 2 over a panel follows pass 1 over it by this many panels);
  * 0 = automatic (the panels the blocks in flight hold, plus one). A tuning knob: results do not depend on it. */
 #define CSPB_GEMVER_LAG_MASK 0xff00

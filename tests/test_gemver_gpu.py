@@ -217,3 +217,33 @@ def test_gemver_rejects_bad_ports(cuda):
         cb.gemver(d["A"], d["u1"][:10], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1, beta=1)
     with pytest.raises(ValueError):
         cb.gemver(d["A"].double(), d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1, beta=1)
+
+
+@pytest.mark.parametrize("n,dtype_name,lda", [(777, "float32", 777), (2048, "bfloat16", 2048), (1001, "bfloat16", 1008),
+                                              (4104, "bfloat16", 4104), (257, "float32", 261), (64, "bfloat16", 72)])
+def test_gemver_lowrank_against_f64(cuda, n, dtype_name, lda):
+    """Without Â, the low-rank form (the rank-2 update as four dot products): x and w against the f64 GEMVER of the
+    same (bf16-rounded) matrix, bit-identical on a repeat, and the flag is ignored when Â is requested."""
+    import torch
+    import cospanmdao_b200 as cb
+    dt = getattr(torch, dtype_name)
+    full = torch.empty((n, lda), dtype=torch.float32, device=cuda)
+    cb.fill_hash(full, 41, 0)
+    A = full.to(dt)[:, :n]
+    d = _inputs(torch, n, seed=11)
+    args = (A, d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"])
+    B, x, w = cb.gemver(*args, alpha=0.8, beta=-1.3, want_B=False, schedule="lowrank")
+    assert B is None
+    Ah = _np(A.float())
+    h = {k: _np(v) for k, v in d.items()}
+    xo, wo, _ = oracle.gemver_f64(n, Ah, h["u1"], h["v1"], h["u2"], h["v2"], h["y"], h["z"], 0.8, -1.3)
+    assert oracle.rel_l2(_np(x), xo) < TOL and oracle.rel_l2(_np(w), wo) < TOL
+    _, x2, w2 = cb.gemver(*args, alpha=0.8, beta=-1.3, want_B=False, schedule="lowrank")
+    assert torch.equal(x, x2) and torch.equal(w, w2)
+    if dtype_name == "bfloat16":  # the default for a bf16 matrix without Â
+        _, x3, w3 = cb.gemver(*args, alpha=0.8, beta=-1.3, want_B=False)
+        assert torch.equal(x, x3) and torch.equal(w, w3)
+    # with Â requested the flag is ignored: the barrier schedule's bits
+    Bb, xb, wb = cb.gemver(*args, alpha=0.8, beta=-1.3, schedule="barrier")
+    Bl, xl, wl = cb.gemver(*args, alpha=0.8, beta=-1.3, schedule="lowrank")
+    assert torch.equal(Bb, Bl) and torch.equal(xb, xl) and torch.equal(wb, wl)
