@@ -35,6 +35,7 @@ BF16 = 1
 GEMVER_PANEL = 1
 GEMVER_BULK = 2
 GEMVER_LOWRANK = 4
+BATCH_LOWRANK = 1 << 16
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p

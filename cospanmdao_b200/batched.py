@@ -100,9 +100,14 @@ class RaggedBatch:
         return out
 
     # ---- the launch ------------------------------------------------------------------------------------------------
-    def run(self, tune: int = 0, stream=None, check: bool = False):
+    def run(self, tune: int = 0, stream=None, check: bool = False, lowrank: bool | None = None):
+        """One launch over the batch. lowrank: instances without B take the low-rank form (the rank-2 update as dot
+        products); None follows cb.gemver's 'auto' schedule (bf16 without B)."""
         import cospanmdao_b200 as cb
         torch = _torch()
+        if lowrank is None:
+            lowrank = self.dtype == torch.bfloat16 and self.B is None
+        tune = int(tune) | (_capi.BATCH_LOWRANK if lowrank else 0)
         p = int(self.ws.data_ptr())
         wp = (p + 255) // 256 * 256
         d = _capi.BatchedDesc(self.count, self.max_elems, self.max_vec, BF16 if self.dtype == torch.bfloat16 else F32,

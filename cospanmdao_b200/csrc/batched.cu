@@ -190,14 +190,48 @@ __device__ __forceinline__ void instance_x(const PassArgs& a, const float* z, fl
     }
 }
 
-template <typename T, int WX>
-__device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(a, unit, vec_ok, smem);
+// x over [c0, c1) in the low-rank form (no Â): x[j] = z[j] + β · (Σ_s P[s][j] + v1[j]·s1 + v2[j]·s2), the strips in
+// order as instance_x, s1 = u1·y and s2 = u2·y (block_dot2: every block of the instance forms the same two values).
+__device__ __forceinline__ void instance_x_lr(const PassArgs& a, const float* z, float beta, float* x, int64_t c0,
+                                              int64_t c1) {
+    double s1, s2;
+    block_dot2(a.u1, a.u2, a.cyB, a.n, s1, s2);
+    for (int64_t j = c0 + threadIdx.x; j < c1; j += blockDim.x) {
+        double s = 0.0;
+        int64_t st = 0;
+        for (; st + 8 <= a.strips; st += 8) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = __ldcg(a.PB + (st + k) * a.n + j);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) s += v[k];
+        }
+        for (; st < a.strips; ++st) s += __ldcg(a.PB + st * a.n + j);
+        s = __fma_rn(double(__ldcg(a.v1 + j)), s1, s);
+        s = __fma_rn(double(__ldcg(a.v2 + j)), s2, s);
+        const double zz = z ? double(__ldcg(z + j)) : 0.0;
+        x[j] = float(zz + double(beta) * s);
+    }
 }
-// Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update.
-template <typename T, int WX>
+
+// rows in flight of the low-rank units (16-bit storage: 8, which keeps every variant of this kernel free of spills;
+// the batching does not change the arithmetic)
+template <typename T> inline constexpr int kLrRows = sizeof(T) == 4 ? 16 : 8;
+
+// LR: an instance without Â takes the low-rank form of cspb_gemver_fused with CSPB_GEMVER_LOWRANK (column sums of
+// A·y, then row dots of A·x; the rank-2 terms in the finishes).
+template <typename T, int WX, bool LR>
+__device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
+    if (LR && a.dst == nullptr) pass_unit<T, WX, true, false, false, true, false, kLrRows<T>>(a, unit, vec_ok, smem);
+    else pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(a, unit, vec_ok, smem);
+}
+// Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update
+// (or, low-rank, without it).
+template <typename T, int WX, bool LR>
 __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    if (sizeof(T) == 4 && a.dst != nullptr) {
+    if (LR && a.dst == nullptr) {
+        pass_unit<T, WX, true, false, false, false, true, kLrRows<T>, true>(a, unit, vec_ok, smem);
+    } else if (sizeof(T) == 4 && a.dst != nullptr) {
         PassArgs b = a;
         b.src = a.dst;
         b.lds = a.ldd;
@@ -208,7 +242,7 @@ __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_
     }
 }
 
-template <typename T>
+template <typename T, bool LR>
 __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     constexpr bool bf16 = sizeof(T) == 2;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, 1>() > pass_smem_bytes<T, 4>()
@@ -276,17 +310,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 const int64_t c = unit % a.chunks, strip = unit / a.chunks;
                 if (!pass2) {
                     switch (wx) {
-                        case 1: unit1<T, 1>(a, unit, vec_ok, smem); break;
-                        case 4: unit1<T, 4>(a, unit, vec_ok, smem); break;
-                        default: unit1<T, 2>(a, unit, vec_ok, smem); break;
+                        case 1: unit1<T, 1, LR>(a, unit, vec_ok, smem); break;
+                        case 4: unit1<T, 4, LR>(a, unit, vec_ok, smem); break;
+                        default: unit1<T, 2, LR>(a, unit, vec_ok, smem); break;
                     }
                     count_done(g.chunk_done + ubase + uint64_t(c));
                 } else {
                     if (!wait_for(g.x_ready + ubase + uint64_t(c), 1u)) { stop = true; break; }
                     switch (wx) {
-                        case 1: unit2<T, 1>(a, unit, vec_ok, smem); break;
-                        case 4: unit2<T, 4>(a, unit, vec_ok, smem); break;
-                        default: unit2<T, 2>(a, unit, vec_ok, smem); break;
+                        case 1: unit2<T, 1, LR>(a, unit, vec_ok, smem); break;
+                        case 4: unit2<T, 4, LR>(a, unit, vec_ok, smem); break;
+                        default: unit2<T, 2, LR>(a, unit, vec_ok, smem); break;
                     }
                     count_done(g.strip_done + sbase + uint64_t(strip));
                 }
@@ -298,7 +332,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 if (!wait_for(g.chunk_done + ubase + uint64_t(c), uint32_t(a.strips))) { stop = true; break; }
                 const int64_t CW = cols_of(wx, bf16);
                 const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
-                instance_x(a, z, beta, x, c * CW, c1);
+                if (LR && a.dst == nullptr) instance_x_lr(a, z, beta, x, c * CW, c1);
+                else instance_x(a, z, beta, x, c * CW, c1);
                 __syncthreads();
                 if (threadIdx.x == 0) {
                     __threadfence();
@@ -311,6 +346,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 const int64_t strip = int64_t(f - sbase);
                 if (!wait_for(g.strip_done + sbase + uint64_t(strip), uint32_t(a.chunks))) { stop = true; break; }
                 const int64_t S = rows_of(wx);
+                const bool lr = LR && a.dst == nullptr;
+                double t1 = 0.0, t2 = 0.0;
+                if (lr) block_dot2(a.v1, a.v2, a.xv, a.n, t1, t2);  // x is complete: every chunk fed this strip
                 for (int64_t row = strip * S + threadIdx.x; row < (strip + 1) * S && row < a.n; row += blockDim.x) {
                     float sum = 0.f;
                     int64_t cc = 0;
@@ -322,7 +360,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                         for (int t = 0; t < 16; ++t) sum += v[t];
                     }
                     for (; cc < a.chunks; ++cc) sum += __ldcg(a.Wp + cc * a.n + row);
-                    a.rout1[row] = a.rscale1 * sum;
+                    if (lr) {
+                        double dd = double(sum);
+                        dd = __fma_rn(double(__ldcg(a.u1 + row)), t1, dd);
+                        dd = __fma_rn(double(__ldcg(a.u2 + row)), t2, dd);
+                        a.rout1[row] = float(double(a.rscale1) * dd);
+                    } else {
+                        a.rout1[row] = a.rscale1 * sum;
+                    }
                 }
             }
             __syncthreads();  // s_ok and the unit's shared memory are reused by the next item
@@ -399,6 +444,8 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
               void* workspace, size_t workspace_bytes, void* stream) {
     if (count < 1 || count > (int64_t(1) << 26) || max_elems < 1 || max_vec < 1) return CSPB_ERR_ARGUMENT;
     if (a_dtype != CSPB_F32 && a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    const bool lowrank = (tune & CSPB_BATCH_LOWRANK) != 0;
+    tune &= ~CSPB_BATCH_LOWRANK;
     if (tune < 0 || tune >= cspb_gemver_batched_tunings()) return CSPB_ERR_UNSUPPORTED;
     for (uint32_t b = 0; b < 4; ++b)
         if (((uint32_t(tune) >> (2 * b)) & 3u) == 3u) return CSPB_ERR_UNSUPPORTED;
@@ -464,8 +511,10 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     g.x_ready = reinterpret_cast<uint32_t*>(ws + L.off_xr);
     g.cap_units = L.capU;
     g.ctrl = reinterpret_cast<uint32_t*>(ws);
-    const void* kern = bf16 ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16>)
-                            : reinterpret_cast<const void*>(batch::k_run<float>);
+    const void* kern = bf16 ? (lowrank ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, true>)
+                                       : reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, false>))
+                            : (lowrank ? reinterpret_cast<const void*>(batch::k_run<float, true>)
+                                       : reinterpret_cast<const void*>(batch::k_run<float, false>));
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, batch::kThreads, 0) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;

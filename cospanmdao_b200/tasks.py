@@ -9,6 +9,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
+from . import _capi
 from ._capi import BF16, F32, lib
 
 GEMVER_TASK = np.dtype([("n", "<i8"), ("lda", "<i8"), ("ldb", "<i8"), ("A", "<u8"), ("B", "<u8"), ("u1", "<u8"),
@@ -57,7 +58,11 @@ class TaskRunner:
             dst.copy_(src, non_blocking=host_staging is not None)
         return addr
 
-    def gemver(self, table: np.ndarray, *, bf16: bool, tune: int = 0, stream=None, host_staging=None):
+    def gemver(self, table: np.ndarray, *, bf16: bool, tune: int = 0, lowrank: bool | None = None, stream=None,
+               host_staging=None):
+        """Runs a GEMVER task table. lowrank: tasks without B take the low-rank form (the rank-2 update as dot
+        products); None (the default) follows cb.gemver's 'auto' schedule, so that every task gets the single call's
+        form: low-rank for bf16, not for f32."""
         import cospanmdao_b200 as cb
         torch = _torch()
         count = int(table.size)
@@ -70,7 +75,10 @@ class TaskRunner:
         taddr = self.upload(table, s, host_staging)
         need = int(lib().cspb_gemver_batched_workspace_bytes(count, max_elems, max_vec))
         wp, wb = self._buf("_ws", need)
-        st = lib().cspb_gemver_tasks(C.c_void_p(taddr), count, max_elems, max_vec, BF16 if bf16 else F32, int(tune),
+        if lowrank is None:
+            lowrank = bf16
+        word = int(tune) | (_capi.BATCH_LOWRANK if lowrank else 0)
+        st = lib().cspb_gemver_tasks(C.c_void_p(taddr), count, max_elems, max_vec, BF16 if bf16 else F32, word,
                                      C.c_void_p(wp), wb, C.c_void_p(int(s.cuda_stream)))
         cb._raise(st, "gemver tasks")
         return wp

@@ -221,6 +221,10 @@ typedef struct cspb_gemver_task {
     float beta;
 } cspb_gemver_task;
 
+/* tune | CSPB_BATCH_LOWRANK (both batched entry points): an instance or task without B takes the low-rank form of
+ * cspb_gemver_fused with CSPB_GEMVER_LOWRANK (the rank-2 update as dot products in the finishes); instances with B
+ * are unchanged. */
+#define CSPB_BATCH_LOWRANK (1 << 16)
 int cspb_gemver_tasks(const cspb_gemver_task* tasks, int64_t count, int64_t max_elems, int64_t max_vec,
                       int32_t a_dtype, int32_t tune, void* workspace, size_t workspace_bytes, void* stream);
 
