@@ -280,6 +280,34 @@ def bench_gemver_bf16(torch, cb, dist, args):
     return res
 
 
+def bench_sharded(torch, cb, dist, args):
+    """ONE GEMVER of size n split by rows over the job's ranks (cospanmdao_b200.sharded): strong scaling, the rank's
+    rows per GPU plus one exchange of the n f64 column-sum shares (all-gather over NCCL, summed in rank order). ms is
+    the max over ranks; GB/s is the whole GEMVER's algorithmic bytes over it."""
+    from cospanmdao_b200 import workloads
+    from cospanmdao_b200.sharded import gemver_sharded, shard_rows
+    n = args.n
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = workloads.gemver_inputs(n, 0, device=dev)  # every rank builds the same GEMVER and takes its rows
+    r0, r1 = shard_rows(n, dist.world)[dist.rank]
+    A = d["A"][r0:r1].contiguous()
+    rows = {k: d[k][r0:r1].contiguous() for k in ("u1", "u2", "y")}
+    del d["A"]
+    ws = cb.Workspace(dev)
+    ranks = dist.r if dist.world > 1 else None
+
+    def step():
+        gemver_sharded(A, rows["u1"], d["v1"], rows["u2"], d["v2"], rows["y"], d["z"], alpha=1.5, beta=1.2,
+                       ranks=ranks, workspace=ws)
+
+    ms = timed(torch, dist, step, args.steps, args.warmup)
+    nbytes = gemver_bytes(n)
+    del A, rows, d
+    torch.cuda.empty_cache()
+    return {"ms": ms, "gbs_whole_gemver": nbytes / (ms * 1e-3) / 1e9, "ranks": dist.world, "rows_per_rank": r1 - r0,
+            "scaling": "strong", "exchange_bytes_per_rank": 8 * n}
+
+
 def bench_chain(torch, cb, dist, args):
     from cospanmdao_b200 import workloads
     n = args.n
@@ -584,6 +612,7 @@ def main(argv=None) -> int:
     secondaries = {
         "gemver_bf16_storage": lambda: bench_gemver_bf16(torch, cb, dist, args),
         "gemver_chain": lambda: bench_chain(torch, cb, dist, args),
+        "gemver_sharded": lambda: bench_sharded(torch, cb, dist, args),
         "ns_residual": lambda: bench_ns(torch, cb, dist, args),
         "ragged_batch": lambda: bench_ragged(torch, cb, dist, args, pk),
         "serving": lambda: bench_serving(torch, dist, args),

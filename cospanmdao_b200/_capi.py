@@ -54,6 +54,13 @@ class GemverDesc(C.Structure):
                 ("workspace", vp), ("workspace_bytes", sz)]
 
 
+class GemverRowsDesc(C.Structure):
+    _fields_ = [("n", i64), ("rows", i64), ("lda", i64), ("ldb", i64), ("a_dtype", i32), ("flags", i32),
+                ("A", vp), ("u1", vp), ("v1", vp), ("u2", vp), ("v2", vp), ("y", vp), ("z", vp),
+                ("alpha", C.c_float), ("beta", C.c_float), ("B", vp), ("x", vp), ("w", vp),
+                ("workspace", vp), ("workspace_bytes", sz)]
+
+
 class BicgkDesc(C.Structure):
     _fields_ = [("n", i64), ("ldb", i64), ("b_dtype", i32), ("flags", i32), ("B", vp), ("p", vp), ("r", vp),
                 ("q", vp), ("s", vp), ("workspace", vp), ("workspace_bytes", sz)]
@@ -101,6 +108,9 @@ PROTOTYPES = {
     "cspb_read_status": (C.c_int, [vp, C.POINTER(u32), vp]),
     "cspb_gemver_workspace_bytes": (sz, [i64]),
     "cspb_gemver_fused": (C.c_int, [C.POINTER(GemverDesc), vp]),
+    "cspb_gemver_rows_workspace_bytes": (sz, [i64, i64]),
+    "cspb_gemver_rows_partial": (C.c_int, [C.POINTER(GemverRowsDesc), vp, vp]),
+    "cspb_gemver_rows_finish": (C.c_int, [C.POINTER(GemverRowsDesc), vp, vp]),
     "cspb_bicgk_workspace_bytes": (sz, [i64]),
     "cspb_bicgk_fused": (C.c_int, [C.POINTER(BicgkDesc), vp]),
     "cspb_chain_workspace_bytes": (sz, [i64]),

@@ -161,6 +161,7 @@ __device__ __forceinline__ PassArgs instance_args(const RunK& g, int64_t k, int 
         vec_ok = true;  // rows padded to 8 elements, A and B 16-byte aligned (checked by the host)
     }
     a.n = n;
+    a.rows = n;
     a.PB = g.P + __ldcg(g.off[SP] + k);
     a.Wp = g.Wp + __ldcg(g.off[SW] + k);
     a.strip_done = g.strip_done + __ldcg(g.off[SS] + k);

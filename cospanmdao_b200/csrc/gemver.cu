@@ -299,6 +299,59 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain_g2(ChainK g, int vec_
     rowsum_finish(g.p4);
 }
 
+// Row shards of ONE GEMVER across GPUs (one process per GPU). A shard holds rows [r0, r0 + rows) of A, u1, u2, y and
+// all of v1, v2, z. The only exchange is the column sums: Âᵀy = Σ over shards of the shard's rows' share.
+//   partial: Â rows (stored when B is given) and the shard's f64 column sums colsum[j] = Σ_{i in shard} Â[i][j]·y[i]
+//   (the caller adds the shards' colsum in rank order, the same total on every rank)
+//   finish:  x = float(z + β·total) over all n columns, then w = α·Â·x over the shard's rows (pass 2 of k_gemver)
+struct RowsK {
+    PassArgs p;
+    uint32_t* ctrl;
+    int64_t units;
+    double* colsum;
+    const double* total;
+    const float* z;
+    float beta;
+    float* x;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kPassThreads, 2) k_rows_partial(RowsK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        pass_unit<T, kWX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(g.p, u, vec_ok != 0, smem);
+        u = share_work(next);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_f64(g.p.PB, g.p.strips, g.p.n, g.colsum);
+}
+
+// FROM_B: the shard's Â rows were stored by the partial launch and are read-only here (the non-coherent path);
+// otherwise A again, re-applying the update (as k_gemver's pass 2).
+template <typename T, bool FROM_B>
+__global__ void __launch_bounds__(kPassThreads, 2) k_rows_finish(RowsK g, int vec_ok) {
+    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    const int64_t n = g.p.n;
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += gthreads) {
+        const double zz = g.z ? double(__ldcg(g.z + j)) : 0.0;
+        g.x[j] = float(zz + double(g.beta) * __ldcg(g.total + j));
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+        const int64_t unit = g.units - 1 - int64_t(u);
+        if constexpr (FROM_B)
+            pass_unit<float, kWX, true, false, false, false, true, 16, true>(g.p, unit, vec_ok != 0, smem);
+        else
+            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p, unit, vec_ok != 0, smem);
+        u = share_work(next);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish(g.p);
+}
+
 }  // namespace cspb
 
 // =====================================================================================================================
@@ -436,6 +489,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
 
     PassArgs p1{};
     p1.n = n;
+    p1.rows = n;
     p1.src = d->A;
     p1.lds = d->lda;
     p1.dst = d->B;
@@ -565,6 +619,7 @@ int cspb_bicgk_fused(const cspb_bicgk_desc* d, void* stream) {
     g.s = d->s;
     PassArgs& p = g.p;
     p.n = n;
+    p.rows = n;
     p.src = d->B;
     p.lds = d->ldb;
     p.cyB = d->r;
@@ -613,6 +668,7 @@ int cspb_gemver_chain(const cspb_chain_desc* d, void* stream) {
     float* Wp = reinterpret_cast<float*>(ws + L.off_Wp);
     PassArgs base{};
     base.n = n;
+    base.rows = n;
     base.lds = n;
     base.ldd = n;
     base.strips = L.strips;
@@ -663,6 +719,102 @@ int cspb_gemver_chain(const cspb_chain_desc* d, void* stream) {
     const bool disjoint = b1 + mbytes <= b2 || b2 + mbytes <= b1;
     return disjoint ? launch_coop(k_chain_g2<true>, args, L.units, 0, ws, st)
                     : launch_coop(k_chain_g2<false>, args, L.units, 0, ws, st);
+}
+
+// ---- row shards ------------------------------------------------------------------------------------------------
+
+static PassLayout rows_layout(int64_t n, int64_t rows) {
+    PassLayout L = pass_layout(n, kS, kCW32, 1, false);  // chunks and the column-length arrays follow n
+    const int64_t strips = (rows + kS - 1) / kS;
+    L.strips = strips;
+    L.units = strips * L.chunks;
+    return L;
+}
+
+size_t cspb_gemver_rows_workspace_bytes(int64_t n, int64_t rows) {
+    if (n < 1 || rows < 1 || rows > n) return 0;
+    return rows_layout(n, rows).total;
+}
+
+static int rows_args(const cspb_gemver_rows_desc* d, bool finish, RowsK& g, PassLayout& L, int& vec_ok, bool& bf16) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    const int64_t n = d->n, rows = d->rows;
+    if (n < 1 || n > (int64_t(1) << 31) || rows < 1 || rows > n) return CSPB_ERR_ARGUMENT;
+    if (d->a_dtype != CSPB_F32 && d->a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
+    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    if (!d->A || !d->u1 || !d->v1 || !d->u2 || !d->v2 || !d->y) return CSPB_ERR_ARGUMENT;
+    if (finish && (!d->x || !d->w)) return CSPB_ERR_ARGUMENT;
+    if (d->lda < n || (d->B && d->ldb < n)) return CSPB_ERR_ARGUMENT;
+    L = rows_layout(n, rows);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+    bf16 = d->a_dtype == CSPB_BF16;
+    char* ws = static_cast<char*>(d->workspace);
+    PassArgs p{};
+    p.n = n;
+    p.rows = rows;
+    p.strips = L.strips;
+    p.chunks = L.chunks;
+    p.src = d->A;
+    p.lds = d->lda;
+    p.u1 = d->u1; p.v1 = d->v1; p.u2 = d->u2; p.v2 = d->v2;
+    if (!finish) {
+        p.dst = d->B;
+        p.ldd = d->ldb;
+        p.cyB = d->y;
+        p.PB = reinterpret_cast<double*>(ws + L.off_PB);
+    } else {
+        if (!bf16 && d->B) {
+            p.src = d->B;
+            p.lds = d->ldb;
+        }
+        p.xv = d->x;
+        p.Wp = reinterpret_cast<float*>(ws + L.off_Wp);
+        p.strip_done = reinterpret_cast<uint32_t*>(ws + L.off_done);
+        p.rout1 = d->w;
+        p.rscale1 = d->alpha;
+    }
+    g = RowsK{};
+    g.p = p;
+    g.ctrl = reinterpret_cast<uint32_t*>(ws);
+    g.units = L.units;
+    g.z = d->z;
+    g.beta = d->beta;
+    g.x = d->x;
+    const int eb = bf16 ? 2 : 4;
+    vec_ok = vec_aligned(d->A, d->lda, eb) && vec_aligned(d->B, d->ldb, 4) ? 1 : 0;
+    return CSPB_OK;
+}
+
+int cspb_gemver_rows_partial(const cspb_gemver_rows_desc* d, double* colsum, void* stream) {
+    RowsK g;
+    PassLayout L;
+    int vec_ok = 0;
+    bool bf16 = false;
+    const int rc = rows_args(d, false, g, L, vec_ok, bf16);
+    if (rc != CSPB_OK) return rc;
+    if (!colsum) return CSPB_ERR_ARGUMENT;
+    g.colsum = colsum;
+    void* args[] = {&g, &vec_ok};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (bf16) return launch_coop(k_rows_partial<__nv_bfloat16>, args, L.units, L.off_PA, d->workspace, st);
+    return launch_coop(k_rows_partial<float>, args, L.units, L.off_PA, d->workspace, st);
+}
+
+int cspb_gemver_rows_finish(const cspb_gemver_rows_desc* d, const double* colsum_total, void* stream) {
+    RowsK g;
+    PassLayout L;
+    int vec_ok = 0;
+    bool bf16 = false;
+    const int rc = rows_args(d, true, g, L, vec_ok, bf16);
+    if (rc != CSPB_OK) return rc;
+    if (!colsum_total) return CSPB_ERR_ARGUMENT;
+    g.total = colsum_total;
+    void* args[] = {&g, &vec_ok};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t units = L.units > L.chunks ? L.units : L.chunks;  // the x phase wants blocks too
+    if (bf16) return launch_coop(k_rows_finish<__nv_bfloat16, false>, args, units, L.off_PA, d->workspace, st);
+    if (d->B) return launch_coop(k_rows_finish<float, true>, args, units, L.off_PA, d->workspace, st);
+    return launch_coop(k_rows_finish<float, false>, args, units, L.off_PA, d->workspace, st);
 }
 
 }  // extern "C"

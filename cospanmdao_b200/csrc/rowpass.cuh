@@ -35,7 +35,8 @@ struct PassGeo {
 };
 
 struct PassArgs {
-    int64_t n;
+    int64_t n;         // columns (and the stride of PA / PB / Wp)
+    int64_t rows;      // rows: n, except for a row shard of a larger GEMVER (sharded.cu)
     const void* src;   // the matrix read (T, or f32 when the pass reads B)
     int64_t lds;
     float* dst;        // STORE target (f32); NULL: no store
@@ -197,7 +198,7 @@ __device__ __forceinline__ void unit_epilogue(const PassArgs& a, int64_t strip, 
         sync();
         for (int t = threadIdx.x; t < S; t += kPassThreads) {
             const int64_t row = strip * S + t;
-            if (row < n) {
+            if (row < a.rows) {
                 float s = red2[t];
 #pragma unroll
                 for (int x = 1; x < WX; ++x) s += red2[x * S + t];
@@ -217,7 +218,7 @@ __device__ __forceinline__ void unit_epilogue(const PassArgs& a, int64_t strip, 
         if (s_last) {
             for (int t = threadIdx.x; t < S; t += kPassThreads) {
                 const int64_t row = strip * S + t;
-                if (row < n) {
+                if (row < a.rows) {
                     // chunks in order; 16 loads in flight at a time (the partials sit in L2)
                     float s = 0.f;
                     int64_t c = 0;
@@ -250,7 +251,7 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
     const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
     const int64_t r0 = strip * S + wy * 32;
     const int64_t c0 = chunk * CW + int64_t(wx * 32 + lane) * VEC;
-    const int64_t rem_r = n - r0, rem_c = n - c0;
+    const int64_t rem_r = a.rows - r0, rem_c = n - c0;
     const int nrows = rem_r <= 0 ? 0 : (rem_r >= 32 ? 32 : int(rem_r));
     const int ncols = rem_c <= 0 ? 0 : (rem_c >= VEC ? VEC : int(rem_c));
 
@@ -365,7 +366,7 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
 // block, so a deferred pass gives the same bits), and rout2 likewise; by every thread of the grid, no barrier inside.
 __device__ __forceinline__ void rowsum_finish(const PassArgs& a) {
     const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t row = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < a.n; row += gthreads) {
+    for (int64_t row = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < a.rows; row += gthreads) {
         float s = 0.f;
         int64_t c = 0;
         for (; c + 16 <= a.chunks; c += 16) {
@@ -515,6 +516,24 @@ __device__ __forceinline__ void rowsum_finish_lr(const PassArgs& a, const float*
         d = __fma_rn(double(__ldcg(u1 + row)), t1, d);
         d = __fma_rn(double(__ldcg(u2 + row)), t2, d);
         a.rout1[row] = float(double(a.rscale1) * d);
+    }
+}
+
+// out[j] = Σ_strips P[st][j] in f64 over every column, in colsum_finish's order (four strided sums, then pairs), not
+// rounded: a row shard's share of the column sums, added across shards by the caller (sharded GEMVER).
+__device__ __forceinline__ void colsum_f64(const double* P, int64_t strips, int64_t n, double* out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gthreads = int64_t(gridDim.x) * blockDim.x;
+    const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int64_t base = gtid - lane; base < 4 * n; base += gthreads) {
+        const int64_t item = base + lane;
+        const bool valid = item < 4 * n;
+        const int64_t j = item >> 2;
+        const int q = int(item & 3);
+        double s = valid ? strided_strip_sum(P, strips, n, j, q) : 0.0;
+        s += __shfl_xor_sync(kFull, s, 1);
+        s += __shfl_xor_sync(kFull, s, 2);
+        if (valid && q == 0) out[j] = s;
     }
 }
 

@@ -77,6 +77,15 @@ class Ranks:
         self.pg.all_gather(out, t)
         return [int(o.item()) for o in out]
 
+    def all_gather_tensor(self, t):
+        """Every rank's copy of the tensor `t` (same shape and dtype on every rank), in rank order."""
+        if not self.pg:
+            return [t]
+        import torch
+        out = [torch.empty_like(t) for _ in range(self.world)]
+        self.pg.all_gather(out, t.contiguous())
+        return out
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()

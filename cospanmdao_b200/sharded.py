@@ -1,0 +1,97 @@
+"""One large GEMVER split by rows across the GPUs of a node (one process per GPU): the path's one exchange step.
+
+Rank r holds rows [r0, r1) of A (and of B, u1, u2, y, w) and all of v1, v2, z (shard_rows gives the split). Every row
+is independent except for the column sums Âᵀy, which need every row. So a forward is:
+
+  1. cspb_gemver_rows_partial: the rank's Â rows and its share of the column sums, n values in f64;
+  2. the exchange: an all-gather of the shares (n · 8 bytes per rank; NCCL over NVLink on GPUs, gloo on the CPU) and
+     their sum in rank order, so that every rank holds the same total and forms the same x;
+  3. cspb_gemver_rows_finish: x over all n columns, then w over the rank's rows.
+
+The all-gather plus a fixed-order sum (instead of an all-reduce) keeps x independent of the collective's reduction
+order. Scaling is strong (the GEMVER's size is fixed); the exchange is n · 8 · world bytes against a shard's 12 · n²
+/ world bytes of matrix traffic.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _capi
+from ._capi import BF16, F32, lib
+
+
+def shard_rows(n: int, world: int, align: int = 128) -> list[tuple[int, int]]:
+    """Contiguous row ranges [r0, r1) for `world` ranks, near-equal and (but the last) multiples of `align` rows, so
+    that shards cut at the kernels' 128-row strips. A rank may get an empty range when n is small."""
+    if n < 0 or world < 1 or align < 1:
+        raise ValueError("shard_rows needs n >= 0, world >= 1 and align >= 1")
+    blocks = (n + align - 1) // align
+    cuts = [min(n, (blocks * r // world) * align) for r in range(world)] + [n]
+    return [(cuts[r], cuts[r + 1]) for r in range(world)]
+
+
+def combine_column_sums(share, ranks):
+    """The sum of every rank's share of the column sums, added in rank order (the same bits on every rank)."""
+    parts = ranks.all_gather_tensor(share) if ranks is not None else [share]
+    total = parts[0].clone()
+    for p in parts[1:]:
+        total += p
+    return total
+
+
+def _desc(A, u1, v1, u2, v2, y, z, alpha, beta, B, x, w, wp, wb):
+    import torch
+    n = A.shape[1]
+    return _capi.GemverRowsDesc(n, A.shape[0], A.stride(0), B.stride(0) if B is not None else n,
+                                BF16 if A.dtype == torch.bfloat16 else F32, 0, _ptr(A), _ptr(u1), _ptr(v1), _ptr(u2),
+                                _ptr(v2), _ptr(y), _ptr(z), float(alpha), float(beta), _ptr(B), _ptr(x), _ptr(w), wp,
+                                wb)
+
+
+def _ptr(t):
+    return None if t is None else int(t.data_ptr())
+
+
+def gemver_rows_partial(A, u1, v1, u2, v2, y, *, B=None, colsum=None, workspace=None, stream=None):
+    """The rank's Â rows (into B when given) and its share of the column sums (f64, n). A: (rows, n) f32 or bf16
+    with contiguous rows; u1, u2, y: rows; v1, v2: n."""
+    import torch
+    import cospanmdao_b200 as cb
+    rows, n = A.shape
+    colsum = torch.empty(n, dtype=torch.float64, device=A.device) if colsum is None else colsum
+    ws = workspace or cb.default_workspace(A.device, stream)
+    wp, wb = ws.ptr(int(lib().cspb_gemver_rows_workspace_bytes(n, rows)))
+    d = _desc(A, u1, v1, u2, v2, y, None, 0.0, 0.0, B, None, None, wp, wb)
+    cb._raise(lib().cspb_gemver_rows_partial(C.byref(d), C.c_void_p(_ptr(colsum)), C.c_void_p(cb._stream(stream))),
+              "gemver rows partial")
+    return colsum
+
+
+def gemver_rows_finish(A, u1, v1, u2, v2, y, z, total, *, alpha, beta, B=None, x=None, w=None, workspace=None,
+                       stream=None):
+    """x over all n columns from the summed column sums, then w over the rank's rows. Returns (x, w)."""
+    import torch
+    import cospanmdao_b200 as cb
+    rows, n = A.shape
+    x = torch.empty(n, dtype=torch.float32, device=A.device) if x is None else x
+    w = torch.empty(rows, dtype=torch.float32, device=A.device) if w is None else w
+    ws = workspace or cb.default_workspace(A.device, stream)
+    wp, wb = ws.ptr(int(lib().cspb_gemver_rows_workspace_bytes(n, rows)))
+    d = _desc(A, u1, v1, u2, v2, y, z, alpha, beta, B, x, w, wp, wb)
+    cb._raise(lib().cspb_gemver_rows_finish(C.byref(d), C.c_void_p(_ptr(total)), C.c_void_p(cb._stream(stream))),
+              "gemver rows finish")
+    return x, w
+
+
+def gemver_sharded(A, u1, v1, u2, v2, y, z=None, *, alpha, beta, ranks=None, want_B=True, workspace=None,
+                   stream=None):
+    """This rank's part of one row-sharded GEMVER: (B rows or None, x (all n), w rows). `ranks` is a
+    replicas.Ranks joined to the job's process group (None: a single rank)."""
+    import torch
+    rows, n = A.shape
+    B = torch.empty((rows, n), dtype=torch.float32, device=A.device) if want_B else None
+    share = gemver_rows_partial(A, u1, v1, u2, v2, y, B=B, workspace=workspace, stream=stream)
+    total = combine_column_sums(share, ranks)
+    x, w = gemver_rows_finish(A, u1, v1, u2, v2, y, z, total, alpha=alpha, beta=beta, B=B, workspace=workspace,
+                              stream=stream)
+    return B, x, w

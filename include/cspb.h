@@ -116,6 +116,43 @@ typedef struct cspb_gemver_desc {
 size_t cspb_gemver_workspace_bytes(int64_t n);
 int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream);
 
+/* ONE GEMVER split by rows across GPUs (one process per GPU). The reference runs a GEMVER on one device only; this
+ * splits its stages (examples/gemver-chain/components.hpp:85-97 Rank2Update, :142-167 GemvTPartial, :176-220
+ * ColReduce, :227-266 Gemv) at the one place that needs every row: ColReduce's sum over row strips. A shard holds
+ * rows [r0, r0 + rows) of A, B, u1, u2, y and w, and all n entries of v1, v2, z and x:
+ *   cspb_gemver_rows_partial  Â rows (stored when B is not NULL) and colsum[j] = Σ_{i in shard} Â[i][j]·y[i] (f64, n)
+ *   (the caller exchanges colsum and adds the shards' values in rank order: the same total on every rank)
+ *   cspb_gemver_rows_finish   x = float(z + β·total) over all n columns, then w = α·Â·x over the shard's rows
+ * A, B, u1, u2, y and w point at the shard's first row. flags must be 0. Each call is one cooperative launch on the
+ * caller's stream; the workspace (cspb_gemver_rows_workspace_bytes) may be shared by the two calls of a shard. With
+ * one shard (rows = n) the results equal cspb_gemver_fused's within rounding of the column sums' grouping. */
+typedef struct cspb_gemver_rows_desc {
+    int64_t n;         /* columns: the whole GEMVER's size, >= 1 */
+    int64_t rows;      /* this shard's rows, 1 <= rows <= n */
+    int64_t lda;       /* row stride of A in elements, >= n */
+    int64_t ldb;       /* row stride of B in elements, >= n (ignored when B is NULL) */
+    int32_t a_dtype;   /* CSPB_F32 or CSPB_BF16 */
+    int32_t flags;     /* 0 */
+    const void* A;     /* rows × n */
+    const float* u1;   /* rows */
+    const float* v1;   /* n */
+    const float* u2;   /* rows */
+    const float* v2;   /* n */
+    const float* y;    /* rows */
+    const float* z;    /* n, may be NULL */
+    float alpha;
+    float beta;
+    float* B;          /* rows × n, may be NULL */
+    float* x;          /* n: written by the finish */
+    float* w;          /* rows: written by the finish */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_gemver_rows_desc;
+
+size_t cspb_gemver_rows_workspace_bytes(int64_t n, int64_t rows);
+int cspb_gemver_rows_partial(const cspb_gemver_rows_desc* d, double* colsum, void* stream);
+int cspb_gemver_rows_finish(const cspb_gemver_rows_desc* d, const double* colsum_total, void* stream);
+
 /* ==================================================================================================================
  * BiCGK:  q = B·p ;  s = Bᵀ·r   (one pass over B)
  *

@@ -1,0 +1,79 @@
+"""The host side of the row-sharded GEMVER (cospanmdao_b200.sharded) on the CPU: the row split, and the exchange of
+the column-sum shares between two gloo ranks. Each rank's share is computed here in numpy f64 from the oracle's
+formula (standing in for cspb_gemver_rows_partial); the exchange must give both ranks the same total, bit for bit
+the rank-order sum, and the x formed from it must match the f64 oracle's."""
+import json
+import os
+import socket
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _problem(n):
+    rng = np.random.default_rng(5)
+    A = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+    vec = {k: rng.uniform(0, 1, n).astype(np.float32) for k in ("u1", "v1", "u2", "v2", "y", "z")}
+    return A, vec
+
+
+def _share(A, vec, r0, r1):
+    # Σ_{i in [r0, r1)} Â[i][j]·y[i] in f64, Â in f32 as the kernels form it
+    Ah = (A[r0:r1] + np.outer(vec["u1"][r0:r1], vec["v1"]).astype(np.float32)) + \
+        np.outer(vec["u2"][r0:r1], vec["v2"]).astype(np.float32)
+    return (Ah.astype(np.float64) * vec["y"][r0:r1, None].astype(np.float64)).sum(axis=0)
+
+
+def _rank(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import torch
+    from cospanmdao_b200.replicas import Ranks
+    from cospanmdao_b200.sharded import combine_column_sums, shard_rows
+    r = Ranks().init("gloo", timeout_s=60)
+    n = 600
+    A, vec = _problem(n)
+    r0, r1 = shard_rows(n, world)[rank]
+    share = torch.from_numpy(_share(A, vec, r0, r1))
+    total = combine_column_sums(share, r)
+    np.save(Path(out_dir) / f"total{rank}.npy", total.numpy())
+    Path(out_dir, f"r{rank}.json").write_text(json.dumps({"r0": r0, "r1": r1}))
+    r.barrier()
+    r.close()
+
+
+def test_two_ranks_exchange_the_column_sums(tmp_path):
+    import torch.multiprocessing as mp
+    import oracle
+    world, n = 2, 600
+    mp.start_processes(_rank, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True, start_method="spawn")
+    totals = [np.load(tmp_path / f"total{r}.npy") for r in range(world)]
+    assert np.array_equal(totals[0], totals[1])
+    A, vec = _problem(n)
+    spans = [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
+    assert spans[0]["r0"] == 0 and spans[0]["r1"] == spans[1]["r0"] and spans[1]["r1"] == n
+    want = _share(A, vec, spans[0]["r0"], spans[0]["r1"]) + _share(A, vec, spans[1]["r0"], spans[1]["r1"])
+    assert np.array_equal(totals[0], want)  # the rank-order sum, bit for bit
+    x = (vec["z"].astype(np.float64) + 1.2 * totals[0]).astype(np.float32)
+    xo, _, _ = oracle.gemver_f64(n, A, vec["u1"], vec["v1"], vec["u2"], vec["v2"], vec["y"], vec["z"], 1.0, 1.2)
+    assert oracle.rel_l2(x, xo) < 1e-5
+
+
+def test_shard_rows():
+    from cospanmdao_b200.sharded import shard_rows
+    for n in (0, 1, 127, 128, 129, 1000, 16384):
+        for world in (1, 2, 3, 8):
+            s = shard_rows(n, world)
+            assert len(s) == world and s[0][0] == 0 and s[-1][1] == n
+            assert all(a <= b for a, b in s) and all(s[i][1] == s[i + 1][0] for i in range(world - 1))
+            assert all(a % 128 == 0 for a, _ in s)
+    assert shard_rows(16384, 8) == [(2048 * r, 2048 * (r + 1)) for r in range(8)]
+    with pytest.raises(ValueError):
+        shard_rows(10, 0)

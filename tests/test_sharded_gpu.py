@@ -1,0 +1,86 @@
+"""One GEMVER split by rows (cospanmdao_b200.sharded, cspb_gemver_rows_partial / _finish), on one GPU.
+
+The ranks run one after another on the same GPU: each partial is a complete launch, the exchange is the rank-order sum
+of the shares on the host side, and no kernel waits on another rank. Â rows must equal the fused GEMVER's bit for
+bit (the same per-element formula), x must be the same on every rank, and x and w must match the fused GEMVER and the
+f64 oracle within the f32 tolerance (the column sums are grouped by shard)."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _np(t):
+    return t.detach().float().cpu().numpy()
+
+
+@pytest.mark.parametrize("n,world,dtype_name,want_B", [(1000, 1, "float32", True), (1000, 2, "float32", True),
+                                                       (3000, 3, "float32", False), (2048, 4, "bfloat16", True),
+                                                       (777, 2, "bfloat16", False), (300, 3, "float32", True)])
+def test_row_shards_match_the_fused_gemver(cuda, n, world, dtype_name, want_B):
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200 import workloads
+    from cospanmdao_b200.sharded import gemver_rows_finish, gemver_rows_partial, shard_rows
+    dt = getattr(torch, dtype_name)
+    d = workloads.gemver_inputs(n, 13, dtype=dt, device=cuda)
+    alpha, beta = 1.5, -0.7
+    Bf, xf, wf = cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=alpha, beta=beta,
+                           want_B=want_B, schedule="barrier")
+    shards = shard_rows(n, world)
+    assert shards[0][0] == 0 and shards[-1][1] == n
+    Bs, shares = [], []
+    for r0, r1 in shards:
+        B = torch.empty((r1 - r0, n), dtype=torch.float32, device=cuda) if want_B else None
+        shares.append(gemver_rows_partial(d["A"][r0:r1], d["u1"][r0:r1], d["v1"], d["u2"][r0:r1], d["v2"],
+                                          d["y"][r0:r1], B=B, workspace=cb.Workspace(cuda)))
+        Bs.append(B)
+    total = shares[0].clone()
+    for s in shares[1:]:
+        total += s
+    xs, ws = [], []
+    for (r0, r1), B in zip(shards, Bs):
+        x, w = gemver_rows_finish(d["A"][r0:r1], d["u1"][r0:r1], d["v1"], d["u2"][r0:r1], d["v2"], d["y"][r0:r1],
+                                  d["z"], total, alpha=alpha, beta=beta, B=B, workspace=cb.Workspace(cuda))
+        xs.append(x)
+        ws.append(w)
+    torch.cuda.synchronize()
+    for x in xs[1:]:
+        assert torch.equal(x, xs[0])  # every rank forms the same x from the same total
+    w = torch.cat(ws)
+    if want_B:
+        assert torch.equal(torch.cat(Bs), Bf)
+    assert oracle.rel_l2(_np(xs[0]), _np(xf)) < TOL and oracle.rel_l2(_np(w), _np(wf)) < TOL
+    h = {k: _np(v) for k, v in d.items()}
+    xo, wo, _ = oracle.gemver_f64(n, h["A"], h["u1"], h["v1"], h["u2"], h["v2"], h["y"], h["z"], alpha, beta)
+    assert oracle.rel_l2(_np(xs[0]), xo) < TOL and oracle.rel_l2(_np(w), wo) < TOL
+
+
+def test_one_shard_equals_the_rank_loop_helper(cuda):
+    """gemver_sharded with no process group is the one-shard case."""
+    import torch
+    from cospanmdao_b200 import workloads
+    from cospanmdao_b200.sharded import gemver_sharded
+    n = 512
+    d = workloads.gemver_inputs(n, 2, device=cuda)
+    B, x, w = gemver_sharded(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.0, beta=2.0)
+    B2, x2, w2 = gemver_sharded(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.0, beta=2.0)
+    torch.cuda.synchronize()
+    assert torch.equal(B, B2) and torch.equal(x, x2) and torch.equal(w, w2)
+    h = {k: _np(v) for k, v in d.items()}
+    xo, wo, _ = oracle.gemver_f64(n, h["A"], h["u1"], h["v1"], h["u2"], h["v2"], h["y"], h["z"], 1.0, 2.0)
+    assert oracle.rel_l2(_np(x), xo) < TOL and oracle.rel_l2(_np(w), wo) < TOL
+
+
+def test_row_shard_argument_errors(cuda):
+    import ctypes as C
+    from cospanmdao_b200 import _capi
+    lib = _capi.lib()
+    d = _capi.GemverRowsDesc()
+    d.n, d.rows = 100, 101  # more rows than columns
+    assert lib.cspb_gemver_rows_partial(C.byref(d), None, None) == _capi.ERR_ARGUMENT
+    assert lib.cspb_gemver_rows_workspace_bytes(100, 101) == 0
