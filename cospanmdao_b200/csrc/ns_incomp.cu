@@ -10,7 +10,9 @@
 // No reference code computes this residual (the reference's ns-residual is the compressible one, ns_comp.cu); the
 // formula is the workload's definition, and the oracle is an f64 restatement of it.
 //
-// Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. Work item = one warp on a strip of 32·VEC columns × H rows:
+// Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. f32 fields that are 16-byte aligned with nx % 4 == 0 take
+// the block-tile path (nsi_tile below). Otherwise (bf16 storage, or unaligned / ragged rows) the register path:
+// work item = one warp on a strip of 32·VEC columns × H rows:
 // each lane owns 4 consecutive cells of a row (one 16-byte f32 / 8-byte bf16 load per field per row), x-neighbours come from the
 // adjacent lanes by shuffle (the warp's edge lanes load one wrapped scalar), and the warp marches down its rows
 // keeping the rows above and below in registers, two rows of loads in flight. Each input is read from HBM once (the
@@ -85,17 +87,22 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
     right = need_r ? row.r : from_right;
 }
 
-// ---- f32 rows through a shared-memory ring (cp.async) -------------------------------------------------------------
-// A warp streams the rows of u, v, p through its own ring of kNsiRing shared-memory slots instead of registers: each
-// lane copies its 16-byte cells of a row (cp.async, no register held while the copy is in flight), lane 0 and the
-// last active lane copy the two wrapped halo cells of the strip, and the warp computes row j from the slots of rows
-// j-1, j, j+1 while rows j+2 .. j+kNsiRing-2 are still arriving. A slot is one row of one field: [3] the cell left of
-// the strip, [4 .. 4+128) the strip's cells, [4 + cells] the cell right of it. Measured on B200 at 4096², a ring of 4
-// slots (26 KB per warp row set, 4 blocks of 8 warps per SM) runs a little faster than rings of 5 or 8 slots with
-// fewer blocks: the warps, not the depth of each warp's ring, keep the memory system busy.
-constexpr int kNsiRing = 4;
-constexpr int kNsiSlot = 136;  // floats
-constexpr size_t kNsiRingBytes = size_t(kNsiWarps) * kNsiRing * 3 * kNsiSlot * sizeof(float);
+// ---- f32 by block tiles (cp.async) -------------------------------------------------------------------------------
+// A block computes one tile of kNsiTileCols × kNsiTileRows cells. It first copies the tile's rows of u, v, p with the
+// rows above and below it and the two wrapped halo columns into shared memory (cp.async: each warp takes every 8th
+// row, each lane its 16-byte cells, lane 0 and the last active lane the halo cells), waits once, then computes its
+// rows from shared memory and stores the residuals. Four such blocks per SM keep whole tiles (3 × 34 rows × 512 B
+// each) in flight while other blocks compute. Measured on B200 at 4096²: 82 µs against 136 µs for a per-warp ring of
+// 4 row slots (one row in flight per warp), with bit-identical residuals; taller tiles (48, 64 rows: 2-3 blocks per
+// SM) ran 91-94 µs. A tile row is [3] the cell left of the tile, [4 .. 4+128) its cells, [4 + cols] the cell right.
+constexpr int kNsiTileCols = 128;
+constexpr int kNsiTileRows = 32;
+constexpr int kNsiPitch = 136;  // floats per tile row
+constexpr size_t kNsiTileBytes = size_t(3) * (kNsiTileRows + 2) * kNsiPitch * sizeof(float);
+
+__host__ __device__ inline int64_t nsi_tiles(int nx, int ny) {
+    return int64_t((nx + kNsiTileCols - 1) / kNsiTileCols) * ((ny + kNsiTileRows - 1) / kNsiTileRows);
+}
 
 __device__ __forceinline__ uint32_t nsi_smem(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
 __device__ __forceinline__ void nsi_cp16(void* dst, const void* src) {
@@ -104,75 +111,58 @@ __device__ __forceinline__ void nsi_cp16(void* dst, const void* src) {
 __device__ __forceinline__ void nsi_cp4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(nsi_smem(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void nsi_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void nsi_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// One warp item (a strip of 128 columns × H rows) of an f32 residual with nx % 4 == 0 and 16-byte aligned fields.
-// The residuals are the register path's, operation for operation; the squares of a lane's 4 cells are summed in f32
-// before each f64 addition (a quarter of the conversions).
-__device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float* ring, double& su, double& sv,
-                                              double& sc) {
-    const int lane = threadIdx.x & 31;
-    const int seg = int(item % g.segs);
-    const int strip = int(item / g.segs);
-    const int sc0 = seg * 128;                               // first column of the strip
-    const int scols = g.nx - sc0 >= 128 ? 128 : g.nx - sc0;  // a multiple of 4
-    const int c0 = sc0 + lane * 4;
+// Tile b of an f32 residual with nx % 4 == 0 and 16-byte aligned fields. The residuals are the register path's,
+// operation for operation; each lane's 4 squares are summed in f32 before one f64 addition per norm.
+__device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, float* buf, double& su, double& sv, double& sc) {
+    constexpr int kField = (kNsiTileRows + 2) * kNsiPitch;  // floats between the fields
+    const int tilesx = (g.nx + kNsiTileCols - 1) / kNsiTileCols;
+    const int x0 = int(b % tilesx) * kNsiTileCols, y0 = int(b / tilesx) * kNsiTileRows;
+    const int scols = g.nx - x0 >= kNsiTileCols ? kNsiTileCols : g.nx - x0;  // a multiple of 4
+    const int th = g.ny - y0 >= kNsiTileRows ? kNsiTileRows : g.ny - y0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool active = lane * 4 < scols;
     const bool last = active && (lane + 1) * 4 >= scols;
-    const int j0 = strip * g.H;
-    const int j1 = min(g.ny, j0 + g.H);
+    const int c0 = x0 + lane * 4;
+    const int lcol = x0 == 0 ? g.nx - 1 : x0 - 1;
+    const int rcol = (x0 + scols) % g.nx;
     const int64_t nx = g.nx;
     const float* U = static_cast<const float*>(g.u);
     const float* V = static_cast<const float*>(g.v);
     const float* P = static_cast<const float*>(g.p);
-    const int lcol = sc0 == 0 ? g.nx - 1 : sc0 - 1;
-    const int rcol = (sc0 + scols) % g.nx;
-    constexpr int kField = kNsiSlot, kRow = 3 * kNsiSlot;  // floats between the fields of a slot, between slots
-    float* const mine = ring + 4 + lane * 4;                 // this lane's cells in slot 0, field 0
-    // rows j0-1 .. j1 are read; one commit group per row (empty past j1); row r goes to slot (r - j0 + 1) % kNsiRing
-    int s_next = 0, r_next = j0 - 1;
-    auto issue = [&]() {
-        if (r_next <= j1) {
-            const int rr = r_next < 0 ? r_next + g.ny : (r_next >= g.ny ? r_next - g.ny : r_next);
-            const int64_t ro = int64_t(rr) * nx;
-            float* sl = ring + s_next * kRow;
-            if (active) {
-                nsi_cp16(sl + 4 + lane * 4, U + ro + c0);
-                nsi_cp16(sl + kField + 4 + lane * 4, V + ro + c0);
-                nsi_cp16(sl + 2 * kField + 4 + lane * 4, P + ro + c0);
-            }
-            if (lane == 0) {
-                nsi_cp4(sl + 3, U + ro + lcol);
-                nsi_cp4(sl + kField + 3, V + ro + lcol);
-                nsi_cp4(sl + 2 * kField + 3, P + ro + lcol);
-            }
-            if (last) {
-                nsi_cp4(sl + 4 + scols, U + ro + rcol);
-                nsi_cp4(sl + kField + 4 + scols, V + ro + rcol);
-                nsi_cp4(sl + 2 * kField + 4 + scols, P + ro + rcol);
-            }
-        }
-        nsi_commit();
-        ++r_next;
-        s_next = s_next + 1 == kNsiRing ? 0 : s_next + 1;
-    };
-#pragma unroll 1
-    for (int q = 0; q < kNsiRing - 1; ++q) issue();
-    const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
-    int sS = 0, sC = 1, sN = 2;  // the slots of rows j-1, j, j+1
-#pragma unroll 1
-    for (int j = j0; j < j1; ++j) {
-        issue();  // row j+kNsiRing-2, into the slot row j-2 left (free since the last iteration's __syncwarp)
-        // issued: rows j0-1 .. j+kNsiRing-2, one group each; rows up to j+1 must have landed (for this lane)
-        nsi_wait<kNsiRing - 3>();
-        __syncwarp();  // and every lane's copies are visible to the warp
+    // tile row r holds grid row y0 - 1 + r (wrapped), r = 0 .. th + 1
+    for (int r = warp; r < th + 2; r += kNsiWarps) {
+        int gy = y0 - 1 + r;
+        gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
+        const int64_t ro = int64_t(gy) * nx;
+        float* row = buf + r * kNsiPitch;
         if (active) {
-            const float* a = mine + sC * kRow;
-            const float* mS = mine + sS * kRow;
-            const float* mN = mine + sN * kRow;
-            float cu[6], cv[6], cp[6];  // W, 4 cells, E of row j
+            nsi_cp16(row + 4 + lane * 4, U + ro + c0);
+            nsi_cp16(row + kField + 4 + lane * 4, V + ro + c0);
+            nsi_cp16(row + 2 * kField + 4 + lane * 4, P + ro + c0);
+        }
+        if (lane == 0) {
+            nsi_cp4(row + 3, U + ro + lcol);
+            nsi_cp4(row + kField + 3, V + ro + lcol);
+            nsi_cp4(row + 2 * kField + 3, P + ro + lcol);
+        }
+        if (last) {
+            nsi_cp4(row + 4 + scols, U + ro + rcol);
+            nsi_cp4(row + kField + 4 + scols, V + ro + rcol);
+            nsi_cp4(row + 2 * kField + 4 + scols, P + ro + rcol);
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    if (active) {
+        const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
+        const float* const mine = buf + 4 + lane * 4;
+        for (int j = warp; j < th; j += kNsiWarps) {
+            const float* a = mine + (j + 1) * kNsiPitch;
+            const float* mS = mine + j * kNsiPitch;
+            const float* mN = mine + (j + 2) * kNsiPitch;
+            float cu[6], cv[6], cp[6];  // W, 4 cells, E of the row
             float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
             {
                 const float4 ua = *reinterpret_cast<const float4*>(a);
@@ -196,7 +186,7 @@ __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float
                 pN[0] = pn.x; pN[1] = pn.y; pN[2] = pn.z; pN[3] = pn.w;
             }
             float oru[4], orv[4], orc[4];
-            float qu = 0.f, qv = 0.f, qc = 0.f;  // the lane's 4 squares in f32, then one f64 addition per norm
+            float qu = 0.f, qv = 0.f, qc = 0.f;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const float uc = cu[e + 1], vc = cv[e + 1];
@@ -219,31 +209,79 @@ __device__ __forceinline__ void nsi_rows_ring(const NsiK& g, int64_t item, float
             su += double(qu);
             sv += double(qv);
             sc += double(qc);
-            const int64_t ro = int64_t(j) * nx + c0;
+            const int64_t ro = int64_t(y0 + j) * nx + c0;
             st_f4(g.ru + ro, make_float4(oru[0], oru[1], oru[2], oru[3]));
             st_f4(g.rv + ro, make_float4(orv[0], orv[1], orv[2], orv[3]));
             st_f4(g.rc + ro, make_float4(orc[0], orc[1], orc[2], orc[3]));
         }
-        __syncwarp();  // every lane is done with row j-1's slot before the next iteration refills it
-        sS = sC;
-        sC = sN;
-        sN = sN + 1 == kNsiRing ? 0 : sN + 1;
     }
-    nsi_wait<0>();
-    __syncwarp();
+}
+
+// The norms of block b: a warp xor tree, the block in warp order into part[b]; the last block to finish (counter
+// `done`) sums the partials with all its threads in a fixed assignment and order (strided per thread, an xor tree per
+// warp, the warps in order). Bit-identical on every run.
+__device__ __forceinline__ void nsi_norms(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done, double su,
+                                          double sv, double sc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        su += __shfl_xor_sync(0xffffffffu, su, off);
+        sv += __shfl_xor_sync(0xffffffffu, sv, off);
+        sc += __shfl_xor_sync(0xffffffffu, sc, off);
+    }
+    __shared__ double s_red[kNsiWarps][3];
+    __shared__ int s_last;
+    if (lane == 0) { s_red[warp][0] = su; s_red[warp][1] = sv; s_red[warp][2] = sc; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double s = s_red[0][threadIdx.x];
+        for (int w = 1; w < kNsiWarps; ++w) s += s_red[w][threadIdx.x];
+        g.part[b * 3 + threadIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(done, 1u) == uint32_t(nblocks - 1);
+    __syncthreads();
+    if (s_last) {  // block-uniform: the whole block sums the partials, thread t the blocks t, t + 256, ... in order
+        __threadfence();
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int64_t q = threadIdx.x; q < nblocks; q += blockDim.x) {
+            a0 += __ldcg(g.part + q * 3 + 0);
+            a1 += __ldcg(g.part + q * 3 + 1);
+            a2 += __ldcg(g.part + q * 3 + 2);
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+        }
+        if (lane == 0) { s_red[warp][0] = a0; s_red[warp][1] = a1; s_red[warp][2] = a2; }
+        __syncthreads();
+        if (threadIdx.x < 3 && g.norms) {
+            double t = s_red[0][threadIdx.x];
+            for (int w = 1; w < kNsiWarps; ++w) t += s_red[w][threadIdx.x];
+            g.norms[threadIdx.x] = sqrt(t);
+        }
+    }
+    __syncthreads();  // the shared memory of this block is reused by the next block of a persistent caller
+}
+
+// Tile b (of nblocks) of an f32 residual, with its norms.
+__device__ __forceinline__ void nsi_tile_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done, float* buf) {
+    double su = 0.0, sv = 0.0, sc = 0.0;
+    nsi_tile(g, b, buf, su, sv, sc);
+    nsi_norms(g, b, nblocks, done, su, sv, sc);
 }
 
 // Block b (of nblocks) of one residual: its 8 warps take items 8b .. 8b+7. Its norm partial goes to part[b]; the last
 // block to finish (counter `done`) sums the partials in block order.
 template <typename T, int VEC>
-__device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done,
-                                          float* ring = nullptr) {
+__device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t item = b * kNsiWarps + warp;
     double su = 0.0, sv = 0.0, sc = 0.0;
-    if constexpr (sizeof(T) == 4 && VEC == 4) {
-        if (item < g.items) nsi_rows_ring(g, item, ring + size_t(warp) * kNsiRing * 3 * kNsiSlot, su, sv, sc);
-    } else if (item < g.items) {  // warp-uniform
+    if (item < g.items) {  // warp-uniform
         const int seg = int(item % g.segs);
         const int strip = int(item / g.segs);
         const int c0 = seg * 32 * VEC + lane * VEC;
@@ -328,43 +366,17 @@ __device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblo
             p0 = p1; p1 = p2; p2 = p3;
         }
     }
-    // ---- the norms: warp xor tree, block in warp order, grid in block order by the last block ----
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
-        su += __shfl_xor_sync(0xffffffffu, su, off);
-        sv += __shfl_xor_sync(0xffffffffu, sv, off);
-        sc += __shfl_xor_sync(0xffffffffu, sc, off);
-    }
-    __shared__ double s_red[kNsiWarps][3];
-    __shared__ int s_last;
-    if (lane == 0) { s_red[warp][0] = su; s_red[warp][1] = sv; s_red[warp][2] = sc; }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        double s = s_red[0][threadIdx.x];
-        for (int w = 1; w < kNsiWarps; ++w) s += s_red[w][threadIdx.x];
-        g.part[b * 3 + threadIdx.x] = s;
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(done, 1u) == uint32_t(nblocks - 1);
-    __syncthreads();
-    if (s_last && threadIdx.x < 3) {
-        __threadfence();
-        double s = 0.0;
-        for (int64_t q = 0; q < nblocks; ++q) s += __ldcg(g.part + q * 3 + threadIdx.x);
-        if (g.norms) g.norms[threadIdx.x] = sqrt(s);
-    }
-    __syncthreads();  // s_red / s_last are reused by the next block of a persistent caller
+    nsi_norms(g, b, nblocks, done, su, sv, sc);
 }
 
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
     nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
 }
-// The f32 ring path: 4 blocks per SM (the waves nsi_shape fills), so at most 64 registers a thread.
-__global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_ring(NsiK g) {
-    extern __shared__ __align__(16) float nsi_ring[];
-    nsi_block<float, 4>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_ring);
+// The f32 tile path: one block per tile, 4 blocks per SM (64 registers a thread at most).
+__global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_tile(NsiK g) {
+    extern __shared__ __align__(16) float nsi_buf[];
+    nsi_tile_block(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_buf);
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
@@ -411,10 +423,11 @@ __global__ void k_nsi_plan(NsiTasksK g) {
         const cspb_ns_incomp_task& t = g.tasks[k];
         uint64_t nb = 0;
         if (t.nx >= 3 && t.ny >= 3 && t.u && t.v && t.p && t.ru && t.rv && t.rc) {
-            const int vfast = 4;
+            const bool fast = nsi_fast(t, 4);
             int H, segs;
             int64_t items, blocks;
-            nsi_shape(t.nx, t.ny, nsi_fast(t, vfast) ? vfast : 1, H, segs, items, blocks);
+            if (fast && !g.bf16) blocks = nsi_tiles(t.nx, t.ny);  // the f32 tile path
+            else nsi_shape(t.nx, t.ny, fast ? 4 : 1, H, segs, items, blocks);
             nb = uint64_t(blocks);
         } else {
             set_status(g.ctrl, CSPB_DEV_NEGATIVE);
@@ -425,7 +438,7 @@ __global__ void k_nsi_plan(NsiTasksK g) {
 
 template <typename T>
 __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
-    extern __shared__ __align__(16) float nsi_ring[];
+    extern __shared__ __align__(16) float nsi_buf[];
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = __ldcg(g.boff + g.count) <= g.cap_blocks && !status_bad(g.ctrl);
     __syncthreads();
@@ -462,7 +475,9 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
         const bool fast = nsi_fast(t, vfast);
         NsiK k{};
         int64_t blocks;
-        nsi_shape(t.nx, t.ny, fast ? vfast : 1, k.H, k.segs, k.items, blocks);
+        const bool tile = fast && sizeof(T) == 4;
+        if (tile) blocks = nsi_tiles(t.nx, t.ny);
+        else nsi_shape(t.nx, t.ny, fast ? vfast : 1, k.H, k.segs, k.items, blocks);
         k.nx = t.nx;
         k.ny = t.ny;
         k.inv2h = float(1.0 / (2.0 * t.h));
@@ -474,7 +489,8 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
         k.part = g.part + 3 * __ldcg(g.boff + lo);
         k.ctrl = g.ctrl;
         const int64_t b = int64_t(v) - int64_t(__ldcg(g.boff + lo));
-        if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo, nsi_ring);
+        if (tile) nsi_tile_block(k, b, blocks, g.done + lo, nsi_buf);
+        else if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
         else nsi_block<T, 1>(k, b, blocks, g.done + lo);
         v = share_work(next);
     }
@@ -488,9 +504,9 @@ using cspb_host::aligned;
 
 namespace {
 
-// The ring needs more than the default 48 KB of dynamic shared memory per block.
-bool ring_ready(const void* kern) {
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kNsiRingBytes)) == cudaSuccess;
+// A tile needs more than the default 48 KB of dynamic shared memory per block.
+bool tile_ready(const void* kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kNsiTileBytes)) == cudaSuccess;
 }
 
 struct NsiPlan {
@@ -538,8 +554,10 @@ extern "C" {
 
 size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny) {
     if (nx < 3 || ny < 3) return 0;
-    // the scalar plan (vec 1) has the most blocks
-    return nsi_plan(nx, ny, 1).ws;
+    // the scalar plan (vec 1) or the f32 tiles: whichever has more blocks
+    const size_t tiles = align_up(kCtrlBytes + size_t(nsi_tiles(nx, ny)) * 3 * sizeof(double), 256);
+    const size_t scalar = nsi_plan(nx, ny, 1).ws;
+    return tiles > scalar ? tiles : scalar;
 }
 
 int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
@@ -554,7 +572,12 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     const bool in_al = aligned(d->u, 16) && aligned(d->v, 16) && aligned(d->p, 16);
     const bool out_al = aligned(d->ru, 16) && aligned(d->rv, 16) && aligned(d->rc, 16);
     const bool fast = in_al && out_al && d->nx % vfast == 0;
-    const NsiPlan P = nsi_plan(d->nx, d->ny, fast ? vfast : 1);
+    NsiPlan P = nsi_plan(d->nx, d->ny, fast ? vfast : 1);
+    const bool tile = fast && !bf16;
+    if (tile) {
+        P.blocks = nsi_tiles(d->nx, d->ny);
+        P.ws = align_up(kCtrlBytes + size_t(P.blocks) * 3 * sizeof(double), 256);
+    }
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < P.ws) return CSPB_ERR_WORKSPACE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
@@ -577,8 +600,8 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
         if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
     } else if (fast) {
-        if (!ring_ready(reinterpret_cast<const void*>(k_ns_incomp_ring))) return CSPB_ERR_LAUNCH;
-        k_ns_incomp_ring<<<grid, block, kNsiRingBytes, st>>>(g);
+        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile))) return CSPB_ERR_LAUNCH;
+        k_ns_incomp_tile<<<grid, block, kNsiTileBytes, st>>>(g);
     } else {
         k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
@@ -622,8 +645,8 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
     if (r != CSPB_OK) return r;
     const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16>)
                               : reinterpret_cast<const void*>(k_nsi_tasks<float>);
-    const size_t smem = g.bf16 ? 0 : kNsiRingBytes;
-    if (smem && !ring_ready(kern)) return CSPB_ERR_LAUNCH;
+    const size_t smem = g.bf16 ? 0 : kNsiTileBytes;
+    if (smem && !tile_ready(kern)) return CSPB_ERR_LAUNCH;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNsiThreads, smem) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;
