@@ -308,6 +308,31 @@ def bench_sharded(torch, cb, dist, args):
             "scaling": "strong", "exchange_bytes_per_rank": 8 * n}
 
 
+def bench_ns_sharded(torch, cb, dist, args):
+    """ONE incompressible NS residual on the --grid² periodic grid split into y-slabs over the job's ranks
+    (cospanmdao_b200.sharded): strong scaling, one all-gather of the slabs' boundary rows and one of their squared
+    sums per step. ms is the max over ranks; GB/s is the whole grid's 24 B per cell over it."""
+    from cospanmdao_b200 import workloads
+    from cospanmdao_b200.sharded import ns_incompressible_sharded, shard_rows
+    N = args.grid
+    dev = torch.device("cuda", torch.cuda.current_device())
+    u, v, p, h = workloads.ns_fields(N, seed=0, device=dev)  # every rank builds the same grid and takes its rows
+    r0, r1 = shard_rows(N, dist.world, 32)[dist.rank]
+    mine = [f[r0:r1].contiguous() for f in (u, v, p)]
+    del u, v, p
+    ws = cb.Workspace(dev)
+    ranks = dist.r if dist.world > 1 else None
+
+    def step():
+        ns_incompressible_sharded(*mine, h=h, nu=1e-3, ranks=ranks, workspace=ws)
+
+    ms = timed(torch, dist, step, args.steps, args.warmup)
+    del mine
+    torch.cuda.empty_cache()
+    return {"ms": ms, "gbs_whole_grid": 24.0 * N * N / (ms * 1e-3) / 1e9, "ranks": dist.world, "rows_per_rank": r1 - r0,
+            "scaling": "strong", "halo_bytes_per_rank": 2 * 3 * 4 * N}
+
+
 def bench_chain(torch, cb, dist, args):
     from cospanmdao_b200 import workloads
     n = args.n
@@ -613,6 +638,7 @@ def main(argv=None) -> int:
         "gemver_bf16_storage": lambda: bench_gemver_bf16(torch, cb, dist, args),
         "gemver_chain": lambda: bench_chain(torch, cb, dist, args),
         "gemver_sharded": lambda: bench_sharded(torch, cb, dist, args),
+        "ns_sharded": lambda: bench_ns_sharded(torch, cb, dist, args),
         "ns_residual": lambda: bench_ns(torch, cb, dist, args),
         "ragged_batch": lambda: bench_ragged(torch, cb, dist, args, pk),
         "serving": lambda: bench_serving(torch, dist, args),

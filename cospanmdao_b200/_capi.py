@@ -61,6 +61,12 @@ class GemverRowsDesc(C.Structure):
                 ("workspace", vp), ("workspace_bytes", sz)]
 
 
+class NsIncompSlabDesc(C.Structure):
+    _fields_ = [("nx", i32), ("rows", i32), ("dtype", i32), ("flags", i32), ("h", C.c_double), ("nu", C.c_double),
+                ("u", vp), ("v", vp), ("p", vp), ("up", vp * 3), ("dn", vp * 3), ("ru", vp), ("rv", vp), ("rc", vp),
+                ("sums", vp), ("workspace", vp), ("workspace_bytes", sz)]
+
+
 class BicgkDesc(C.Structure):
     _fields_ = [("n", i64), ("ldb", i64), ("b_dtype", i32), ("flags", i32), ("B", vp), ("p", vp), ("r", vp),
                 ("q", vp), ("s", vp), ("workspace", vp), ("workspace_bytes", sz)]
@@ -108,6 +114,8 @@ PROTOTYPES = {
     "cspb_read_status": (C.c_int, [vp, C.POINTER(u32), vp]),
     "cspb_gemver_workspace_bytes": (sz, [i64]),
     "cspb_gemver_fused": (C.c_int, [C.POINTER(GemverDesc), vp]),
+    "cspb_ns_incomp_slab_workspace_bytes": (sz, [i32, i32]),
+    "cspb_ns_incomp_slab": (C.c_int, [C.POINTER(NsIncompSlabDesc), vp]),
     "cspb_gemver_rows_workspace_bytes": (sz, [i64, i64]),
     "cspb_gemver_rows_partial": (C.c_int, [C.POINTER(GemverRowsDesc), vp, vp]),
     "cspb_gemver_rows_finish": (C.c_int, [C.POINTER(GemverRowsDesc), vp, vp]),

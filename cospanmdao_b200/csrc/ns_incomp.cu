@@ -37,6 +37,11 @@ struct NsiK {
     double* norms;
     double* part;      // [blocks][3]
     uint32_t* ctrl;
+    // a y-slab of a larger grid (tile path only): the rows above and below the slab come from these rows of u, v, p
+    // (nx floats each) instead of wrapping, and `norms` receives the squared sums, not their roots
+    const float* up[3];
+    const float* dn[3];
+    int slab;
 };
 
 template <typename T, int VEC>
@@ -133,23 +138,31 @@ __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, float* buf, d
     // tile row r holds grid row y0 - 1 + r (wrapped), r = 0 .. th + 1
     for (int r = warp; r < th + 2; r += kNsiWarps) {
         int gy = y0 - 1 + r;
-        gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
-        const int64_t ro = int64_t(gy) * nx;
+        const float *ru_, *rv_, *rp_;  // the row's start in each field
+        if (g.slab && gy < 0) {
+            ru_ = g.up[0]; rv_ = g.up[1]; rp_ = g.up[2];
+        } else if (g.slab && gy >= g.ny) {
+            ru_ = g.dn[0]; rv_ = g.dn[1]; rp_ = g.dn[2];
+        } else {
+            gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
+            const int64_t ro = int64_t(gy) * nx;
+            ru_ = U + ro; rv_ = V + ro; rp_ = P + ro;
+        }
         float* row = buf + r * kNsiPitch;
         if (active) {
-            nsi_cp16(row + 4 + lane * 4, U + ro + c0);
-            nsi_cp16(row + kField + 4 + lane * 4, V + ro + c0);
-            nsi_cp16(row + 2 * kField + 4 + lane * 4, P + ro + c0);
+            nsi_cp16(row + 4 + lane * 4, ru_ + c0);
+            nsi_cp16(row + kField + 4 + lane * 4, rv_ + c0);
+            nsi_cp16(row + 2 * kField + 4 + lane * 4, rp_ + c0);
         }
         if (lane == 0) {
-            nsi_cp4(row + 3, U + ro + lcol);
-            nsi_cp4(row + kField + 3, V + ro + lcol);
-            nsi_cp4(row + 2 * kField + 3, P + ro + lcol);
+            nsi_cp4(row + 3, ru_ + lcol);
+            nsi_cp4(row + kField + 3, rv_ + lcol);
+            nsi_cp4(row + 2 * kField + 3, rp_ + lcol);
         }
         if (last) {
-            nsi_cp4(row + 4 + scols, U + ro + rcol);
-            nsi_cp4(row + kField + 4 + scols, V + ro + rcol);
-            nsi_cp4(row + 2 * kField + 4 + scols, P + ro + rcol);
+            nsi_cp4(row + 4 + scols, ru_ + rcol);
+            nsi_cp4(row + kField + 4 + scols, rv_ + rcol);
+            nsi_cp4(row + 2 * kField + 4 + scols, rp_ + rcol);
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -261,7 +274,7 @@ __device__ __forceinline__ void nsi_norms(const NsiK& g, int64_t b, int64_t nblo
         if (threadIdx.x < 3 && g.norms) {
             double t = s_red[0][threadIdx.x];
             for (int w = 1; w < kNsiWarps; ++w) t += s_red[w][threadIdx.x];
-            g.norms[threadIdx.x] = sqrt(t);
+            g.norms[threadIdx.x] = g.slab ? t : sqrt(t);  // a slab's squared sums are added across slabs first
         }
     }
     __syncthreads();  // the shared memory of this block is reused by the next block of a persistent caller
@@ -654,6 +667,49 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
     if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(kNsiThreads), args, smem, st) != cudaSuccess)
         return CSPB_ERR_LAUNCH;
     return CSPB_OK;
+}
+
+size_t cspb_ns_incomp_slab_workspace_bytes(int32_t nx, int32_t rows) {
+    if (nx < 3 || rows < 1) return 0;
+    return align_up(kCtrlBytes + size_t(nsi_tiles(nx, rows)) * 3 * sizeof(double), 256);
+}
+
+int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    if (d->nx < 3 || d->rows < 1) return CSPB_ERR_ARGUMENT;
+    if (!d->u || !d->v || !d->p || !d->ru || !d->rv || !d->rc || !d->sums) return CSPB_ERR_ARGUMENT;
+    for (int f = 0; f < 3; ++f)
+        if (!d->up[f] || !d->dn[f]) return CSPB_ERR_ARGUMENT;
+    if (!(d->h > 0.0) || !(d->nu >= 0.0)) return CSPB_ERR_ARGUMENT;
+    if (d->flags != 0) return CSPB_ERR_UNSUPPORTED;
+    // the tile path only: 16-byte aligned f32 rows
+    bool al = d->nx % 4 == 0 && aligned(d->u, 16) && aligned(d->v, 16) && aligned(d->p, 16) && aligned(d->ru, 16) &&
+              aligned(d->rv, 16) && aligned(d->rc, 16);
+    for (int f = 0; f < 3; ++f) al = al && aligned(d->up[f], 16) && aligned(d->dn[f], 16);
+    if (!al) return CSPB_ERR_UNSUPPORTED;
+    const size_t need = cspb_ns_incomp_slab_workspace_bytes(d->nx, d->rows);
+    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < need) return CSPB_ERR_WORKSPACE;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
+    NsiK g{};
+    g.nx = d->nx;
+    g.ny = d->rows;
+    g.inv2h = float(1.0 / (2.0 * d->h));
+    g.invh2 = float(1.0 / (d->h * d->h));
+    g.nu = float(d->nu);
+    g.u = d->u; g.v = d->v; g.p = d->p;
+    g.ru = d->ru; g.rv = d->rv; g.rc = d->rc;
+    g.norms = d->sums;
+    g.ctrl = static_cast<uint32_t*>(d->workspace);
+    g.part = reinterpret_cast<double*>(static_cast<char*>(d->workspace) + kCtrlBytes);
+    for (int f = 0; f < 3; ++f) {
+        g.up[f] = d->up[f];
+        g.dn[f] = d->dn[f];
+    }
+    g.slab = 1;
+    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile))) return CSPB_ERR_LAUNCH;
+    k_ns_incomp_tile<<<dim3(unsigned(nsi_tiles(d->nx, d->rows))), dim3(kNsiThreads), kNsiTileBytes, st>>>(g);
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
 }  // extern "C"

@@ -1,5 +1,7 @@
-"""One large GEMVER split by rows across the GPUs of a node (one process per GPU): the path's one exchange step.
+"""One large GEMVER split by rows, and one NS residual split into y-slabs, across the GPUs of a node (one process per
+GPU), each with its one exchange step.
 
+GEMVER
 Rank r holds rows [r0, r1) of A (and of B, u1, u2, y, w) and all of v1, v2, z (shard_rows gives the split). Every row
 is independent except for the column sums Âᵀy, which need every row. So a forward is:
 
@@ -95,3 +97,64 @@ def gemver_sharded(A, u1, v1, u2, v2, y, z=None, *, alpha, beta, ranks=None, wan
     x, w = gemver_rows_finish(A, u1, v1, u2, v2, y, z, total, alpha=alpha, beta=beta, B=B, workspace=workspace,
                               stream=stream)
     return B, x, w
+
+
+# ---- the incompressible NS residual in y-slabs ------------------------------------------------------------------------
+# Rank r holds rows [r0, r1) of u, v, p (shard_rows(ny, world, 32): tile-aligned). The stencil needs one row above and
+# one below each slab (periodic over the whole grid): every rank contributes its first and last rows to ONE
+# all-gather (2 · 3 · nx floats per rank) and takes the last row of the previous rank and the first row of the next.
+# Each rank then runs cspb_ns_incomp_slab; its residual rows are bit-identical to the whole grid's. The norms are
+# the square roots of the slabs' squared sums, added in rank order (a second all-gather of 3 doubles per rank).
+
+def exchange_halos(first, last, ranks):
+    """first, last: this rank's first and last rows of u, v, p (three (nx,) tensors each). Returns (up, dn): the rows
+    above this rank's slab (the previous rank's last rows, periodic) and below it (the next rank's first rows), three
+    tensors each. One slab: the grid wraps onto itself, and the rows are returned as they are (no copy)."""
+    import torch
+    if ranks is None or ranks.world == 1:
+        return list(last), list(first)
+    parts = ranks.all_gather_tensor(torch.stack([torch.stack(list(first)), torch.stack(list(last))]))
+    up = parts[(ranks.rank - 1) % ranks.world][1]
+    dn = parts[(ranks.rank + 1) % ranks.world][0]
+    return [up[f] for f in range(3)], [dn[f] for f in range(3)]
+
+
+def combine_sums(sums, ranks):
+    """The squared sums of every rank's slab, added in rank order, then their roots: the whole grid's norms."""
+    if ranks is None or ranks.world == 1:
+        return sums.sqrt()
+    parts = ranks.all_gather_tensor(sums)
+    total = parts[0].clone()
+    for q in parts[1:]:
+        total += q
+    return total.sqrt()
+
+
+def ns_incompressible_slab(u, v, p, up, dn, *, h, nu, out=None, sums=None, workspace=None, stream=None):
+    """The residual of one slab: u, v, p (rows, nx) f32; up, dn the rows above and below it (three (nx,) rows of u,
+    v, p each, or a (3, nx) tensor). Returns (ru, rv, rc, sums), sums being the slab's 3 squared sums (f64)."""
+    import torch
+    import cospanmdao_b200 as cb
+    rows, nx = u.shape
+    dev = u.device
+    ru, rv, rc = out if out is not None else tuple(torch.empty((rows, nx), dtype=torch.float32, device=dev)
+                                                  for _ in range(3))
+    sums = torch.empty(3, dtype=torch.float64, device=dev) if sums is None else sums
+    up = [up[f].contiguous() for f in range(3)]
+    dn = [dn[f].contiguous() for f in range(3)]
+    ws = workspace or cb.default_workspace(dev, stream)
+    wp, wb = ws.ptr(int(lib().cspb_ns_incomp_slab_workspace_bytes(nx, rows)))
+    d = _capi.NsIncompSlabDesc(nx, rows, F32, 0, float(h), float(nu), _ptr(u), _ptr(v), _ptr(p),
+                               (C.c_void_p * 3)(*[_ptr(up[f]) for f in range(3)]),
+                               (C.c_void_p * 3)(*[_ptr(dn[f]) for f in range(3)]), _ptr(ru), _ptr(rv), _ptr(rc),
+                               _ptr(sums), wp, wb)
+    cb._raise(lib().cspb_ns_incomp_slab(C.byref(d), C.c_void_p(cb._stream(stream))), "ns incompressible slab")
+    return ru, rv, rc, sums
+
+
+def ns_incompressible_sharded(u, v, p, *, h, nu, ranks=None, workspace=None, stream=None):
+    """This rank's slab of one NS residual: (ru, rv, rc) of its rows and the whole grid's norms (3, f64)."""
+    import torch
+    up, dn = exchange_halos((u[0], v[0], p[0]), (u[-1], v[-1], p[-1]), ranks)
+    ru, rv, rc, sums = ns_incompressible_slab(u, v, p, up, dn, h=h, nu=nu, workspace=workspace, stream=stream)
+    return ru, rv, rc, combine_sums(sums, ranks)

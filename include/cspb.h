@@ -325,6 +325,35 @@ typedef struct cspb_ns_incomp_desc {
 size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny);
 int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream);
 
+/* One y-slab of a larger periodic grid (one process per GPU): rows [r0, r0 + rows) of u, v, p, with the row above
+ * (r0 - 1) and the row below (r0 + rows), wrapped over the whole grid, passed as `up` and `dn` (nx floats of u, v, p
+ * each) instead of being read from the slab. The residual rows are bit-identical to cspb_ns_incompressible's on the
+ * whole grid; `sums` receives the slab's squared sums Σ r_u², Σ r_v², Σ r_c² (f64, 3), which the caller adds across
+ * slabs in a fixed order before taking the roots. f32 storage, nx % 4 == 0, every pointer 16-byte aligned; flags
+ * must be 0. The reference runs its residual on one device only (no counterpart); the exchange it implies is the
+ * one-row halo of each slab. */
+typedef struct cspb_ns_incomp_slab_desc {
+    int32_t nx, rows;    /* nx >= 3, rows >= 1 */
+    int32_t dtype;       /* CSPB_F32 */
+    int32_t flags;       /* 0 */
+    double h;
+    double nu;
+    const float* u;      /* rows × nx */
+    const float* v;
+    const float* p;
+    const float* up[3];  /* the row above the slab: u, v, p */
+    const float* dn[3];  /* the row below the slab: u, v, p */
+    float* ru;           /* rows × nx */
+    float* rv;
+    float* rc;
+    double* sums;        /* 3 doubles: the slab's squared sums */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_ns_incomp_slab_desc;
+
+size_t cspb_ns_incomp_slab_workspace_bytes(int32_t nx, int32_t rows);
+int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream);
+
 /* Many incompressible residuals (any sizes, one storage dtype) in ONE persistent launch, from a DEVICE array of task
  * descriptors. max_cells bounds Σ nx·ny (it sizes the workspace). Per-task results, norms included, are bit-identical
  * to cspb_ns_incompressible on the same task (the same decomposition, the same reduction order). */

@@ -77,3 +77,39 @@ def test_shard_rows():
     assert shard_rows(16384, 8) == [(2048 * r, 2048 * (r + 1)) for r in range(8)]
     with pytest.raises(ValueError):
         shard_rows(10, 0)
+
+
+def _halo_rank(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import torch
+    from cospanmdao_b200.replicas import Ranks
+    from cospanmdao_b200.sharded import combine_sums, exchange_halos
+    r = Ranks().init("gloo", timeout_s=60)
+    nx = 12
+    # rank q's first row of field f holds 100·q + 10·f + 0, its last row 100·q + 10·f + 1 (every column)
+    first = [torch.full((nx,), 100.0 * rank + 10 * f) for f in range(3)]
+    last = [t + 1 for t in first]
+    up, dn = exchange_halos(first, last, r)
+    up, dn = torch.stack(up), torch.stack(dn)
+    norms = combine_sums(torch.tensor([1.0 + rank, 2.0, 3.0 * rank], dtype=torch.float64), r)
+    np.save(Path(out_dir) / f"halo{rank}.npy", np.stack([up.numpy(), dn.numpy()]))
+    np.save(Path(out_dir) / f"norms{rank}.npy", norms.numpy())
+    r.barrier()
+    r.close()
+
+
+def test_three_ranks_exchange_halo_rows(tmp_path):
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_halo_rank, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for q in range(world):
+        up, dn = np.load(tmp_path / f"halo{q}.npy")
+        prev, nxt = (q - 1) % world, (q + 1) % world
+        for f in range(3):
+            assert np.all(up[f] == 100.0 * prev + 10 * f + 1)  # the previous rank's last row
+            assert np.all(dn[f] == 100.0 * nxt + 10 * f)       # the next rank's first row
+    want = np.sqrt(np.array([1.0 + 2.0 + 3.0, 2.0 * 3, 3.0 * (0 + 1 + 2)]))
+    for q in range(world):
+        assert np.array_equal(np.load(tmp_path / f"norms{q}.npy"), want)

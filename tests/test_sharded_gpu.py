@@ -84,3 +84,33 @@ def test_row_shard_argument_errors(cuda):
     d.n, d.rows = 100, 101  # more rows than columns
     assert lib.cspb_gemver_rows_partial(C.byref(d), None, None) == _capi.ERR_ARGUMENT
     assert lib.cspb_gemver_rows_workspace_bytes(100, 101) == 0
+
+
+@pytest.mark.parametrize("nx,ny,world", [(512, 512, 1), (512, 512, 2), (260, 150, 3), (1024, 700, 5)])
+def test_ns_slabs_match_the_whole_grid(cuda, nx, ny, world):
+    """cspb_ns_incomp_slab on y-slabs with the neighbouring rows passed as halos: the residual rows equal the whole
+    grid's bit for bit (the same per-cell formula), and the roots of the rank-order sums of the slabs' squared sums
+    equal the whole grid's norms to f64 rounding."""
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200.sharded import ns_incompressible_slab, shard_rows
+    g = torch.Generator(device="cpu").manual_seed(nx + ny + world)
+    u, v, p = ((torch.rand((ny, nx), generator=g) - 0.5).to(cuda) for _ in range(3))
+    h, nu = 0.05, 1e-3
+    ru, rv, rc, norms = cb.ns_incompressible(u, v, p, h=h, nu=nu)
+    outs, sums = [], []
+    for r0, r1 in shard_rows(ny, world, 32):
+        assert r1 > r0
+        up = torch.stack([f[(r0 - 1) % ny] for f in (u, v, p)])
+        dn = torch.stack([f[r1 % ny] for f in (u, v, p)])
+        a, b, c, s = ns_incompressible_slab(u[r0:r1], v[r0:r1], p[r0:r1], up, dn, h=h, nu=nu,
+                                            workspace=cb.Workspace(cuda))
+        outs.append((a, b, c))
+        sums.append(s)
+    torch.cuda.synchronize()
+    for k, whole in enumerate((ru, rv, rc)):
+        assert torch.equal(torch.cat([o[k] for o in outs]), whole)
+    total = sums[0].clone()
+    for s in sums[1:]:
+        total += s
+    assert torch.allclose(total.sqrt(), norms, rtol=1e-12, atol=0)
