@@ -449,8 +449,10 @@ __global__ void k_nsi_plan(NsiTasksK g) {
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
+// MINB: blocks per SM the registers must allow (f32: 4, so that its tiles run 4 blocks per SM as in the single
+// call; bf16: 2, its register path's 128 registers)
+template <typename T, int MINB>
+__global__ void __launch_bounds__(kNsiThreads, MINB) k_nsi_tasks(NsiTasksK g) {
     extern __shared__ __align__(16) float nsi_buf[];
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = __ldcg(g.boff + g.count) <= g.cap_blocks && !status_bad(g.ctrl);
@@ -502,9 +504,14 @@ __global__ void __launch_bounds__(kNsiThreads) k_nsi_tasks(NsiTasksK g) {
         k.part = g.part + 3 * __ldcg(g.boff + lo);
         k.ctrl = g.ctrl;
         const int64_t b = int64_t(v) - int64_t(__ldcg(g.boff + lo));
-        if (tile) nsi_tile_block(k, b, blocks, g.done + lo, nsi_buf);
-        else if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
-        else nsi_block<T, 1>(k, b, blocks, g.done + lo);
+        if (tile) {
+            nsi_tile_block(k, b, blocks, g.done + lo, nsi_buf);
+        } else if constexpr (sizeof(T) == 2) {  // f32 fast tasks are tiles
+            if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
+            else nsi_block<T, 1>(k, b, blocks, g.done + lo);
+        } else {
+            nsi_block<T, 1>(k, b, blocks, g.done + lo);
+        }
         v = share_work(next);
     }
 }
@@ -656,8 +663,8 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
     const int r = cspb_exclusive_scan_u64(g.blocks, g.boff, count, ws + L.off_scan, cspb_scan_workspace_bytes(count),
                                           stream);
     if (r != CSPB_OK) return r;
-    const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16>)
-                              : reinterpret_cast<const void*>(k_nsi_tasks<float>);
+    const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16, 2>)
+                              : reinterpret_cast<const void*>(k_nsi_tasks<float, 4>);
     const size_t smem = g.bf16 ? 0 : kNsiTileBytes;
     if (smem && !tile_ready(kern)) return CSPB_ERR_LAUNCH;
     int per_sm = 0;
