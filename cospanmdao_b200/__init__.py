@@ -147,9 +147,10 @@ def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: b
     stride from A.stride(0) is honoured). schedule 'barrier' (three streaming passes), 'bulk' (the same passes fed
     through a shared-memory ring by bulk copies; used when n is a multiple of 4 (f32) / 8 (bf16) and the operands are
     16-byte aligned, else 'barrier') or 'panel' (column panels pipelined through L2) all give the same bits.
-    'lowrank' (only without Â: want_B False and no B) applies the rank-2 update as four dot products, so both passes
-    over A are plain GEMVs: other rounding, within the f64 tolerance. 'auto' (the default) is 'lowrank' for a bfloat16
-    matrix without Â and 'barrier' otherwise. Returns (B or None, x, w)."""
+    'lowrank' applies the rank-2 update as four dot products: without Â both passes over A are plain GEMVs; with Â
+    and a bfloat16 matrix only w does (pass 2 re-reads A); with Â and a float32 matrix it is 'barrier'. Other rounding,
+    within the f64 tolerance. 'auto' (the default) is 'lowrank' for a bfloat16 matrix and 'barrier' otherwise.
+    Returns (B or None, x, w)."""
     if schedule not in ("auto", "panel", "barrier", "bulk", "lowrank"):
         raise ValueError("schedule must be 'auto', 'barrier', 'bulk', 'panel' or 'lowrank'")
     torch = _torch()
@@ -178,7 +179,7 @@ def gemver(A, u1, v1, u2, v2, y, z=None, *, alpha: float, beta: float, want_B: b
     if not 0 <= int(lag) <= 255:
         raise ValueError("lag must be in [0, 255]")
     if schedule == "auto":
-        schedule = "lowrank" if B is None and A.dtype == torch.bfloat16 else "barrier"
+        schedule = "lowrank" if A.dtype == torch.bfloat16 else "barrier"
     flags = {"panel": _capi.GEMVER_PANEL, "bulk": _capi.GEMVER_BULK,
              "lowrank": _capi.GEMVER_LOWRANK}.get(schedule, 0) | (int(lag) << 8)
     d = _capi.GemverDesc(n, A.stride(0), B.stride(0) if B is not None else n, _mat_dtype(A), flags, _ptr(A), _ptr(u1),

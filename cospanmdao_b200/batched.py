@@ -102,11 +102,11 @@ class RaggedBatch:
     # ---- the launch ------------------------------------------------------------------------------------------------
     def run(self, tune: int = 0, stream=None, check: bool = False, lowrank: bool | None = None):
         """One launch over the batch. lowrank: instances without B take the low-rank form (the rank-2 update as dot
-        products); None follows cb.gemver's 'auto' schedule (bf16 without B)."""
+        products; with B only w of a bf16 batch); None follows cb.gemver's 'auto' schedule (bf16)."""
         import cospanmdao_b200 as cb
         torch = _torch()
         if lowrank is None:
-            lowrank = self.dtype == torch.bfloat16 and self.B is None
+            lowrank = self.dtype == torch.bfloat16
         tune = int(tune) | (_capi.BATCH_LOWRANK if lowrank else 0)
         p = int(self.ws.data_ptr())
         wp = (p + 255) // 256 * 256

@@ -219,8 +219,8 @@ __device__ __forceinline__ void instance_x_lr(const PassArgs& a, const float* z,
 // the batching does not change the arithmetic)
 template <typename T> inline constexpr int kLrRows = sizeof(T) == 4 ? 16 : 8;
 
-// LR: an instance without Â takes the low-rank form of cspb_gemver_fused with CSPB_GEMVER_LOWRANK (column sums of
-// A·y, then row dots of A·x; the rank-2 terms in the finishes).
+// LR: an instance takes the low-rank form of cspb_gemver_fused with CSPB_GEMVER_LOWRANK: without Â, column sums of
+// A·y, then row dots of A·x, the rank-2 terms in the finishes; with Â and a 16-bit A, pass 2 and the w finish only.
 template <typename T, int WX, bool LR>
 __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
     if (LR && a.dst == nullptr) pass_unit<T, WX, true, false, false, true, false, kLrRows<T>>(a, unit, vec_ok, smem);
@@ -230,8 +230,10 @@ __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_
 // (or, low-rank, without it).
 template <typename T, int WX, bool LR>
 __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    if (LR && a.dst == nullptr) {
-        pass_unit<T, WX, true, false, false, false, true, kLrRows<T>, true>(a, unit, vec_ok, smem);
+    if (LR && (a.dst == nullptr || sizeof(T) == 2)) {  // low-rank: w from A (also when a 16-bit A's Â is stored)
+        PassArgs b = a;
+        b.dst = nullptr;  // pass 2 only reads A
+        pass_unit<T, WX, true, false, false, false, true, kLrRows<T>, true>(b, unit, vec_ok, smem);
     } else if (sizeof(T) == 4 && a.dst != nullptr) {
         PassArgs b = a;
         b.src = a.dst;
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 const int64_t strip = int64_t(f - sbase);
                 if (!wait_for(g.strip_done + sbase + uint64_t(strip), uint32_t(a.chunks))) { stop = true; break; }
                 const int64_t S = rows_of(wx);
-                const bool lr = LR && a.dst == nullptr;
+                const bool lr = LR && (a.dst == nullptr || bf16);  // as unit2
                 double t1 = 0.0, t2 = 0.0;
                 if (lr) block_dot2(a.v1, a.v2, a.xv, a.n, t1, t2);  // x is complete: every chunk fed this strip
                 for (int64_t row = strip * S + threadIdx.x; row < (strip + 1) * S && row < a.n; row += blockDim.x) {

@@ -83,18 +83,25 @@ struct LowRankK {
     float* x;
 };
 
-template <typename T>
+// STORE: Â is requested (16-bit A only): pass 1 forms and stores it and x comes from its column sums, as k_gemver's;
+// only pass 2 takes the low-rank form (w from A, the rank-2 terms in the finish) instead of forming Â again.
+template <typename T, bool STORE>
 __global__ void __launch_bounds__(kPassThreads, 2) k_gemver_lr(LowRankK g, int vec_ok) {
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
     for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0);
-        pass_unit<T, kWX, true, false, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
+        if constexpr (STORE) pass_unit<T, kWX, true, true, false, true, false, 0>(g.p1, u, vec_ok != 0, smem);
+        else pass_unit<T, kWX, true, false, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
         u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
-    double s1, s2;
-    block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
-    colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, s1, s2, g.x);
+    if constexpr (STORE) {
+        colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
+    } else {
+        double s1, s2;
+        block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
+        colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, s1, s2, g.x);
+    }
     if (!grid_barrier(g.ctrl)) return;
     for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
@@ -518,13 +525,19 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t zero = L.off_PA;  // ctrl, strip_done, chunk_done, x_ready
 
-    // without Â, the low-rank form (takes precedence over the schedule flags)
-    if ((d->flags & CSPB_GEMVER_LOWRANK) && d->B == nullptr) {
+    // the low-rank form: without Â (any dtype), or with Â and a 16-bit matrix (pass 2 only); it takes precedence over
+    // the schedule flags. With Â and an f32 matrix pass 2 reads the stored Â, and the flag is ignored.
+    if ((d->flags & CSPB_GEMVER_LOWRANK) && (d->B == nullptr || bf16)) {
+        const bool store = d->B != nullptr;
         LowRankK g{};
         g.p1 = p1;
-        g.p1.dst = nullptr;
-        g.p1.u1 = g.p1.v1 = g.p1.u2 = g.p1.v2 = nullptr;
+        if (!store) {
+            g.p1.dst = nullptr;
+            g.p1.u1 = g.p1.v1 = g.p1.u2 = g.p1.v2 = nullptr;
+        }
         g.p2 = p2;
+        g.p2.src = d->A;  // pass 2 reads A (the 16-bit matrix), never the stored Â
+        g.p2.lds = d->lda;
         g.ctrl = reinterpret_cast<uint32_t*>(ws);
         g.units = L.units;
         g.u1 = d->u1; g.v1 = d->v1; g.u2 = d->u2; g.v2 = d->v2;
@@ -533,8 +546,9 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
         g.beta = d->beta;
         g.x = d->x;
         void* args[] = {&g, const_cast<int*>(&vec_ok)};
-        if (bf16) return launch_coop(k_gemver_lr<__nv_bfloat16>, args, L.units, zero, ws, st);
-        return launch_coop(k_gemver_lr<float>, args, L.units, zero, ws, st);
+        if (bf16 && store) return launch_coop(k_gemver_lr<__nv_bfloat16, true>, args, L.units, zero, ws, st);
+        if (bf16) return launch_coop(k_gemver_lr<__nv_bfloat16, false>, args, L.units, zero, ws, st);
+        return launch_coop(k_gemver_lr<float, false>, args, L.units, zero, ws, st);
     }
     // the bulk-copy ring: every row segment and vector piece must start on 16 bytes and be a multiple of 16 bytes long
     const int vw = bf16 ? 8 : 4;

@@ -60,9 +60,9 @@ class TaskRunner:
 
     def gemver(self, table: np.ndarray, *, bf16: bool, tune: int = 0, lowrank: bool | None = None, stream=None,
                host_staging=None):
-        """Runs a GEMVER task table. lowrank: tasks without B take the low-rank form (the rank-2 update as dot
-        products); None (the default) follows cb.gemver's 'auto' schedule, so that every task gets the single call's
-        form: low-rank for bf16, not for f32."""
+        """Runs a GEMVER task table. lowrank: the low-rank form (the rank-2 update as dot products) for tasks without
+        B, and for w of bf16 tasks with B; None (the default) follows cb.gemver's 'auto' schedule, so that every task
+        gets the single call's form: low-rank for bf16, not for f32."""
         import cospanmdao_b200 as cb
         torch = _torch()
         count = int(table.size)

@@ -85,8 +85,10 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream);
 #define CSPB_GEMVER_BULK 2
 /* flags = CSPB_GEMVER_LOWRANK with B == NULL: x and w are formed from A with the rank-2 update applied as four dot
  * products, x = β·(Aᵀy + v1(u1·y) + v2(u2·y)) + z and w = α·(A·x + u1(v1·x) + u2(v2·x)), in two streaming passes with
- * no per-element update. Other rounding than the schedules that form Â (within the f64 tolerance, not the same bits);
- * ignored when B is requested. No counterpart in the reference, whose GEMVER always forms B. */
+ * no per-element update. With B requested and a CSPB_BF16 matrix, pass 1 forms and stores Â and x comes from its
+ * column sums as in the other schedules; only w takes the low-rank form (pass 2 re-reads the 16-bit A instead of
+ * forming Â again). Other rounding than the schedules that form Â (within the f64 tolerance, not the same bits);
+ * ignored for an f32 matrix with B. No counterpart in the reference, whose GEMVER always forms B. */
 #define CSPB_GEMVER_LOWRANK 4
 /* bits 8..15 of flags: the panel schedule's lag (pass 2 over a panel follows pass 1 over it by this many panels);
  * 0 = automatic (the panels the blocks in flight hold, plus one). A tuning knob: results do not depend on it. */

@@ -243,7 +243,14 @@ def test_gemver_lowrank_against_f64(cuda, n, dtype_name, lda):
     if dtype_name == "bfloat16":  # the default for a bf16 matrix without Â
         _, x3, w3 = cb.gemver(*args, alpha=0.8, beta=-1.3, want_B=False)
         assert torch.equal(x, x3) and torch.equal(w, w3)
-    # with Â requested the flag is ignored: the barrier schedule's bits
+    # with Â requested: Â and x are the barrier schedule's bits; w is the barrier's for f32 (the flag is ignored) and
+    # the low-rank w for bf16 (within the tolerance of the f64 result)
     Bb, xb, wb = cb.gemver(*args, alpha=0.8, beta=-1.3, schedule="barrier")
     Bl, xl, wl = cb.gemver(*args, alpha=0.8, beta=-1.3, schedule="lowrank")
-    assert torch.equal(Bb, Bl) and torch.equal(xb, xl) and torch.equal(wb, wl)
+    assert torch.equal(Bb, Bl) and torch.equal(xb, xl)
+    if dtype_name == "float32":
+        assert torch.equal(wb, wl)
+    else:
+        assert oracle.rel_l2(_np(wl), wo) < TOL
+        _, _, wa = cb.gemver(*args, alpha=0.8, beta=-1.3)  # the default for bf16
+        assert torch.equal(wa, wl)
