@@ -25,19 +25,19 @@ namespace nsc {
 constexpr int TX = 32, TY = 16;              // tile of cells
 constexpr int LX = TX + 4, LY = TY + 4;      // with the 2-cell halo
 constexpr int LC = LX * LY;                  // 720
-constexpr int GX = TX + 2, GY = TY + 2;      // cells [-1, T] that need gradients and slopes
-constexpr int GC = GX * GY;                  // 612
 constexpr int NXF = (TX + 1) * TY;           // x-faces of the tile's rows
 constexpr int NYF = TX * (TY + 1);           // y-faces of the tile's columns
 constexpr int kThreads = 256;
 
 constexpr float kG = 1.4f, kMu = 0.01f, kPr = 0.72f, kCfl = 0.5f;
 
+// The tile's state in shared memory: primitives and temperature of the tile with its 2-cell halo, and both fluxes of
+// every face. A face forms the gradients and limited slopes of its two cells from W and T itself, with the formulas
+// a per-cell table would hold (the same bits): a table of both for the 612 cells [-1, T] took 34 KB more, which left
+// room for 2 tiles per SM instead of 4.
 struct Smem {
     float W[4][LC];  // primitives ρ u v p
     float T[LC];     // p / ρ
-    float G[6][GC];  // ux uy vx vy Tx Ty
-    float S[8][GC];  // x-slopes ρ u v p, y-slopes ρ u v p
     float FX[8][NXF];  // HLLC 0..3, viscous 4..7
     float FY[8][NYF];
 };
@@ -135,7 +135,7 @@ constexpr int kDtKey = 16, kWsBits = 17, kSq0 = 18;
 __device__ __forceinline__ int wrapi(int k, int n) { return ((k % n) + n) % n; }
 
 template <int LIM>
-__global__ void __launch_bounds__(kThreads, 2) k_ns_comp(K g) {
+__global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& s = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x;
@@ -173,58 +173,44 @@ __global__ void __launch_bounds__(kThreads, 2) k_ns_comp(K g) {
     }
     __syncthreads();
 
-    // 2. cell gradients and limited slopes of cells [-1, T] (tile_gradients, tile_reconstruct)
-    for (int idx = tid; idx < GC; idx += kThreads) {
-        const int gb = idx / GX, ga = idx - gb * GX;
-        const int c = (gb + 1) * LX + (ga + 1);
-        s.G[0][idx] = 0.5f * (s.W[1][c + 1] - s.W[1][c - 1]);
-        s.G[1][idx] = 0.5f * (s.W[1][c + LX] - s.W[1][c - LX]);
-        s.G[2][idx] = 0.5f * (s.W[2][c + 1] - s.W[2][c - 1]);
-        s.G[3][idx] = 0.5f * (s.W[2][c + LX] - s.W[2][c - LX]);
-        s.G[4][idx] = 0.5f * (s.T[c + 1] - s.T[c - 1]);
-        s.G[5][idx] = 0.5f * (s.T[c + LX] - s.T[c - LX]);
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const float w0 = s.W[v][c];
-            s.S[v][idx] = slope<LIM>(w0 - s.W[v][c - 1], s.W[v][c + 1] - w0);
-            s.S[4 + v][idx] = slope<LIM>(w0 - s.W[v][c - LX], s.W[v][c + LX] - w0);
-        }
-    }
-    __syncthreads();
-
-    // 3. every face of the tile's cells, once (tile_conv_flux, tile_visc_flux)
+    // 2. every face of the tile's cells, once (tile_gradients, tile_reconstruct, tile_conv_flux, tile_visc_flux):
+    // the limited slopes along the face's direction and the 6 gradients of its two cells, then both fluxes
     for (int f = tid; f < NXF + NYF; f += kThreads) {
-        int d, cl, cr, gl, gr;
+        int d, cl, cr;
         if (f < NXF) {
             d = 0;
             const int r = f / (TX + 1), k = f - r * (TX + 1);  // between tile cells (r, k-1) and (r, k)
             cl = (r + 2) * LX + (k + 1);
             cr = cl + 1;
-            gl = (r + 1) * GX + k;
-            gr = gl + 1;
         } else {
             d = 1;
             const int q = f - NXF;
             const int r = q / TX, k = q - r * TX;  // between tile cells (r-1, k) and (r, k)
             cl = (r + 1) * LX + (k + 2);
             cr = cl + LX;
-            gl = r * GX + (k + 1);
-            gr = gl + GX;
         }
+        const int st = d == 0 ? 1 : LX;  // the neighbour along the face's direction
         float pl[4], pr[4], wl[4], wr[4], gL[6], gR[6], Fc[4], Fv[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             pl[v] = s.W[v][cl];
             pr[v] = s.W[v][cr];
-            wl[v] = pl[v] + 0.5f * s.S[4 * d + v][gl];
-            wr[v] = pr[v] - 0.5f * s.S[4 * d + v][gr];
+            const float sl = slope<LIM>(pl[v] - s.W[v][cl - st], s.W[v][cl + st] - pl[v]);
+            const float sr = slope<LIM>(pr[v] - s.W[v][cr - st], s.W[v][cr + st] - pr[v]);
+            wl[v] = pl[v] + 0.5f * sl;
+            wr[v] = pr[v] - 0.5f * sr;
         }
         hllc(wl, wr, d, Fc);
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            gL[q] = s.G[q][gl];
-            gR[q] = s.G[q][gr];
-        }
+        auto grads = [&](int c, float (&gq)[6]) {  // ux uy vx vy Tx Ty of cell c
+            gq[0] = 0.5f * (s.W[1][c + 1] - s.W[1][c - 1]);
+            gq[1] = 0.5f * (s.W[1][c + LX] - s.W[1][c - LX]);
+            gq[2] = 0.5f * (s.W[2][c + 1] - s.W[2][c - 1]);
+            gq[3] = 0.5f * (s.W[2][c + LX] - s.W[2][c - LX]);
+            gq[4] = 0.5f * (s.T[c + 1] - s.T[c - 1]);
+            gq[5] = 0.5f * (s.T[c + LX] - s.T[c - LX]);
+        };
+        grads(cl, gL);
+        grads(cr, gR);
         visc(pl, pr, s.T[cl], s.T[cr], gL, gR, d, Fv);
         float* out = d == 0 ? &s.FX[0][f] : &s.FY[0][f - NXF];
         const int stride = d == 0 ? NXF : NYF;
@@ -236,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_ns_comp(K g) {
     }
     __syncthreads();
 
-    // 4. R = -div F_conv + div F_visc per cell (cell_divergence), and the per-cell diagnostics
+    // 3. R = -div F_conv + div F_visc per cell (cell_divergence), and the per-cell diagnostics
     float dtmin = 3.0e38f, wsmax = 0.0f;
     float sqf[4] = {0.f, 0.f, 0.f, 0.f};
     double sqd[4] = {0.0, 0.0, 0.0, 0.0};
@@ -266,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_ns_comp(K g) {
         wsmax = fmx(wsmax, ws);
     }
 
-    // 5. the tile's reductions (fixed order: xor tree in the warp, warps in order)
+    // 4. the tile's reductions (fixed order: xor tree in the warp, warps in order)
     __shared__ float r_dt[kThreads / 32], r_ws[kThreads / 32], r_sqf[kThreads / 32][4];
     __shared__ double r_sqd[kThreads / 32][4];
     __shared__ int s_last;
