@@ -460,7 +460,10 @@ def bench_serving(torch, dist, args):
     wl = serving.make_workload(args.requests, rate=None, seed=0)
     srv = serving.Server(wl, budget_bytes=120e9, max_batch=args.max_batch, depth=4)
     srv.run()  # warm-up pass (allocations, first launches)
-    sat = srv.run()
+    # the server is driven from the host: a host stall longer than the queued work (4 batches, ~24 ms) idles the GPU,
+    # so each figure is the median run of three, with every run's value listed
+    runs = sorted((srv.run() for _ in range(3)), key=lambda r: r["req_per_s"])
+    sat = dict(runs[1], runs_req_per_s=[r["req_per_s"] for r in runs])
     sample = [int(i) for i in np.linspace(0, wl.count - 1, 24).astype(int)]
     res["batched_bf16_saturation"] = {k: v for k, v in sat.items()}
     res["same_alone_and_in_mix"] = bool(serving.check_mix(srv, sample))
@@ -473,7 +476,9 @@ def bench_serving(torch, dist, args):
     rate = 0.5 * sat["req_per_s"]
     wl2 = serving.make_workload(args.requests, rate=rate, seed=1)
     srv2 = serving.Server(wl2, budget_bytes=120e9, max_batch=args.max_batch, depth=4)
-    res["batched_bf16_at_rate"] = dict(srv2.run(), rate_req_per_s=rate)
+    srv2.run()  # warm-up pass
+    runs = sorted((srv2.run() for _ in range(3)), key=lambda r: r["p99_ms"])
+    res["batched_bf16_at_rate"] = dict(runs[1], rate_req_per_s=rate, runs_p99_ms=[r["p99_ms"] for r in runs])
     del srv2
     torch.cuda.empty_cache()
     pl2 = serving.plain(wl2)
