@@ -57,15 +57,20 @@ __device__ __forceinline__ float slope(float a, float b) {
     }
 }
 
-// HLLC with Davis speeds; d = 0 normal x, d = 1 normal y; L / R primitives (ρ, u, v, p).
-__device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], int d, float (&F)[4]) {
-    const float g = kG;
+// 1 / (γ - 1), rounded once
+constexpr float kInvGm1 = 1.0f / (kG - 1.0f);
+
+// HLLC with Davis speeds; D = 0 normal x, D = 1 normal y; L / R primitives (ρ, u, v, p). The divisions by ρ of a side
+// are products with its reciprocal (one correctly rounded reciprocal per side), p / (γ - 1) a product with 1 / (γ - 1).
+template <int D>
+__device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], float (&F)[4]) {
     const float rl = L[0], rr = R[0], pl = L[3], pr = R[3];
-    const float unl = d == 0 ? L[1] : L[2], utl = d == 0 ? L[2] : L[1];
-    const float unr = d == 0 ? R[1] : R[2], utr = d == 0 ? R[2] : R[1];
-    const float cl = sqrtf(g * pl / rl), cr = sqrtf(g * pr / rr);
-    const float El = pl / (g - 1.0f) + 0.5f * rl * (unl * unl + utl * utl);
-    const float Er = pr / (g - 1.0f) + 0.5f * rr * (unr * unr + utr * utr);
+    const float unl = L[1 + D], utl = L[2 - D];
+    const float unr = R[1 + D], utr = R[2 - D];
+    const float irl = __frcp_rn(rl), irr = __frcp_rn(rr);
+    const float cl = sqrtf(kG * pl * irl), cr = sqrtf(kG * pr * irr);
+    const float El = pl * kInvGm1 + 0.5f * rl * (unl * unl + utl * utl);
+    const float Er = pr * kInvGm1 + 0.5f * rr * (unr * unr + utr * utr);
     const float sl = fmn(unl - cl, unr - cr);
     const float sr = fmx(unl + cl, unr + cr);
     const float sm = (pr - pl + rl * unl * (sl - unl) - rr * unr * (sr - unr)) / (rl * (sl - unl) - rr * (sr - unr));
@@ -77,31 +82,34 @@ __device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], i
     } else {
         const bool left = sm >= 0.0f;
         const float r = left ? rl : rr, un = left ? unl : unr, ut = left ? utl : utr, p = left ? pl : pr;
-        const float E = left ? El : Er, s = left ? sl : sr;
-        const float k = r * (s - un) / (s - sm);
-        const float Es = k * (E / r + (sm - un) * (sm + p / (r * (s - un))));
+        const float E = left ? El : Er, s = left ? sl : sr, ir = left ? irl : irr;
+        const float a = s - un;
+        const float k = r * a / (s - sm);
+        const float Es = k * (E * ir + (sm - un) * (sm + p * ir / a));
         f0 = r * un + s * (k - r);
         f1 = r * un * un + p + s * (k * sm - r * un);
         f2 = r * un * ut + s * (k * ut - r * ut);
         f3 = (E + p) * un + s * (Es - E);
     }
     F[0] = f0;
-    F[1] = d == 0 ? f1 : f2;
-    F[2] = d == 0 ? f2 : f1;
+    F[1 + D] = f1;
+    F[2 - D] = f2;
     F[3] = f3;
 }
 
-// L / R primitives of the two cells of the face, their temperatures and cell gradients (ux uy vx vy Tx Ty).
-__device__ __forceinline__ void visc(const float (&L)[4], const float (&R)[4], float TL, float TR, const float (&gl)[6],
-                                     const float (&gr)[6], int d, float (&F)[4]) {
+// The viscous flux through a face of normal D: the normal derivatives are the differences of the two cells; the
+// tangential ones (ut_u, ut_v, ut_T) the means of the two cells' central differences.
+template <int D>
+__device__ __forceinline__ void visc(const float (&L)[4], const float (&R)[4], float TL, float TR, float du_t,
+                                     float dv_t, float dT_t, float (&F)[4]) {
     const float uf = 0.5f * (L[1] + R[1]), vf = 0.5f * (L[2] + R[2]);
     float ux, uy, vx, vy, Tx, Ty;
-    if (d == 0) {
+    if (D == 0) {
         ux = R[1] - L[1]; vx = R[2] - L[2]; Tx = TR - TL;
-        uy = 0.5f * (gl[1] + gr[1]); vy = 0.5f * (gl[3] + gr[3]); Ty = 0.5f * (gl[5] + gr[5]);
+        uy = du_t; vy = dv_t; Ty = dT_t;
     } else {
         uy = R[1] - L[1]; vy = R[2] - L[2]; Ty = TR - TL;
-        ux = 0.5f * (gl[0] + gr[0]); vx = 0.5f * (gl[2] + gr[2]); Tx = 0.5f * (gl[4] + gr[4]);
+        ux = du_t; vx = dv_t; Tx = dT_t;
     }
     const float mu = kMu;
     const float k = mu * kG / ((kG - 1.0f) * kPr);
@@ -110,10 +118,41 @@ __device__ __forceinline__ void visc(const float (&L)[4], const float (&R)[4], f
     const float tyy = mu * (2.0f * vy - 2.0f / 3.0f * dv);
     const float txy = mu * (uy + vx);
     F[0] = 0.0f;
-    if (d == 0) {
+    if (D == 0) {
         F[1] = txx; F[2] = txy; F[3] = uf * txx + vf * txy + k * Tx;
     } else {
         F[1] = txy; F[2] = tyy; F[3] = uf * txy + vf * tyy + k * Ty;
+    }
+}
+
+// One face of normal D between cells cl and cl + st (st the neighbour along the normal): the limited slopes of both
+// cells along the normal, the reconstructed states, the HLLC flux, the tangential gradients of both cells and the
+// viscous flux; the 8 fluxes go to out[v * stride] (HLLC 0..3, viscous 4..7).
+template <int LIM, int D, int stride>
+__device__ __forceinline__ void face(const Smem& s, int cl, float* out) {
+    constexpr int st = D == 0 ? 1 : LX;  // along the normal
+    constexpr int tn = D == 0 ? LX : 1;  // along the face
+    const int cr = cl + st;
+    float pl[4], pr[4], wl[4], wr[4], Fc[4], Fv[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float a = s.W[v][cl - st], b = s.W[v][cr + st];
+        pl[v] = s.W[v][cl];
+        pr[v] = s.W[v][cr];
+        const float sl = slope<LIM>(pl[v] - a, pr[v] - pl[v]);
+        const float sr = slope<LIM>(pr[v] - pl[v], b - pr[v]);
+        wl[v] = pl[v] + 0.5f * sl;
+        wr[v] = pr[v] - 0.5f * sr;
+    }
+    hllc<D>(wl, wr, Fc);
+    auto tangential = [&](const float* q) {  // the mean of the two cells' central differences along the face
+        return 0.5f * (0.5f * (q[cl + tn] - q[cl - tn]) + 0.5f * (q[cr + tn] - q[cr - tn]));
+    };
+    visc<D>(pl, pr, s.T[cl], s.T[cr], tangential(s.W[1]), tangential(s.W[2]), tangential(s.T), Fv);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        out[v * stride] = Fc[v];
+        out[(4 + v) * stride] = Fv[v];
     }
 }
 
@@ -163,61 +202,35 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
         const float mu = __ldg(g.U + plane + c) * sg;
         const float mv = __ldg(g.U + 2 * plane + c) * sg;
         const float E = __ldg(g.U + 3 * plane + c);
-        const float u = mu / r, v = mv / r;
+        const float ir = __frcp_rn(r);
+        const float u = mu * ir, v = mv * ir;
         const float p = (kG - 1.0f) * (E - 0.5f * r * (u * u + v * v));
         s.W[0][idx] = r;
         s.W[1][idx] = u;
         s.W[2][idx] = v;
         s.W[3][idx] = p;
-        s.T[idx] = p / r;
+        s.T[idx] = p * ir;
     }
     __syncthreads();
 
-    // 2. every face of the tile's cells, once (tile_gradients, tile_reconstruct, tile_conv_flux, tile_visc_flux):
-    // the limited slopes along the face's direction and the 6 gradients of its two cells, then both fluxes
+    // 2. every face of the tile's cells, once (tile_gradients, tile_reconstruct, tile_conv_flux, tile_visc_flux).
+    // Work items in warp-uniform runs: the 17 rows of y-faces, the 16 rows of x-faces west of each tile cell (a warp
+    // per row, so the reads are conflict-free), then the 16 x-faces on the tile's east edge.
     for (int f = tid; f < NXF + NYF; f += kThreads) {
-        int d, cl, cr;
-        if (f < NXF) {
-            d = 0;
-            const int r = f / (TX + 1), k = f - r * (TX + 1);  // between tile cells (r, k-1) and (r, k)
-            cl = (r + 2) * LX + (k + 1);
-            cr = cl + 1;
+        if (f < NYF) {
+            const int r = f / TX, k = f - r * TX;  // between tile cells (r-1, k) and (r, k)
+            face<LIM, 1, NYF>(s, (r + 1) * LX + (k + 2), &s.FY[0][f]);
         } else {
-            d = 1;
-            const int q = f - NXF;
-            const int r = q / TX, k = q - r * TX;  // between tile cells (r-1, k) and (r, k)
-            cl = (r + 1) * LX + (k + 2);
-            cr = cl + LX;
-        }
-        const int st = d == 0 ? 1 : LX;  // the neighbour along the face's direction
-        float pl[4], pr[4], wl[4], wr[4], gL[6], gR[6], Fc[4], Fv[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            pl[v] = s.W[v][cl];
-            pr[v] = s.W[v][cr];
-            const float sl = slope<LIM>(pl[v] - s.W[v][cl - st], s.W[v][cl + st] - pl[v]);
-            const float sr = slope<LIM>(pr[v] - s.W[v][cr - st], s.W[v][cr + st] - pr[v]);
-            wl[v] = pl[v] + 0.5f * sl;
-            wr[v] = pr[v] - 0.5f * sr;
-        }
-        hllc(wl, wr, d, Fc);
-        auto grads = [&](int c, float (&gq)[6]) {  // ux uy vx vy Tx Ty of cell c
-            gq[0] = 0.5f * (s.W[1][c + 1] - s.W[1][c - 1]);
-            gq[1] = 0.5f * (s.W[1][c + LX] - s.W[1][c - LX]);
-            gq[2] = 0.5f * (s.W[2][c + 1] - s.W[2][c - 1]);
-            gq[3] = 0.5f * (s.W[2][c + LX] - s.W[2][c - LX]);
-            gq[4] = 0.5f * (s.T[c + 1] - s.T[c - 1]);
-            gq[5] = 0.5f * (s.T[c + LX] - s.T[c - LX]);
-        };
-        grads(cl, gL);
-        grads(cr, gR);
-        visc(pl, pr, s.T[cl], s.T[cr], gL, gR, d, Fv);
-        float* out = d == 0 ? &s.FX[0][f] : &s.FY[0][f - NXF];
-        const int stride = d == 0 ? NXF : NYF;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            out[v * stride] = Fc[v];
-            out[(4 + v) * stride] = Fv[v];
+            int r, k;  // between tile cells (r, k-1) and (r, k)
+            const int q = f - NYF;
+            if (q < TY * TX) {
+                r = q / TX;
+                k = q - r * TX;
+            } else {
+                r = q - TY * TX;
+                k = TX;
+            }
+            face<LIM, 0, NXF>(s, (r + 2) * LX + (k + 1), &s.FX[0][r * (TX + 1) + k]);
         }
     }
     __syncthreads();
@@ -242,10 +255,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
             sqd[v] = __fma_rn(double(rv), double(rv), sqd[v]);
         }
         const int c = (r + 2) * LX + (k + 2);
-        const float rho = s.W[0][c], u = s.W[1][c], vv = s.W[2][c], p = s.W[3][c];
-        const float cs = sqrtf(kG * p / rho);
+        const float rho = s.W[0][c], u = s.W[1][c], vv = s.W[2][c];
+        const float cs = sqrtf(kG * s.T[c]);  // T = p / ρ
         const float ax = fabsf(u) + cs, ay = fabsf(vv) + cs;
-        const float nu = kMu / rho * fmx(4.0f / 3.0f, kG / kPr);
+        const float nu = kMu * __frcp_rn(rho) * fmx(4.0f / 3.0f, kG / kPr);
         const float dt = kCfl / (ax + ay + 4.0f * nu);
         const float ws = fmx(ax, ay);
         dtmin = fmn(dtmin, dt);
