@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
     for (int idx = tid; idx < LC; idx += kThreads) {
         const int lb = idx / LX, la = idx - lb * LX;
         const int j = ty0 - 2 + lb, i = tx0 - 2 + la;
-        const int is = wrapi(i, g.nx);
+        const int is = unsigned(i) < unsigned(g.nx) ? i : wrapi(i, g.nx);  // only halo columns wrap
         int js = j;
         float sg = 1.0f;
         if (j < 0 || j >= g.ny) {
