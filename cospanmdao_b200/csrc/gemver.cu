@@ -85,13 +85,19 @@ struct LowRankK {
 
 // STORE: Â is requested (16-bit A only): pass 1 forms and stores it and x comes from its column sums, as k_gemver's;
 // only pass 2 takes the low-rank form (w from A, the rank-2 terms in the finish) instead of forming Â again.
+// 16-bit A without Â: rows per load batch and blocks per SM of the two streaming passes (8 rows, 3 blocks: 24 warps per
+// SM with 128 B per lane in flight)
+template <typename T, bool STORE> inline constexpr int kLrRB = (sizeof(T) == 2 && !STORE) ? 8 : 16;
+template <typename T, bool STORE> inline constexpr int kLrBlocks = (sizeof(T) == 2 && !STORE) ? 3 : 2;
+
 template <typename T, bool STORE>
-__global__ void __launch_bounds__(kPassThreads, 2) k_gemver_lr(LowRankK g, int vec_ok) {
+__global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_lr(LowRankK g, int vec_ok) {
+    constexpr int RB = kLrRB<T, STORE>;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
     for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0);
         if constexpr (STORE) pass_unit<T, kWX, true, true, false, true, false, 0>(g.p1, u, vec_ok != 0, smem);
-        else pass_unit<T, kWX, true, false, false, true, false, 16>(g.p1, u, vec_ok != 0, smem);
+        else pass_unit<T, kWX, true, false, false, true, false, RB>(g.p1, u, vec_ok != 0, smem);
         u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
@@ -105,7 +111,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver_lr(LowRankK g, int v
     if (!grid_barrier(g.ctrl)) return;
     for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-        pass_unit<T, kWX, true, false, false, false, true, 16, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, smem);
+        pass_unit<T, kWX, true, false, false, false, true, RB, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, smem);
         u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
