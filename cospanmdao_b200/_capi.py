@@ -29,6 +29,7 @@ DEV_TIMEOUT = 1
 DEV_NEGATIVE = 2
 DEV_EXCEEDS32 = 4
 DEV_CAPACITY = 8
+DEV_ARGUMENT = 16
 
 F32 = 0
 BF16 = 1
@@ -36,6 +37,7 @@ GEMVER_PANEL = 1
 GEMVER_BULK = 2
 GEMVER_LOWRANK = 4
 BATCH_LOWRANK = 1 << 16
+BATCH_NO_B = 1 << 17
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p

@@ -221,16 +221,19 @@ template <typename T> inline constexpr int kLrRows = sizeof(T) == 4 ? 16 : 8;
 
 // LR: an instance takes the low-rank form of cspb_gemver_fused with CSPB_GEMVER_LOWRANK: without Â, column sums of
 // A·y, then row dots of A·x, the rank-2 terms in the finishes; with Â and a 16-bit A, pass 2 and the w finish only.
-template <typename T, int WX, bool LR>
+// LEAN: the variant for batches without Â (only the low-rank paths are compiled, so it fits 3 blocks per SM).
+template <typename T, int WX, bool LR, bool LEAN>
 __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    if (LR && a.dst == nullptr) pass_unit<T, WX, true, false, false, true, false, kLrRows<T>>(a, unit, vec_ok, smem);
+    if (LEAN || (LR && a.dst == nullptr)) pass_unit<T, WX, true, false, false, true, false, kLrRows<T>>(a, unit, vec_ok, smem);
     else pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(a, unit, vec_ok, smem);
 }
 // Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update
 // (or, low-rank, without it).
-template <typename T, int WX, bool LR>
+template <typename T, int WX, bool LR, bool LEAN>
 __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
-    if (LR && (a.dst == nullptr || sizeof(T) == 2)) {  // low-rank: w from A (also when a 16-bit A's Â is stored)
+    if (LEAN) {  // no Â in the batch: a.dst is NULL
+        pass_unit<T, WX, true, false, false, false, true, kLrRows<T>, true>(a, unit, vec_ok, smem);
+    } else if (LR && (a.dst == nullptr || sizeof(T) == 2)) {  // low-rank: w from A (also when a 16-bit A's Â is stored)
         PassArgs b = a;
         b.dst = nullptr;  // pass 2 only reads A
         pass_unit<T, WX, true, false, false, false, true, kLrRows<T>, true>(b, unit, vec_ok, smem);
@@ -245,8 +248,9 @@ __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_
     }
 }
 
-template <typename T, bool LR>
-__global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
+template <typename T, bool LR, bool LEAN = false>
+__global__ void __launch_bounds__(kThreads, LEAN ? 3 : 2) k_run(RunK g) {
+    static_assert(!LEAN || LR, "the lean variant is the low-rank form");
     constexpr bool bf16 = sizeof(T) == 2;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, 1>() > pass_smem_bytes<T, 4>()
                                                     ? pass_smem_bytes<T, 1>()
@@ -274,7 +278,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
     const uint64_t e1 = U1, e2 = U1 + C1, e3 = 2 * U1 + C1, e4 = 2 * U1 + C1 + S1;
     __shared__ int s_ok;
     int64_t cur = -1;
-    PassArgs a{};
+    // the instance's arguments: in registers, or (lean variant) in shared memory, written by one thread per instance
+    // change, so that they do not hold ~40 registers across the work loop
+    __shared__ PassArgs s_args;
+    PassArgs a_reg{};
+    PassArgs& a = LEAN ? s_args : a_reg;
     bool vec_ok = false;
     const float* z = nullptr;
     float beta = 0.f;
@@ -287,7 +295,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
         wx = g.wx[k];
         ubase = __ldcg(g.off[SU] + k);
         sbase = __ldcg(g.off[SS] + k);
-        a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
+        if constexpr (LEAN) {  // called by the whole block between items (the previous one ended with a barrier)
+            PassArgs t = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
+            if (threadIdx.x == 0) {
+                if (t.dst != nullptr) {  // a task with B under CSPB_BATCH_NO_B: the call fails, no B is written
+                    set_status(g.ctrl, CSPB_DEV_ARGUMENT);
+                    t.dst = nullptr;
+                }
+                s_args = t;
+            }
+            __syncthreads();
+        } else {
+            a = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
+        }
     };
     auto count_done = [&](uint32_t* counter) {  // this block's unit is complete
         __syncthreads();
@@ -313,17 +333,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 const int64_t c = unit % a.chunks, strip = unit / a.chunks;
                 if (!pass2) {
                     switch (wx) {
-                        case 1: unit1<T, 1, LR>(a, unit, vec_ok, smem); break;
-                        case 4: unit1<T, 4, LR>(a, unit, vec_ok, smem); break;
-                        default: unit1<T, 2, LR>(a, unit, vec_ok, smem); break;
+                        case 1: unit1<T, 1, LR, LEAN>(a, unit, vec_ok, smem); break;
+                        case 4: unit1<T, 4, LR, LEAN>(a, unit, vec_ok, smem); break;
+                        default: unit1<T, 2, LR, LEAN>(a, unit, vec_ok, smem); break;
                     }
                     count_done(g.chunk_done + ubase + uint64_t(c));
                 } else {
                     if (!wait_for(g.x_ready + ubase + uint64_t(c), 1u)) { stop = true; break; }
                     switch (wx) {
-                        case 1: unit2<T, 1, LR>(a, unit, vec_ok, smem); break;
-                        case 4: unit2<T, 4, LR>(a, unit, vec_ok, smem); break;
-                        default: unit2<T, 2, LR>(a, unit, vec_ok, smem); break;
+                        case 1: unit2<T, 1, LR, LEAN>(a, unit, vec_ok, smem); break;
+                        case 4: unit2<T, 4, LR, LEAN>(a, unit, vec_ok, smem); break;
+                        default: unit2<T, 2, LR, LEAN>(a, unit, vec_ok, smem); break;
                     }
                     count_done(g.strip_done + sbase + uint64_t(strip));
                 }
@@ -335,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 if (!wait_for(g.chunk_done + ubase + uint64_t(c), uint32_t(a.strips))) { stop = true; break; }
                 const int64_t CW = cols_of(wx, bf16);
                 const int64_t c1 = (c + 1) * CW < a.n ? (c + 1) * CW : a.n;
-                if (LR && a.dst == nullptr) instance_x_lr(a, z, beta, x, c * CW, c1);
+                if (LEAN || (LR && a.dst == nullptr)) instance_x_lr(a, z, beta, x, c * CW, c1);
                 else instance_x(a, z, beta, x, c * CW, c1);
                 __syncthreads();
                 if (threadIdx.x == 0) {
@@ -349,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_run(RunK g) {
                 const int64_t strip = int64_t(f - sbase);
                 if (!wait_for(g.strip_done + sbase + uint64_t(strip), uint32_t(a.chunks))) { stop = true; break; }
                 const int64_t S = rows_of(wx);
-                const bool lr = LR && (a.dst == nullptr || bf16);  // as unit2
+                const bool lr = LEAN || (LR && (a.dst == nullptr || bf16));  // as unit2
                 double t1 = 0.0, t2 = 0.0;
                 if (lr) block_dot2(a.v1, a.v2, a.xv, a.n, t1, t2);  // x is complete: every chunk fed this strip
                 for (int64_t row = strip * S + threadIdx.x; row < (strip + 1) * S && row < a.n; row += blockDim.x) {
@@ -448,7 +468,8 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     if (count < 1 || count > (int64_t(1) << 26) || max_elems < 1 || max_vec < 1) return CSPB_ERR_ARGUMENT;
     if (a_dtype != CSPB_F32 && a_dtype != CSPB_BF16) return CSPB_ERR_UNSUPPORTED;
     const bool lowrank = (tune & CSPB_BATCH_LOWRANK) != 0;
-    tune &= ~CSPB_BATCH_LOWRANK;
+    const bool no_b = (tune & CSPB_BATCH_NO_B) != 0;
+    tune &= ~(CSPB_BATCH_LOWRANK | CSPB_BATCH_NO_B);
     if (tune < 0 || tune >= cspb_gemver_batched_tunings()) return CSPB_ERR_UNSUPPORTED;
     for (uint32_t b = 0; b < 4; ++b)
         if (((uint32_t(tune) >> (2 * b)) & 3u) == 3u) return CSPB_ERR_UNSUPPORTED;
@@ -514,7 +535,10 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     g.x_ready = reinterpret_cast<uint32_t*>(ws + L.off_xr);
     g.cap_units = L.capU;
     g.ctrl = reinterpret_cast<uint32_t*>(ws);
-    const void* kern = bf16 ? (lowrank ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, true>)
+    // without Â anywhere in the batch, a 16-bit low-rank batch runs the lean variant (3 blocks per SM)
+    const bool lean = bf16 && lowrank && (d ? d->B == nullptr : no_b);
+    const void* kern = lean ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, true, true>)
+                     : bf16 ? (lowrank ? reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, true>)
                                        : reinterpret_cast<const void*>(batch::k_run<__nv_bfloat16, false>))
                             : (lowrank ? reinterpret_cast<const void*>(batch::k_run<float, true>)
                                        : reinterpret_cast<const void*>(batch::k_run<float, false>));

@@ -94,6 +94,7 @@ int cspb_read_status(const void* workspace, uint32_t* raw, void* stream) {
     if (word & CSPB_DEV_NEGATIVE) return CSPB_ERR_NEGATIVE;
     if (word & CSPB_DEV_EXCEEDS32) return CSPB_ERR_EXCEEDS32;
     if (word & CSPB_DEV_CAPACITY) return CSPB_ERR_CAPACITY;
+    if (word & CSPB_DEV_ARGUMENT) return CSPB_ERR_ARGUMENT;
     return CSPB_OK;
 }
 

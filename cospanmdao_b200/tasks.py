@@ -59,10 +59,12 @@ class TaskRunner:
         return addr
 
     def gemver(self, table: np.ndarray, *, bf16: bool, tune: int = 0, lowrank: bool | None = None, stream=None,
-               host_staging=None):
+               host_staging=None, no_b: bool | None = None):
         """Runs a GEMVER task table. lowrank: the low-rank form (the rank-2 update as dot products) for tasks without
         B, and for w of bf16 tasks with B; None (the default) follows cb.gemver's 'auto' schedule, so that every task
-        gets the single call's form: low-rank for bf16, not for f32."""
+        gets the single call's form: low-rank for bf16, not for f32. no_b: pass CSPB_BATCH_NO_B (the kernel variant
+        without the Â paths, for a bf16 low-rank table in which no task has B); None (the default) passes it exactly
+        when no task has B. Returns the workspace pointer, whose status word cspb_read_status reads."""
         import cospanmdao_b200 as cb
         torch = _torch()
         count = int(table.size)
@@ -78,6 +80,10 @@ class TaskRunner:
         if lowrank is None:
             lowrank = bf16
         word = int(tune) | (_capi.BATCH_LOWRANK if lowrank else 0)
+        if no_b is None:
+            no_b = bool(lowrank and bf16 and not table["B"].any())
+        if no_b:
+            word |= _capi.BATCH_NO_B  # no task stores Â: the variant without those paths
         st = lib().cspb_gemver_tasks(C.c_void_p(taddr), count, max_elems, max_vec, BF16 if bf16 else F32, word,
                                      C.c_void_p(wp), wb, C.c_void_p(int(s.cuda_stream)))
         cb._raise(st, "gemver tasks")

@@ -45,6 +45,7 @@ enum {
 #define CSPB_DEV_NEGATIVE 2u
 #define CSPB_DEV_EXCEEDS32 4u
 #define CSPB_DEV_CAPACITY 8u
+#define CSPB_DEV_ARGUMENT 16u  /* a task contradicts a flag of the call (CSPB_BATCH_NO_B); read as CSPB_ERR_ARGUMENT */
 
 /* storage dtypes of the big operands (the matrix of a GEMVER, the fields of a stencil) */
 enum { CSPB_F32 = 0, CSPB_BF16 = 1 };
@@ -264,6 +265,12 @@ typedef struct cspb_gemver_task {
  * cspb_gemver_fused with CSPB_GEMVER_LOWRANK (the rank-2 update as dot products in the finishes); instances with B
  * are unchanged. */
 #define CSPB_BATCH_LOWRANK (1 << 16)
+/* tune | CSPB_BATCH_LOWRANK | CSPB_BATCH_NO_B (cspb_gemver_tasks, bf16 A): the caller states that no task has B. The
+ * launch then uses a kernel variant without the paths that form and store Â, at 3 blocks per SM instead of 2; results
+ * are bit-identical. A task with B under this flag sets CSPB_DEV_ARGUMENT: the call fails (its x and w are not valid)
+ * and no B is written. A packed batch (cspb_gemver_batched) with B == NULL and a bf16 A takes that variant without
+ * the flag. */
+#define CSPB_BATCH_NO_B (1 << 17)
 int cspb_gemver_tasks(const cspb_gemver_task* tasks, int64_t count, int64_t max_elems, int64_t max_vec,
                       int32_t a_dtype, int32_t tune, void* workspace, size_t workspace_bytes, void* stream);
 

@@ -28,6 +28,17 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_capi.PROTOTYPES), set(names) - set(_capi.PROTOTYPES)
 
 
+def test_header_flags_match_the_python_view():
+    """Every CSPB_ flag and device status bit the header defines has the same value in the Python view."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    defs = dict(re.findall(r"#define CSPB_([A-Z0-9_]+) \(?([0-9a-fx <u]+?)\)?\s*$", text, flags=re.M))
+    want = {"DEV_TIMEOUT", "DEV_NEGATIVE", "DEV_EXCEEDS32", "DEV_CAPACITY", "DEV_ARGUMENT", "GEMVER_PANEL",
+            "GEMVER_BULK", "GEMVER_LOWRANK", "BATCH_LOWRANK", "BATCH_NO_B"}
+    assert want <= set(defs), want - set(defs)
+    for name in want:
+        assert eval(defs[name].replace("u", "")) == getattr(_capi, name), name
+
+
 def test_version_and_status_strings():
     assert "sm_100a" in cb.version()
     lib = cb.lib()
