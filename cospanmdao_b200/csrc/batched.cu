@@ -217,7 +217,11 @@ __device__ __forceinline__ void instance_x_lr(const PassArgs& a, const float* z,
 
 // rows in flight of the low-rank units (16-bit storage: 8, which keeps every variant of this kernel free of spills;
 // the batching does not change the arithmetic)
-template <typename T> inline constexpr int kLrRows = sizeof(T) == 4 ? 16 : 8;
+template <typename T> inline constexpr int kLrRows = 8;
+
+// Blocks per SM of a k_run variant: 3 for f32 and for the lean variant (80 registers, the instance's arguments in
+// shared memory, 8-row load batches), 2 for the 16-bit variants that also form Â (128 registers).
+template <typename T, bool LEAN> inline constexpr int kRunBlocks = (sizeof(T) == 4 || LEAN) ? 3 : 2;
 
 // LR: an instance takes the low-rank form of cspb_gemver_fused with CSPB_GEMVER_LOWRANK: without Â, column sums of
 // A·y, then row dots of A·x, the rank-2 terms in the finishes; with Â and a 16-bit A, pass 2 and the w finish only.
@@ -225,7 +229,7 @@ template <typename T> inline constexpr int kLrRows = sizeof(T) == 4 ? 16 : 8;
 template <typename T, int WX, bool LR, bool LEAN>
 __device__ __forceinline__ void unit1(const PassArgs& a, int64_t unit, bool vec_ok, unsigned char* smem) {
     if (LEAN || (LR && a.dst == nullptr)) pass_unit<T, WX, true, false, false, true, false, kLrRows<T>>(a, unit, vec_ok, smem);
-    else pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 16 : 0>(a, unit, vec_ok, smem);
+    else pass_unit<T, WX, true, true, false, true, false, sizeof(T) == 4 ? 8 : 0>(a, unit, vec_ok, smem);
 }
 // Pass 2 reads the stored Â (f32) when there is one and the matrix is f32; otherwise A again, re-applying the update
 // (or, low-rank, without it).
@@ -242,14 +246,14 @@ __device__ __forceinline__ void unit2(const PassArgs& a, int64_t unit, bool vec_
         b.src = a.dst;
         b.lds = a.ldd;
         b.dst = nullptr;  // pass 2 only reads Â
-        pass_unit<float, WX, false, false, false, false, true, 16, true>(b, unit, vec_ok, smem);
+        pass_unit<float, WX, false, false, false, false, true, 8, true>(b, unit, vec_ok, smem);
     } else {
         pass_unit<T, WX, true, true, false, false, true, 0, true>(a, unit, vec_ok, smem);
     }
 }
 
 template <typename T, bool LR, bool LEAN = false>
-__global__ void __launch_bounds__(kThreads, LEAN ? 3 : 2) k_run(RunK g) {
+__global__ void __launch_bounds__(kThreads, (kRunBlocks<T, LEAN>)) k_run(RunK g) {
     static_assert(!LEAN || LR, "the lean variant is the low-rank form");
     constexpr bool bf16 = sizeof(T) == 2;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, 1>() > pass_smem_bytes<T, 4>()
@@ -278,11 +282,12 @@ __global__ void __launch_bounds__(kThreads, LEAN ? 3 : 2) k_run(RunK g) {
     const uint64_t e1 = U1, e2 = U1 + C1, e3 = 2 * U1 + C1, e4 = 2 * U1 + C1 + S1;
     __shared__ int s_ok;
     int64_t cur = -1;
-    // the instance's arguments: in registers, or (lean variant) in shared memory, written by one thread per instance
-    // change, so that they do not hold ~40 registers across the work loop
+    // the instance's arguments: in shared memory for the 3-block variants, written by one thread per instance change,
+    // so that they do not hold ~40 registers across the work loop; in registers otherwise
+    constexpr bool kSharedArgs = kRunBlocks<T, LEAN> == 3;
     __shared__ PassArgs s_args;
     PassArgs a_reg{};
-    PassArgs& a = LEAN ? s_args : a_reg;
+    PassArgs& a = kSharedArgs ? s_args : a_reg;
     bool vec_ok = false;
     const float* z = nullptr;
     float beta = 0.f;
@@ -295,10 +300,10 @@ __global__ void __launch_bounds__(kThreads, LEAN ? 3 : 2) k_run(RunK g) {
         wx = g.wx[k];
         ubase = __ldcg(g.off[SU] + k);
         sbase = __ldcg(g.off[SS] + k);
-        if constexpr (LEAN) {  // called by the whole block between items (the previous one ended with a barrier)
+        if constexpr (kSharedArgs) {  // called by the whole block between items (the previous one ended with a barrier)
             PassArgs t = instance_args<T>(g, k, wx, bf16, vec_ok, z, beta, x);
             if (threadIdx.x == 0) {
-                if (t.dst != nullptr) {  // a task with B under CSPB_BATCH_NO_B: the call fails, no B is written
+                if (LEAN && t.dst != nullptr) {  // a task with B under CSPB_BATCH_NO_B: the call fails, no B is written
                     set_status(g.ctrl, CSPB_DEV_ARGUMENT);
                     t.dst = nullptr;
                 }
