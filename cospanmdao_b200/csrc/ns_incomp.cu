@@ -10,8 +10,9 @@
 // No reference code computes this residual (the reference's ns-residual is the compressible one, ns_comp.cu); the
 // formula is the workload's definition, and the oracle is an f64 restatement of it.
 //
-// Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. f32 fields that are 16-byte aligned with nx % 4 == 0 take
-// the block-tile path (nsi_tile below). Otherwise (bf16 storage, or unaligned / ragged rows) the register path:
+// Layout: u, v, p and r_u, r_v, r_c are (ny, nx) row-major. 16-byte aligned fields whose rows are whole 16-byte
+// chunks (nx % 4 == 0 in f32, nx % 8 == 0 in bf16) take the block-tile path (nsi_tile below). Otherwise (unaligned or
+// ragged rows) the register path:
 // work item = one warp on a strip of 32·VEC columns × H rows:
 // each lane owns 4 consecutive cells of a row (one 16-byte f32 / 8-byte bf16 load per field per row), x-neighbours come from the
 // adjacent lanes by shuffle (the warp's edge lanes load one wrapped scalar), and the warp marches down its rows
@@ -92,22 +93,29 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
     right = need_r ? row.r : from_right;
 }
 
-// ---- f32 by block tiles (cp.async) -------------------------------------------------------------------------------
+// ---- block tiles (cp.async) -------------------------------------------------------------------------------------
 // A block computes one tile of kNsiTileCols × kNsiTileRows cells. It first copies the tile's rows of u, v, p with the
 // rows above and below it and the two wrapped halo columns into shared memory (cp.async: each warp takes every 8th
-// row, each lane its 16-byte cells, lane 0 and the last active lane the halo cells), waits once, then computes its
-// rows from shared memory and stores the residuals. Four such blocks per SM keep whole tiles (3 × 34 rows × 512 B
-// each) in flight while other blocks compute. Measured on B200 at 4096²: 82 µs against 136 µs for a per-warp ring of
-// 4 row slots (one row in flight per warp), with bit-identical residuals; taller tiles (48, 64 rows: 2-3 blocks per
-// SM) ran 91-94 µs. A tile row is [3] the cell left of the tile, [4 .. 4+128) its cells, [4 + cols] the cell right.
+// row, each lane a 16-byte chunk of it, then lane 0 and the last active lane the halo cells), waits once, then
+// computes its rows from shared memory and stores the residuals. Four such blocks per SM keep whole tiles in flight
+// while other blocks compute. Measured on B200 at 4096² (f32): 82 µs against 136 µs for a per-warp ring of 4 row
+// slots (one row in flight per warp), with bit-identical residuals; taller tiles (48, 64 rows: 2-3 blocks per SM) ran
+// 91-94 µs. The fields stay in their storage type in shared memory (bf16 is widened as it is read). A tile row is
+// [c0 - 1] the cell left of the tile, [c0 .. c0 + 128) its cells, [c0 + cols] the cell right, c0 = 16 B / sizeof(T).
 constexpr int kNsiTileCols = 128;
 constexpr int kNsiTileRows = 32;
-constexpr int kNsiPitch = 136;  // floats per tile row
-constexpr size_t kNsiTileBytes = size_t(3) * (kNsiTileRows + 2) * kNsiPitch * sizeof(float);
+template <typename T> inline constexpr int kNsiCell0 = 16 / int(sizeof(T));                 // 4 f32, 8 bf16
+template <typename T> inline constexpr int kNsiPitch = kNsiCell0<T> + kNsiTileCols + kNsiCell0<T>;  // 136, 144
+template <typename T>
+inline constexpr size_t kNsiTileBytes = size_t(3) * (kNsiTileRows + 2) * kNsiPitch<T> * sizeof(T);
 
 __host__ __device__ inline int64_t nsi_tiles(int nx, int ny) {
     return int64_t((nx + kNsiTileCols - 1) / kNsiTileCols) * ((ny + kNsiTileRows - 1) / kNsiTileRows);
 }
+// The tile path takes 16-byte aligned fields (checked by the caller) whose rows are whole 16-byte chunks: nx % 4 == 0
+// in f32, nx % 8 == 0 in bf16. Single calls and task tables use this same rule, so a grid's decomposition (and hence
+// its norms' bits) does not depend on how it was launched.
+__host__ __device__ inline bool nsi_tile_rows(bool bf16, int nx) { return nx % (bf16 ? 8 : 4) == 0; }
 
 __device__ __forceinline__ uint32_t nsi_smem(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
 __device__ __forceinline__ void nsi_cp16(void* dst, const void* src) {
@@ -116,87 +124,126 @@ __device__ __forceinline__ void nsi_cp16(void* dst, const void* src) {
 __device__ __forceinline__ void nsi_cp4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(nsi_smem(dst)), "l"(src) : "memory");
 }
+// 4 consecutive cells of a tile row in shared memory (16-byte aligned in f32, 8-byte in bf16), widened to f32
+template <typename T>
+__device__ __forceinline__ void nsi_ld4(const T* p, float (&c)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        c[0] = q.x; c[1] = q.y; c[2] = q.z; c[3] = q.w;
+    } else {
+        const uint2 q = *reinterpret_cast<const uint2*>(p);
+        c[0] = bf16_lo(q.x); c[1] = bf16_hi(q.x); c[2] = bf16_lo(q.y); c[3] = bf16_hi(q.y);
+    }
+}
+template <typename T>
+__device__ __forceinline__ float nsi_ld1(const T* p) {
+    if constexpr (sizeof(T) == 4) return *p;
+    else return __bfloat162float(*p);
+}
 
-// Tile b of an f32 residual with nx % 4 == 0 and 16-byte aligned fields. The residuals are the register path's,
-// operation for operation; each lane's 4 squares are summed in f32 before one f64 addition per norm.
-__device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, float* buf, double& su, double& sv, double& sc) {
-    constexpr int kField = (kNsiTileRows + 2) * kNsiPitch;  // floats between the fields
+// Tile b of a residual whose rows satisfy nsi_tile_rows. The residuals are the register path's, operation for
+// operation; each lane's 4 squares are summed in f32 before one f64 addition per norm.
+template <typename T>
+__device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, double& su, double& sv, double& sc) {
+    constexpr int C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>;
+    constexpr int VC = 16 / int(sizeof(T));                  // cells per 16-byte copy
+    constexpr int kField = (kNsiTileRows + 2) * PITCH;       // elements between the fields
     const int tilesx = (g.nx + kNsiTileCols - 1) / kNsiTileCols;
     const int x0 = int(b % tilesx) * kNsiTileCols, y0 = int(b / tilesx) * kNsiTileRows;
-    const int scols = g.nx - x0 >= kNsiTileCols ? kNsiTileCols : g.nx - x0;  // a multiple of 4
+    const int scols = g.nx - x0 >= kNsiTileCols ? kNsiTileCols : g.nx - x0;  // a multiple of VC
     const int th = g.ny - y0 >= kNsiTileRows ? kNsiTileRows : g.ny - y0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool active = lane * 4 < scols;
-    const bool last = active && (lane + 1) * 4 >= scols;
-    const int c0 = x0 + lane * 4;
     const int lcol = x0 == 0 ? g.nx - 1 : x0 - 1;
     const int rcol = (x0 + scols) % g.nx;
     const int64_t nx = g.nx;
-    const float* U = static_cast<const float*>(g.u);
-    const float* V = static_cast<const float*>(g.v);
-    const float* P = static_cast<const float*>(g.p);
-    // tile row r holds grid row y0 - 1 + r (wrapped), r = 0 .. th + 1
-    for (int r = warp; r < th + 2; r += kNsiWarps) {
+    const T* U = static_cast<const T*>(g.u);
+    const T* V = static_cast<const T*>(g.v);
+    const T* P = static_cast<const T*>(g.p);
+    // tile row r holds grid row y0 - 1 + r (wrapped, or a slab's halo row), r = 0 .. th + 1
+    auto row_src = [&](int r, const T*& ru_, const T*& rv_, const T*& rp_) {
         int gy = y0 - 1 + r;
-        const float *ru_, *rv_, *rp_;  // the row's start in each field
-        if (g.slab && gy < 0) {
-            ru_ = g.up[0]; rv_ = g.up[1]; rp_ = g.up[2];
-        } else if (g.slab && gy >= g.ny) {
-            ru_ = g.dn[0]; rv_ = g.dn[1]; rp_ = g.dn[2];
-        } else {
-            gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
-            const int64_t ro = int64_t(gy) * nx;
-            ru_ = U + ro; rv_ = V + ro; rp_ = P + ro;
+        if constexpr (sizeof(T) == 4) {  // slabs are f32
+            if (g.slab && gy < 0) {
+                ru_ = g.up[0]; rv_ = g.up[1]; rp_ = g.up[2];
+                return;
+            }
+            if (g.slab && gy >= g.ny) {
+                ru_ = g.dn[0]; rv_ = g.dn[1]; rp_ = g.dn[2];
+                return;
+            }
         }
-        float* row = buf + r * kNsiPitch;
-        if (active) {
-            nsi_cp16(row + 4 + lane * 4, ru_ + c0);
-            nsi_cp16(row + kField + 4 + lane * 4, rv_ + c0);
-            nsi_cp16(row + 2 * kField + 4 + lane * 4, rp_ + c0);
+        gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
+        const int64_t ro = int64_t(gy) * nx;
+        ru_ = U + ro; rv_ = V + ro; rp_ = P + ro;
+    };
+    const int cc = lane * VC;  // this lane's chunk of the row (f32: 32 lanes × 4 cells; bf16: 16 lanes × 8)
+    for (int r = warp; r < th + 2; r += kNsiWarps) {
+        const T *ru_, *rv_, *rp_;
+        row_src(r, ru_, rv_, rp_);
+        T* row = buf + r * PITCH;
+        if (cc < scols) {
+            nsi_cp16(row + C0 + cc, ru_ + x0 + cc);
+            nsi_cp16(row + kField + C0 + cc, rv_ + x0 + cc);
+            nsi_cp16(row + 2 * kField + C0 + cc, rp_ + x0 + cc);
         }
-        if (lane == 0) {
-            nsi_cp4(row + 3, ru_ + lcol);
-            nsi_cp4(row + kField + 3, rv_ + lcol);
-            nsi_cp4(row + 2 * kField + 3, rp_ + lcol);
-        }
-        if (last) {
-            nsi_cp4(row + 4 + scols, ru_ + rcol);
-            nsi_cp4(row + kField + 4 + scols, rv_ + rcol);
-            nsi_cp4(row + 2 * kField + 4 + scols, rp_ + rcol);
+        if constexpr (sizeof(T) == 4) {
+            if (lane == 0) {
+                nsi_cp4(row + C0 - 1, ru_ + lcol);
+                nsi_cp4(row + kField + C0 - 1, rv_ + lcol);
+                nsi_cp4(row + 2 * kField + C0 - 1, rp_ + lcol);
+            }
+            if (cc < scols && cc + VC >= scols) {
+                nsi_cp4(row + C0 + scols, ru_ + rcol);
+                nsi_cp4(row + kField + C0 + scols, rv_ + rcol);
+                nsi_cp4(row + 2 * kField + C0 + scols, rp_ + rcol);
+            }
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
+    if constexpr (sizeof(T) == 2) {
+        // 2-byte halo cells are below cp.async's 4-byte minimum: plain loads, issued after all the row copies, by
+        // lanes 0-5 of each warp (lane = 2·field + side) for the warp's rows
+        if (lane < 6) {
+            const int f = lane >> 1, side = lane & 1;
+            const int64_t col = side ? rcol : lcol;
+            const int at = f * kField + (side ? C0 + scols : C0 - 1);
+            for (int r = warp; r < th + 2; r += kNsiWarps) {
+                const T *ru_, *rv_, *rp_;
+                row_src(r, ru_, rv_, rp_);
+                const T* src = f == 0 ? ru_ : (f == 1 ? rv_ : rp_);
+                buf[r * PITCH + at] = src[col];
+            }
+        }
+    }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
+    const bool active = lane * 4 < scols;
     if (active) {
+        const int c0 = x0 + lane * 4;
         const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
-        const float* const mine = buf + 4 + lane * 4;
+        const T* const mine = buf + C0 + lane * 4;
         for (int j = warp; j < th; j += kNsiWarps) {
-            const float* a = mine + (j + 1) * kNsiPitch;
-            const float* mS = mine + j * kNsiPitch;
-            const float* mN = mine + (j + 2) * kNsiPitch;
+            const T* a = mine + (j + 1) * PITCH;
+            const T* mS = mine + j * PITCH;
+            const T* mN = mine + (j + 2) * PITCH;
             float cu[6], cv[6], cp[6];  // W, 4 cells, E of the row
             float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
             {
-                const float4 ua = *reinterpret_cast<const float4*>(a);
-                const float4 va = *reinterpret_cast<const float4*>(a + kField);
-                const float4 pa = *reinterpret_cast<const float4*>(a + 2 * kField);
-                cu[0] = a[-1]; cu[1] = ua.x; cu[2] = ua.y; cu[3] = ua.z; cu[4] = ua.w; cu[5] = a[4];
-                cv[0] = a[kField - 1]; cv[1] = va.x; cv[2] = va.y; cv[3] = va.z; cv[4] = va.w; cv[5] = a[kField + 4];
-                cp[0] = a[2 * kField - 1]; cp[1] = pa.x; cp[2] = pa.y; cp[3] = pa.z; cp[4] = pa.w;
-                cp[5] = a[2 * kField + 4];
-                const float4 us = *reinterpret_cast<const float4*>(mS);
-                const float4 un = *reinterpret_cast<const float4*>(mN);
-                const float4 vs = *reinterpret_cast<const float4*>(mS + kField);
-                const float4 vn = *reinterpret_cast<const float4*>(mN + kField);
-                const float4 ps = *reinterpret_cast<const float4*>(mS + 2 * kField);
-                const float4 pn = *reinterpret_cast<const float4*>(mN + 2 * kField);
-                uS[0] = us.x; uS[1] = us.y; uS[2] = us.z; uS[3] = us.w;
-                uN[0] = un.x; uN[1] = un.y; uN[2] = un.z; uN[3] = un.w;
-                vS[0] = vs.x; vS[1] = vs.y; vS[2] = vs.z; vS[3] = vs.w;
-                vN[0] = vn.x; vN[1] = vn.y; vN[2] = vn.z; vN[3] = vn.w;
-                pS[0] = ps.x; pS[1] = ps.y; pS[2] = ps.z; pS[3] = ps.w;
-                pN[0] = pn.x; pN[1] = pn.y; pN[2] = pn.z; pN[3] = pn.w;
+                float ua[4], va[4], pa[4];
+                nsi_ld4(a, ua);
+                nsi_ld4(a + kField, va);
+                nsi_ld4(a + 2 * kField, pa);
+                cu[0] = nsi_ld1(a - 1); cu[5] = nsi_ld1(a + 4);
+                cv[0] = nsi_ld1(a + kField - 1); cv[5] = nsi_ld1(a + kField + 4);
+                cp[0] = nsi_ld1(a + 2 * kField - 1); cp[5] = nsi_ld1(a + 2 * kField + 4);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) { cu[e + 1] = ua[e]; cv[e + 1] = va[e]; cp[e + 1] = pa[e]; }
+                nsi_ld4(mS, uS);
+                nsi_ld4(mN, uN);
+                nsi_ld4(mS + kField, vS);
+                nsi_ld4(mN + kField, vN);
+                nsi_ld4(mS + 2 * kField, pS);
+                nsi_ld4(mN + 2 * kField, pN);
             }
             float oru[4], orv[4], orc[4];
             float qu = 0.f, qv = 0.f, qc = 0.f;
@@ -280,10 +327,11 @@ __device__ __forceinline__ void nsi_norms(const NsiK& g, int64_t b, int64_t nblo
     __syncthreads();  // the shared memory of this block is reused by the next block of a persistent caller
 }
 
-// Tile b (of nblocks) of an f32 residual, with its norms.
-__device__ __forceinline__ void nsi_tile_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done, float* buf) {
+// Tile b (of nblocks) of a residual, with its norms.
+template <typename T>
+__device__ __forceinline__ void nsi_tile_block(const NsiK& g, int64_t b, int64_t nblocks, uint32_t* done, T* buf) {
     double su = 0.0, sv = 0.0, sc = 0.0;
-    nsi_tile(g, b, buf, su, sv, sc);
+    nsi_tile<T>(g, b, buf, su, sv, sc);
     nsi_norms(g, b, nblocks, done, su, sv, sc);
 }
 
@@ -386,10 +434,11 @@ template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
     nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
 }
-// The f32 tile path: one block per tile, 4 blocks per SM (64 registers a thread at most).
+// The tile path: one block per tile, 4 blocks per SM (64 registers a thread at most).
+template <typename T>
 __global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_tile(NsiK g) {
-    extern __shared__ __align__(16) float nsi_buf[];
-    nsi_tile_block(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, nsi_buf);
+    extern __shared__ __align__(16) unsigned char nsi_raw[];
+    nsi_tile_block<T>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, reinterpret_cast<T*>(nsi_raw));
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
@@ -439,7 +488,7 @@ __global__ void k_nsi_plan(NsiTasksK g) {
             const bool fast = nsi_fast(t, 4);
             int H, segs;
             int64_t items, blocks;
-            if (fast && !g.bf16) blocks = nsi_tiles(t.nx, t.ny);  // the f32 tile path
+            if (fast && nsi_tile_rows(g.bf16 != 0, t.nx)) blocks = nsi_tiles(t.nx, t.ny);  // the tile path
             else nsi_shape(t.nx, t.ny, fast ? 4 : 1, H, segs, items, blocks);
             nb = uint64_t(blocks);
         } else {
@@ -449,11 +498,10 @@ __global__ void k_nsi_plan(NsiTasksK g) {
     }
 }
 
-// MINB: blocks per SM the registers must allow (f32: 4, so that its tiles run 4 blocks per SM as in the single
-// call; bf16: 2, its register path's 128 registers)
+// MINB: blocks per SM the registers must allow (4, so that tiles run 4 blocks per SM as in the single call)
 template <typename T, int MINB>
 __global__ void __launch_bounds__(kNsiThreads, MINB) k_nsi_tasks(NsiTasksK g) {
-    extern __shared__ __align__(16) float nsi_buf[];
+    extern __shared__ __align__(16) unsigned char nsi_raw[];
     __shared__ int s_go;
     if (threadIdx.x == 0) s_go = __ldcg(g.boff + g.count) <= g.cap_blocks && !status_bad(g.ctrl);
     __syncthreads();
@@ -490,7 +538,7 @@ __global__ void __launch_bounds__(kNsiThreads, MINB) k_nsi_tasks(NsiTasksK g) {
         const bool fast = nsi_fast(t, vfast);
         NsiK k{};
         int64_t blocks;
-        const bool tile = fast && sizeof(T) == 4;
+        const bool tile = fast && nsi_tile_rows(sizeof(T) == 2, t.nx);
         if (tile) blocks = nsi_tiles(t.nx, t.ny);
         else nsi_shape(t.nx, t.ny, fast ? vfast : 1, k.H, k.segs, k.items, blocks);
         k.nx = t.nx;
@@ -505,7 +553,7 @@ __global__ void __launch_bounds__(kNsiThreads, MINB) k_nsi_tasks(NsiTasksK g) {
         k.ctrl = g.ctrl;
         const int64_t b = int64_t(v) - int64_t(__ldcg(g.boff + lo));
         if (tile) {
-            nsi_tile_block(k, b, blocks, g.done + lo, nsi_buf);
+            nsi_tile_block<T>(k, b, blocks, g.done + lo, reinterpret_cast<T*>(nsi_raw));
         } else if constexpr (sizeof(T) == 2) {  // f32 fast tasks are tiles
             if (fast) nsi_block<T, vfast>(k, b, blocks, g.done + lo);
             else nsi_block<T, 1>(k, b, blocks, g.done + lo);
@@ -524,9 +572,9 @@ using cspb_host::aligned;
 
 namespace {
 
-// A tile needs more than the default 48 KB of dynamic shared memory per block.
-bool tile_ready(const void* kern) {
-    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kNsiTileBytes)) == cudaSuccess;
+// An f32 tile needs more than the default 48 KB of dynamic shared memory per block.
+bool tile_ready(const void* kern, size_t bytes) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)) == cudaSuccess;
 }
 
 struct NsiPlan {
@@ -593,7 +641,7 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     const bool out_al = aligned(d->ru, 16) && aligned(d->rv, 16) && aligned(d->rc, 16);
     const bool fast = in_al && out_al && d->nx % vfast == 0;
     NsiPlan P = nsi_plan(d->nx, d->ny, fast ? vfast : 1);
-    const bool tile = fast && !bf16;
+    const bool tile = fast && nsi_tile_rows(bf16, d->nx);
     if (tile) {
         P.blocks = nsi_tiles(d->nx, d->ny);
         P.ws = align_up(kCtrlBytes + size_t(P.blocks) * 3 * sizeof(double), 256);
@@ -616,12 +664,17 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     g.ctrl = static_cast<uint32_t*>(d->workspace);
     g.part = reinterpret_cast<double*>(static_cast<char*>(d->workspace) + kCtrlBytes);
     const dim3 grid(unsigned(P.blocks)), block(kNsiThreads);
-    if (bf16) {
+    if (tile && bf16) {
+        const size_t bytes = kNsiTileBytes<__nv_bfloat16>;
+        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<__nv_bfloat16>), bytes)) return CSPB_ERR_LAUNCH;
+        k_ns_incomp_tile<__nv_bfloat16><<<grid, block, bytes, st>>>(g);
+    } else if (bf16) {
         if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
-    } else if (fast) {
-        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile))) return CSPB_ERR_LAUNCH;
-        k_ns_incomp_tile<<<grid, block, kNsiTileBytes, st>>>(g);
+    } else if (tile) {
+        const size_t bytes = kNsiTileBytes<float>;
+        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), bytes)) return CSPB_ERR_LAUNCH;
+        k_ns_incomp_tile<float><<<grid, block, bytes, st>>>(g);
     } else {
         k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
@@ -663,10 +716,10 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
     const int r = cspb_exclusive_scan_u64(g.blocks, g.boff, count, ws + L.off_scan, cspb_scan_workspace_bytes(count),
                                           stream);
     if (r != CSPB_OK) return r;
-    const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16, 2>)
+    const void* kern = g.bf16 ? reinterpret_cast<const void*>(k_nsi_tasks<__nv_bfloat16, 4>)
                               : reinterpret_cast<const void*>(k_nsi_tasks<float, 4>);
-    const size_t smem = g.bf16 ? 0 : kNsiTileBytes;
-    if (smem && !tile_ready(kern)) return CSPB_ERR_LAUNCH;
+    const size_t smem = g.bf16 ? kNsiTileBytes<__nv_bfloat16> : kNsiTileBytes<float>;
+    if (!tile_ready(kern, smem)) return CSPB_ERR_LAUNCH;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kNsiThreads, smem) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;
@@ -714,8 +767,8 @@ int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
         g.dn[f] = d->dn[f];
     }
     g.slab = 1;
-    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile))) return CSPB_ERR_LAUNCH;
-    k_ns_incomp_tile<<<dim3(unsigned(nsi_tiles(d->nx, d->rows))), dim3(kNsiThreads), kNsiTileBytes, st>>>(g);
+    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), kNsiTileBytes<float>)) return CSPB_ERR_LAUNCH;
+    k_ns_incomp_tile<float><<<dim3(unsigned(nsi_tiles(d->nx, d->rows))), dim3(kNsiThreads), kNsiTileBytes<float>, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
