@@ -280,8 +280,12 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
 #pragma unroll
     for (int k = 0; k < 32; ++k) racc[k] = 0.f;
 
+    // the arguments the row loop uses, in registers: `a` may live in shared memory (a persistent caller's cached
+    // instance), which the loop's own shared-memory stores would otherwise make the compiler read again
     const LT* src = static_cast<const LT*>(a.src);
-    const bool store = a.dst != nullptr;
+    const int64_t lds = a.lds, ldd = a.ldd;
+    float* const dst = a.dst;
+    const bool store = dst != nullptr;
     float* rdot = reinterpret_cast<float*>(smem) + size_t(warp) * 32 * 32;  // rolled loop: [row][lane] of the warp
 
     auto batch = [&](int kb) {
@@ -289,7 +293,7 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
             uint4 raw[RB];
 #pragma unroll
             for (int k = 0; k < RB; ++k)
-                raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<LT, NC>(src + (r0 + kb + k) * a.lds, c0, ncols, vec_ok)
+                raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<LT, NC>(src + (r0 + kb + k) * lds, c0, ncols, vec_ok)
                                                        : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
             for (int k = 0; k < RB; ++k) {
@@ -306,7 +310,7 @@ __device__ __forceinline__ void pass_unit(const PassArgs& a, int64_t unit, bool 
                     for (int e = 0; e < VEC; ++e)
                         b[e] = RANK2 ? __fadd_rn(__fadd_rn(val[e], __fmul_rn(u1k, v1c[e])), __fmul_rn(u2k, v2c[e]))
                                      : val[e];
-                    if (store && ncols > 0) store_vec<VEC>(a.dst + (r0 + kk) * a.ldd, c0, ncols, vec_ok, b);
+                    if (store && ncols > 0) store_vec<VEC>(dst + (r0 + kk) * ldd, c0, ncols, vec_ok, b);
                     if constexpr (kF32Part<LT>) {
                         // 16-bit storage: 8 products of a column in f32, then into the f64 sum (one conversion per 8 rows)
                         const bool flush = (kk & 7) == 7 || kk == nrows - 1;
