@@ -11,6 +11,7 @@
 //            (examples/gemver-chain/components.hpp:85-265, :366-470)             → cspb_gemver_fused
 //   BiCGK    BicgkOnePass → RowReduce → ColReduce<false>   (components.hpp:277-358) → cspb_bicgk_fused
 //            Gemv → GemvTPartial → ColReduce<false>        (the unfused / parallel / fused BiCGK)
+//   chain    GEMVER → BiCGK → GEMVER wired as the Chain system (systems.hpp:214-266) → cspb_gemver_chain
 //   NS       the 19 stages of NsFused or the 18 components of NsUnfused (examples/ns-residual/systems.hpp:31-140,
 //            components.hpp:100-852), either limiter and boundary  → cspb_ns_compressible, whose 18 diagnostics
 //            are then copied into the Dt, Ws, Sq, Det and Err variables
@@ -151,7 +152,13 @@ inline bool scale_is_input(Runtime& rt, int v) {
 }
 
 // ---- GEMVER --------------------------------------------------------------------------------------------------------
-inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+struct GemverMatch {
+    ComponentBase *r2u, *gtp, *cred, *gemv;
+    int vB, vP, vbeta, valpha;
+};
+
+// comps[a .. a + 4) by type and wiring (the leaf boundaries and escaping partials are checked by the caller)
+inline bool match_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a, GemverMatch& m) {
     if (a + 4 > L.comps.size()) return false;
     ComponentBase *r2u = L.comps[a], *gtp = L.comps[a + 1], *cred = L.comps[a + 2], *gemv = L.comps[a + 3];
     const std::string t0 = short_type(r2u), t1 = short_type(gtp);
@@ -164,62 +171,89 @@ inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
     if (has_port(gtp, "B") && var_id(rt, gtp, "B") != vB) return false;  // the local variant takes B from its tile
     const int vbeta = var_id(rt, cred, "scale"), valpha = var_id(rt, gemv, "scale");
     if (!scale_is_input(rt, vbeta) || !scale_is_input(rt, valpha)) return false;
+    m = GemverMatch{r2u, gtp, cred, gemv, vB, vP, vbeta, valpha};
+    return true;
+}
+
+// cspb_gemver_fused over a matched run, with its scales β and α
+inline void launch_gemver(Runtime& rt, FastState& st, const GemverMatch& g, std::int64_t n, float beta, float alpha) {
+    cspb_gemver_desc d{};
+    d.n = n;
+    d.lda = n;
+    d.ldb = n;
+    d.a_dtype = CSPB_F32;
+    d.A = rt.var_of_port(g.r2u, "A").data;
+    d.u1 = static_cast<const float*>(rt.var_of_port(g.r2u, "u1").data);
+    d.v1 = static_cast<const float*>(rt.var_of_port(g.r2u, "v1").data);
+    d.u2 = static_cast<const float*>(rt.var_of_port(g.r2u, "u2").data);
+    d.v2 = static_cast<const float*>(rt.var_of_port(g.r2u, "v2").data);
+    d.y = static_cast<const float*>(rt.var_of_port(g.gtp, "y").data);
+    d.z = static_cast<const float*>(rt.var_of_port(g.cred, "z").data);
+    d.beta = beta;
+    d.alpha = alpha;
+    d.B = static_cast<float*>(rt.var_of_port(g.r2u, "B").data);
+    d.x = static_cast<float*>(rt.var_of_port(g.cred, "x").data);
+    d.w = static_cast<float*>(rt.var_of_port(g.gemv, "y").data);
+    d.workspace_bytes = cspb_gemver_workspace_bytes(n);
+    d.workspace = st.workspace(rt, d.workspace_bytes);
+    if (rt.trace)
+        std::fprintf(stderr, "[cospan] fast path cspb_gemver_fused n=%lld for '%s' .. '%s'\n", (long long)n,
+                     g.r2u->path().c_str(), g.gemv->path().c_str());
+    fast_fail(cspb_gemver_fused(&d, rt.stream), "'" + g.r2u->path() + "' (GEMVER fast path)");
+}
+
+// the square matrix a GEMVER run reads (0: not square)
+inline std::int64_t gemver_n(Runtime& rt, const GemverMatch& g) {
+    Var& A = rt.var_of_port(g.r2u, "A");
+    return (A.rank == 2 && A.shape[0] == A.shape[1]) ? std::int64_t(A.shape[0]) : 0;
+}
+
+inline void claim(Runtime& rt, int pat, std::size_t lo, std::size_t hi) {
+    rt.pattern_hi.push_back(hi);
+    rt.pattern_at[lo] = pat;
+    for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+}
+
+inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    GemverMatch g;
+    if (!match_gemver(rt, L, a, g)) return false;
     std::size_t lo, hi;
     if (!whole_leaves(L, a, 4, lo, hi)) return false;
-    if (internal_escapes(rt, {r2u, gtp, cred, gemv}, {vP})) return false;
+    if (internal_escapes(rt, {g.r2u, g.gtp, g.cred, g.gemv}, {g.vP})) return false;
 
     auto st = std::make_shared<FastState>();
-    st->internal = {vP};
-    st->scale_vars = {vbeta, valpha};
+    st->internal = {g.vP};
+    st->scale_vars = {g.vbeta, g.valpha};
     st->scale_version = {~0ull, ~0ull};
     st->scale = {0.f, 0.f};
     rt.pattern_state.push_back(st);
     const int pat = int(rt.pattern_runs.size());
-    rt.pattern_runs.push_back([st, r2u, gtp, cred, gemv](Runtime& rt, std::size_t&) {
+    rt.pattern_runs.push_back([st, g](Runtime& rt, std::size_t&) {
         if (!st->partials_unviewed(rt)) return false;
-        for (ComponentBase* c : {r2u, gtp, cred, gemv}) rt.prepare(c);
-        Var& A = rt.var_of_port(r2u, "A");
-        if (A.rank != 2 || A.shape[0] != A.shape[1]) return false;
-        const std::int64_t n = std::int64_t(A.shape[0]);
+        for (ComponentBase* c : {g.r2u, g.gtp, g.cred, g.gemv}) rt.prepare(c);
+        const std::int64_t n = gemver_n(rt, g);
+        if (n == 0) return false;
         st->refresh(rt);
-        cspb_gemver_desc d{};
-        d.n = n;
-        d.lda = n;
-        d.ldb = n;
-        d.a_dtype = CSPB_F32;
-        d.A = A.data;
-        d.u1 = static_cast<const float*>(rt.var_of_port(r2u, "u1").data);
-        d.v1 = static_cast<const float*>(rt.var_of_port(r2u, "v1").data);
-        d.u2 = static_cast<const float*>(rt.var_of_port(r2u, "u2").data);
-        d.v2 = static_cast<const float*>(rt.var_of_port(r2u, "v2").data);
-        d.y = static_cast<const float*>(rt.var_of_port(gtp, "y").data);
-        d.z = static_cast<const float*>(rt.var_of_port(cred, "z").data);
-        d.beta = st->scale[0];
-        d.alpha = st->scale[1];
-        d.B = static_cast<float*>(rt.var_of_port(r2u, "B").data);
-        d.x = static_cast<float*>(rt.var_of_port(cred, "x").data);
-        d.w = static_cast<float*>(rt.var_of_port(gemv, "y").data);
-        d.workspace_bytes = cspb_gemver_workspace_bytes(n);
-        d.workspace = st->workspace(rt, d.workspace_bytes);
-        if (rt.trace)
-            std::fprintf(stderr, "[cospan] fast path cspb_gemver_fused n=%lld for '%s' .. '%s'\n", (long long)n,
-                         r2u->path().c_str(), gemv->path().c_str());
-        fast_fail(cspb_gemver_fused(&d, rt.stream), "'" + r2u->path() + "' (GEMVER fast path)");
+        launch_gemver(rt, *st, g, n, st->scale[0], st->scale[1]);
         return true;
     });
-    rt.pattern_hi.push_back(hi);
-    rt.pattern_at[lo] = pat;
-    for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+    claim(rt, pat, lo, hi);
     return true;
 }
 
 // ---- BiCGK ---------------------------------------------------------------------------------------------------------
-inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+struct BicgkMatch {
+    ComponentBase *c0, *c1, *c2;
+    int vB, vp, vr, vq, vs, vscale_s, vscale_q;  // vscale_q: -1 for the one-pass form (no scale on q)
+    std::vector<int> internal;
+};
+
+inline bool match_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a, BicgkMatch& m) {
     if (a + 3 > L.comps.size()) return false;
     ComponentBase *c0 = L.comps[a], *c1 = L.comps[a + 1], *c2 = L.comps[a + 2];
     if (short_type(c2) != "ColReduce<false>") return false;
     const std::string t0 = short_type(c0), t1 = short_type(c1);
-    int vB, vp, vr, vq, vs, vscale_q = -1;
+    int vB, vp, vr, vq, vscale_q = -1;
     std::vector<int> internal;
     if (t0 == "BicgkOnePass" && t1 == "RowReduce") {
         vB = var_id(rt, c0, "B");
@@ -240,53 +274,144 @@ inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
     } else {
         return false;
     }
-    vs = var_id(rt, c2, "x");
+    const int vs = var_id(rt, c2, "x");
     const int vscale_s = var_id(rt, c2, "scale");
     if (vB < 0 || vp < 0 || vr < 0 || vq < 0 || vs < 0 || !scale_is_input(rt, vscale_s)) return false;
+    m = BicgkMatch{c0, c1, c2, vB, vp, vr, vq, vs, vscale_s, vscale_q, internal};
+    return true;
+}
+
+// the BiCGK run's scale variables, s's first
+inline std::vector<int> bicgk_scales(const BicgkMatch& m) {
+    std::vector<int> v{m.vscale_s};
+    if (m.vscale_q >= 0) v.push_back(m.vscale_q);
+    return v;
+}
+
+inline void launch_bicgk(Runtime& rt, FastState& st, const BicgkMatch& m, std::int64_t n) {
+    cspb_bicgk_desc d{};
+    d.n = n;
+    d.ldb = n;
+    d.b_dtype = CSPB_F32;
+    d.B = rt.vars[std::size_t(m.vB)].data;
+    d.p = static_cast<const float*>(rt.vars[std::size_t(m.vp)].data);
+    d.r = static_cast<const float*>(rt.vars[std::size_t(m.vr)].data);
+    d.q = static_cast<float*>(rt.vars[std::size_t(m.vq)].data);
+    d.s = static_cast<float*>(rt.vars[std::size_t(m.vs)].data);
+    d.workspace_bytes = cspb_bicgk_workspace_bytes(n);
+    d.workspace = st.workspace(rt, d.workspace_bytes);
+    if (rt.trace)
+        std::fprintf(stderr, "[cospan] fast path cspb_bicgk_fused n=%lld for '%s' .. '%s'\n", (long long)n,
+                     m.c0->path().c_str(), m.c2->path().c_str());
+    fast_fail(cspb_bicgk_fused(&d, rt.stream), "'" + m.c0->path() + "' (BiCGK fast path)");
+}
+
+inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    BicgkMatch m;
+    if (!match_bicgk(rt, L, a, m)) return false;
     std::size_t lo, hi;
     if (!whole_leaves(L, a, 3, lo, hi)) return false;
-    if (internal_escapes(rt, {c0, c1, c2}, internal)) return false;
+    if (internal_escapes(rt, {m.c0, m.c1, m.c2}, m.internal)) return false;
 
     auto st = std::make_shared<FastState>();
-    st->internal = internal;
-    st->scale_vars = {vscale_s};
-    if (vscale_q >= 0) st->scale_vars.push_back(vscale_q);
+    st->internal = m.internal;
+    st->scale_vars = bicgk_scales(m);
     st->scale_version.assign(st->scale_vars.size(), ~0ull);
     st->scale.assign(st->scale_vars.size(), 0.f);
     rt.pattern_state.push_back(st);
     const int pat = int(rt.pattern_runs.size());
-    rt.pattern_runs.push_back([st, c0, c1, c2, vB, vp, vr, vq, vs](Runtime& rt, std::size_t&) {
+    rt.pattern_runs.push_back([st, m](Runtime& rt, std::size_t&) {
         if (!st->partials_unviewed(rt)) return false;
-        for (ComponentBase* c : {c0, c1, c2}) rt.prepare(c);
+        for (ComponentBase* c : {m.c0, m.c1, m.c2}) rt.prepare(c);
         st->refresh(rt);
         for (float s : st->scale)
             if (s != 1.0f) return false;  // the kernel forms q = B·p and s = Bᵀ·r unscaled
-        Var& B = rt.vars[std::size_t(vB)];
+        Var& B = rt.vars[std::size_t(m.vB)];
         if (B.rank != 2 || B.shape[0] != B.shape[1]) return false;
-        const std::int64_t n = std::int64_t(B.shape[0]);
-        cspb_bicgk_desc d{};
-        d.n = n;
-        d.ldb = n;
-        d.b_dtype = CSPB_F32;
-        d.B = B.data;
-        d.p = static_cast<const float*>(rt.vars[std::size_t(vp)].data);
-        d.r = static_cast<const float*>(rt.vars[std::size_t(vr)].data);
-        d.q = static_cast<float*>(rt.vars[std::size_t(vq)].data);
-        d.s = static_cast<float*>(rt.vars[std::size_t(vs)].data);
-        d.workspace_bytes = cspb_bicgk_workspace_bytes(n);
-        d.workspace = st->workspace(rt, d.workspace_bytes);
-        if (rt.trace)
-            std::fprintf(stderr, "[cospan] fast path cspb_bicgk_fused n=%lld for '%s' .. '%s'\n", (long long)n,
-                         c0->path().c_str(), c2->path().c_str());
-        fast_fail(cspb_bicgk_fused(&d, rt.stream), "'" + c0->path() + "' (BiCGK fast path)");
+        launch_bicgk(rt, *st, m, std::int64_t(B.shape[0]));
         return true;
     });
-    rt.pattern_hi.push_back(hi);
-    rt.pattern_at[lo] = pat;
-    for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+    claim(rt, pat, lo, hi);
     return true;
 }
 
+// ---- the gemver chain ----------------------------------------------------------------------------------------------
+// A GEMVER run, a BiCGK run and a GEMVER run, wired as the reference's Chain system (systems.hpp:214-266): BiCGK's B,
+// p, r are G1's B, x, w, and G2's A, y, z are G1's B and BiCGK's q, s. cspb_gemver_chain does the three in six matrix
+// passes (two launches) instead of the single kernels' eight. It takes one α and one β for both GEMVERs, as the
+// reference's chain ties them; if G1's and G2's scales differ at run time, the fast path runs the three single
+// kernels instead.
+inline bool try_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    GemverMatch g1, g2;
+    BicgkMatch bk;
+    if (!match_gemver(rt, L, a, g1) || !match_bicgk(rt, L, a + 4, bk) || !match_gemver(rt, L, a + 7, g2)) return false;
+    if (bk.vB != g1.vB || bk.vp != var_id(rt, g1.cred, "x") || bk.vr != var_id(rt, g1.gemv, "y")) return false;
+    if (var_id(rt, g2.r2u, "A") != g1.vB || var_id(rt, g2.gtp, "y") != bk.vq || var_id(rt, g2.cred, "z") != bk.vs)
+        return false;
+    std::size_t lo, hi;
+    if (!whole_leaves(L, a, 11, lo, hi)) return false;
+    std::vector<int> internal = bk.internal;
+    internal.push_back(g1.vP);
+    internal.push_back(g2.vP);
+    if (internal_escapes(rt, {g1.r2u, g1.gtp, g1.cred, g1.gemv, bk.c0, bk.c1, bk.c2, g2.r2u, g2.gtp, g2.cred, g2.gemv},
+                         internal))
+        return false;
+
+    auto st = std::make_shared<FastState>();
+    st->internal = internal;
+    st->scale_vars = {g1.vbeta, g1.valpha, g2.vbeta, g2.valpha};  // then BiCGK's
+    for (int v : bicgk_scales(bk)) st->scale_vars.push_back(v);
+    st->scale_version.assign(st->scale_vars.size(), ~0ull);
+    st->scale.assign(st->scale_vars.size(), 0.f);
+    rt.pattern_state.push_back(st);
+    const int pat = int(rt.pattern_runs.size());
+    rt.pattern_runs.push_back([st, g1, bk, g2](Runtime& rt, std::size_t&) {
+        if (!st->partials_unviewed(rt)) return false;
+        for (ComponentBase* c : {g1.r2u, g1.gtp, g1.cred, g1.gemv, bk.c0, bk.c1, bk.c2, g2.r2u, g2.gtp, g2.cred, g2.gemv})
+            rt.prepare(c);
+        const std::int64_t n = gemver_n(rt, g1);
+        if (n == 0) return false;
+        st->refresh(rt);
+        for (std::size_t k = 4; k < st->scale.size(); ++k)
+            if (st->scale[k] != 1.0f) return false;  // BiCGK forms q = B·p and s = Bᵀ·r unscaled
+        const float beta1 = st->scale[0], alpha1 = st->scale[1], beta2 = st->scale[2], alpha2 = st->scale[3];
+        if (beta1 != beta2 || alpha1 != alpha2) {
+            // one workspace size for the three (no reallocation between them)
+            st->workspace(rt, std::max(cspb_gemver_workspace_bytes(n), cspb_bicgk_workspace_bytes(n)));
+            launch_gemver(rt, *st, g1, n, beta1, alpha1);
+            launch_bicgk(rt, *st, bk, n);
+            launch_gemver(rt, *st, g2, n, beta2, alpha2);
+            return true;
+        }
+        auto f = [&](ComponentBase* c, const char* port) { return static_cast<float*>(rt.var_of_port(c, port).data); };
+        cspb_chain_desc d{};
+        d.n = n;
+        d.A0 = f(g1.r2u, "A");
+        d.u1a = f(g1.r2u, "u1"); d.v1a = f(g1.r2u, "v1"); d.u2a = f(g1.r2u, "u2"); d.v2a = f(g1.r2u, "v2");
+        d.ya = f(g1.gtp, "y");
+        d.za = f(g1.cred, "z");
+        d.u1b = f(g2.r2u, "u1"); d.v1b = f(g2.r2u, "v1"); d.u2b = f(g2.r2u, "u2"); d.v2b = f(g2.r2u, "v2");
+        d.alpha = alpha1;
+        d.beta = beta1;
+        d.B1 = f(g1.r2u, "B");
+        d.x1 = f(g1.cred, "x");
+        d.w1 = f(g1.gemv, "y");
+        d.q = static_cast<float*>(rt.vars[std::size_t(bk.vq)].data);
+        d.s = static_cast<float*>(rt.vars[std::size_t(bk.vs)].data);
+        d.B2 = f(g2.r2u, "B");
+        d.x2 = f(g2.cred, "x");
+        d.w2 = f(g2.gemv, "y");
+        d.workspace_bytes = cspb_chain_workspace_bytes(n);
+        d.workspace = st->workspace(rt, d.workspace_bytes);
+        if (rt.trace)
+            std::fprintf(stderr, "[cospan] fast path cspb_gemver_chain n=%lld for '%s' .. '%s'\n", (long long)n,
+                         g1.r2u->path().c_str(), g2.gemv->path().c_str());
+        fast_fail(cspb_gemver_chain(&d, rt.stream), "'" + g1.r2u->path() + "' (gemver chain fast path)");
+        return true;
+    });
+    claim(rt, pat, lo, hi);
+    return true;
+}
 
 // ---- NS residual (compressible) ------------------------------------------------------------------------------------
 // A stage's role: its type with the limiter / boundary argument dropped ("Reconstruct<nsr::MinMod>" -> "Reconstruct<>").
@@ -416,7 +541,8 @@ inline void register_patterns(Runtime& rt) {
             ++a;
             continue;
         }
-        if (try_gemver(rt, L, a)) a += 4;
+        if (try_chain(rt, L, a)) a += 11;
+        else if (try_gemver(rt, L, a)) a += 4;
         else if (try_bicgk(rt, L, a)) a += 3;
         else if (try_ns(rt, L, a)) a = L.first[std::size_t(rt.pattern_hi.back()) + 1];
         else ++a;
