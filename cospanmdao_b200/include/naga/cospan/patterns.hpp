@@ -11,7 +11,8 @@
 //            (examples/gemver-chain/components.hpp:85-265, :366-470)             → cspb_gemver_fused
 //   BiCGK    BicgkOnePass → RowReduce → ColReduce<false>   (components.hpp:277-358) → cspb_bicgk_fused
 //            Gemv → GemvTPartial → ColReduce<false>        (the unfused / parallel / fused BiCGK)
-//   chain    GEMVER → BiCGK → GEMVER wired as the Chain system (systems.hpp:214-266) → cspb_gemver_chain
+//   chain    GEMVER → BiCGK → GEMVER wired as the Chain system (systems.hpp:214-266), or the crafted chain's three
+//            groups (systems.hpp:269-330)                                          → cspb_gemver_chain
 //   NS       the 19 stages of NsFused or the 18 components of NsUnfused (examples/ns-residual/systems.hpp:31-140,
 //            components.hpp:100-852), either limiter and boundary  → cspb_ns_compressible, whose 18 diagnostics
 //            are then copied into the Dt, Ws, Sq, Det and Err variables
@@ -336,6 +337,51 @@ inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
 }
 
 // ---- the gemver chain ----------------------------------------------------------------------------------------------
+// The variables cspb_gemver_chain reads and writes, by id (their device pointers are taken at run time).
+struct ChainVars {
+    int A0, u1a, v1a, u2a, v2a, ya, za, u1b, v1b, u2b, v2b, B1, x1, w1, q, s, B2, x2, w2;
+    bool valid() const {
+        for (int v : {A0, u1a, v1a, u2a, v2a, ya, za, u1b, v1b, u2b, v2b, B1, x1, w1, q, s, B2, x2, w2})
+            if (v < 0) return false;
+        return true;
+    }
+};
+
+inline void launch_chain(Runtime& rt, FastState& st, const ChainVars& c, std::int64_t n, float alpha, float beta,
+                         const ComponentBase* first, const ComponentBase* last) {
+    auto f = [&](int v) { return static_cast<float*>(rt.vars[std::size_t(v)].data); };
+    cspb_chain_desc d{};
+    d.n = n;
+    d.A0 = f(c.A0);
+    d.u1a = f(c.u1a); d.v1a = f(c.v1a); d.u2a = f(c.u2a); d.v2a = f(c.v2a);
+    d.ya = f(c.ya);
+    d.za = f(c.za);
+    d.u1b = f(c.u1b); d.v1b = f(c.v1b); d.u2b = f(c.u2b); d.v2b = f(c.v2b);
+    d.alpha = alpha;
+    d.beta = beta;
+    d.B1 = f(c.B1); d.x1 = f(c.x1); d.w1 = f(c.w1);
+    d.q = f(c.q); d.s = f(c.s);
+    d.B2 = f(c.B2); d.x2 = f(c.x2); d.w2 = f(c.w2);
+    d.workspace_bytes = cspb_chain_workspace_bytes(n);
+    d.workspace = st.workspace(rt, d.workspace_bytes);
+    if (rt.trace)
+        std::fprintf(stderr, "[cospan] fast path cspb_gemver_chain n=%lld for '%s' .. '%s'\n", (long long)n,
+                     first->path().c_str(), last->path().c_str());
+    fast_fail(cspb_gemver_chain(&d, rt.stream), "'" + first->path() + "' (gemver chain fast path)");
+}
+
+// G1's side of the chain's variables (a matched GEMVER run)
+inline void chain_g1_vars(Runtime& rt, const GemverMatch& g1, ChainVars& c) {
+    c.A0 = var_id(rt, g1.r2u, "A");
+    c.u1a = var_id(rt, g1.r2u, "u1"); c.v1a = var_id(rt, g1.r2u, "v1");
+    c.u2a = var_id(rt, g1.r2u, "u2"); c.v2a = var_id(rt, g1.r2u, "v2");
+    c.ya = var_id(rt, g1.gtp, "y");
+    c.za = var_id(rt, g1.cred, "z");
+    c.B1 = g1.vB;
+    c.x1 = var_id(rt, g1.cred, "x");
+    c.w1 = var_id(rt, g1.gemv, "y");
+}
+
 // A GEMVER run, a BiCGK run and a GEMVER run, wired as the reference's Chain system (systems.hpp:214-266): BiCGK's B,
 // p, r are G1's B, x, w, and G2's A, y, z are G1's B and BiCGK's q, s. cspb_gemver_chain does the three in six matrix
 // passes (two launches) instead of the single kernels' eight. It takes one α and one β for both GEMVERs, as the
@@ -348,6 +394,16 @@ inline bool try_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
     if (bk.vB != g1.vB || bk.vp != var_id(rt, g1.cred, "x") || bk.vr != var_id(rt, g1.gemv, "y")) return false;
     if (var_id(rt, g2.r2u, "A") != g1.vB || var_id(rt, g2.gtp, "y") != bk.vq || var_id(rt, g2.cred, "z") != bk.vs)
         return false;
+    ChainVars cv;
+    chain_g1_vars(rt, g1, cv);
+    cv.u1b = var_id(rt, g2.r2u, "u1"); cv.v1b = var_id(rt, g2.r2u, "v1");
+    cv.u2b = var_id(rt, g2.r2u, "u2"); cv.v2b = var_id(rt, g2.r2u, "v2");
+    cv.q = bk.vq;
+    cv.s = bk.vs;
+    cv.B2 = g2.vB;
+    cv.x2 = var_id(rt, g2.cred, "x");
+    cv.w2 = var_id(rt, g2.gemv, "y");
+    if (!cv.valid()) return false;
     std::size_t lo, hi;
     if (!whole_leaves(L, a, 11, lo, hi)) return false;
     std::vector<int> internal = bk.internal;
@@ -365,7 +421,7 @@ inline bool try_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
     st->scale.assign(st->scale_vars.size(), 0.f);
     rt.pattern_state.push_back(st);
     const int pat = int(rt.pattern_runs.size());
-    rt.pattern_runs.push_back([st, g1, bk, g2](Runtime& rt, std::size_t&) {
+    rt.pattern_runs.push_back([st, g1, bk, g2, cv](Runtime& rt, std::size_t&) {
         if (!st->partials_unviewed(rt)) return false;
         for (ComponentBase* c : {g1.r2u, g1.gtp, g1.cred, g1.gemv, bk.c0, bk.c1, bk.c2, g2.r2u, g2.gtp, g2.cred, g2.gemv})
             rt.prepare(c);
@@ -383,30 +439,68 @@ inline bool try_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
             launch_gemver(rt, *st, g2, n, beta2, alpha2);
             return true;
         }
-        auto f = [&](ComponentBase* c, const char* port) { return static_cast<float*>(rt.var_of_port(c, port).data); };
-        cspb_chain_desc d{};
-        d.n = n;
-        d.A0 = f(g1.r2u, "A");
-        d.u1a = f(g1.r2u, "u1"); d.v1a = f(g1.r2u, "v1"); d.u2a = f(g1.r2u, "u2"); d.v2a = f(g1.r2u, "v2");
-        d.ya = f(g1.gtp, "y");
-        d.za = f(g1.cred, "z");
-        d.u1b = f(g2.r2u, "u1"); d.v1b = f(g2.r2u, "v1"); d.u2b = f(g2.r2u, "u2"); d.v2b = f(g2.r2u, "v2");
-        d.alpha = alpha1;
-        d.beta = beta1;
-        d.B1 = f(g1.r2u, "B");
-        d.x1 = f(g1.cred, "x");
-        d.w1 = f(g1.gemv, "y");
-        d.q = static_cast<float*>(rt.vars[std::size_t(bk.vq)].data);
-        d.s = static_cast<float*>(rt.vars[std::size_t(bk.vs)].data);
-        d.B2 = f(g2.r2u, "B");
-        d.x2 = f(g2.cred, "x");
-        d.w2 = f(g2.gemv, "y");
-        d.workspace_bytes = cspb_chain_workspace_bytes(n);
-        d.workspace = st->workspace(rt, d.workspace_bytes);
-        if (rt.trace)
-            std::fprintf(stderr, "[cospan] fast path cspb_gemver_chain n=%lld for '%s' .. '%s'\n", (long long)n,
-                         g1.r2u->path().c_str(), g2.gemv->path().c_str());
-        fast_fail(cspb_gemver_chain(&d, rt.stream), "'" + g1.r2u->path() + "' (gemver chain fast path)");
+        launch_chain(rt, *st, cv, n, alpha1, beta1, g1.r2u, g2.gemv);
+        return true;
+    });
+    claim(rt, pat, lo, hi);
+    return true;
+}
+
+// The crafted chain (systems.hpp:269-330): G1 as a GEMVER run; a middle group in which BicgkTileLocal reads each B1
+// tile once for q's and s's partials and Rank2UpdateFromLocal forms B2 from the same tile, then RowReduce → q and
+// ColReduce<false> → s; and G2 without its update (GemvTPartial → ColReduce<true> → Gemv over B2). The same six-pass
+// kernel computes it. The middle group's scale on s must be 1 and both GEMVERs' scales equal; otherwise the run keeps
+// its own bodies.
+inline bool try_crafted_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
+    GemverMatch g1;
+    if (a + 11 > L.comps.size() || !match_gemver(rt, L, a, g1)) return false;
+    ComponentBase *bk = L.comps[a + 4], *r2u = L.comps[a + 5], *rowred = L.comps[a + 6], *creds = L.comps[a + 7];
+    ComponentBase *gtp = L.comps[a + 8], *cred = L.comps[a + 9], *gemv = L.comps[a + 10];
+    if (short_type(bk) != "BicgkTileLocal" || short_type(r2u) != "Rank2UpdateFromLocal" ||
+        short_type(rowred) != "RowReduce" || short_type(creds) != "ColReduce<false>" ||
+        short_type(gtp) != "GemvTPartial" || short_type(cred) != "ColReduce<true>" || short_type(gemv) != "Gemv")
+        return false;
+    if (L.leaf_of[a + 5] != L.leaf_of[a + 4]) return false;  // the update reads the tile BicgkTileLocal loaded
+    const int vPq = var_id(rt, bk, "Pq"), vPs = var_id(rt, bk, "Ps"), vP2 = var_id(rt, gtp, "P");
+    ChainVars cv;
+    chain_g1_vars(rt, g1, cv);
+    if (var_id(rt, bk, "B") != g1.vB || var_id(rt, bk, "p") != cv.x1 || var_id(rt, bk, "r") != cv.w1) return false;
+    if (var_id(rt, rowred, "Pq") != vPq || var_id(rt, creds, "P") != vPs) return false;
+    cv.u1b = var_id(rt, r2u, "u1"); cv.v1b = var_id(rt, r2u, "v1");
+    cv.u2b = var_id(rt, r2u, "u2"); cv.v2b = var_id(rt, r2u, "v2");
+    cv.q = var_id(rt, rowred, "q");
+    cv.s = var_id(rt, creds, "x");
+    cv.B2 = var_id(rt, r2u, "B");
+    cv.x2 = var_id(rt, cred, "x");
+    cv.w2 = var_id(rt, gemv, "y");
+    if (!cv.valid()) return false;
+    if (var_id(rt, gtp, "B") != cv.B2 || var_id(rt, gtp, "y") != cv.q || var_id(rt, cred, "P") != vP2 ||
+        var_id(rt, cred, "z") != cv.s || var_id(rt, gemv, "B") != cv.B2 || var_id(rt, gemv, "x") != cv.x2)
+        return false;
+    const int vscale_s = var_id(rt, creds, "scale"), vbeta2 = var_id(rt, cred, "scale"), valpha2 = var_id(rt, gemv, "scale");
+    if (!scale_is_input(rt, vscale_s) || !scale_is_input(rt, vbeta2) || !scale_is_input(rt, valpha2)) return false;
+    std::size_t lo, hi;
+    if (!whole_leaves(L, a, 11, lo, hi)) return false;
+    const std::vector<ComponentBase*> run{g1.r2u, g1.gtp, g1.cred, g1.gemv, bk, r2u, rowred, creds, gtp, cred, gemv};
+    const std::vector<int> internal{g1.vP, vPq, vPs, vP2};
+    if (internal_escapes(rt, run, internal)) return false;
+
+    auto st = std::make_shared<FastState>();
+    st->internal = internal;
+    st->scale_vars = {g1.vbeta, g1.valpha, vbeta2, valpha2, vscale_s};
+    st->scale_version.assign(st->scale_vars.size(), ~0ull);
+    st->scale.assign(st->scale_vars.size(), 0.f);
+    rt.pattern_state.push_back(st);
+    const int pat = int(rt.pattern_runs.size());
+    rt.pattern_runs.push_back([st, g1, run, cv](Runtime& rt, std::size_t&) {
+        if (!st->partials_unviewed(rt)) return false;
+        for (ComponentBase* c : run) rt.prepare(c);
+        const std::int64_t n = gemver_n(rt, g1);
+        if (n == 0) return false;
+        st->refresh(rt);
+        const float beta1 = st->scale[0], alpha1 = st->scale[1], beta2 = st->scale[2], alpha2 = st->scale[3];
+        if (st->scale[4] != 1.0f || beta1 != beta2 || alpha1 != alpha2) return false;
+        launch_chain(rt, *st, cv, n, alpha1, beta1, run.front(), run.back());
         return true;
     });
     claim(rt, pat, lo, hi);
@@ -541,7 +635,7 @@ inline void register_patterns(Runtime& rt) {
             ++a;
             continue;
         }
-        if (try_chain(rt, L, a)) a += 11;
+        if (try_chain(rt, L, a) || try_crafted_chain(rt, L, a)) a += 11;
         else if (try_gemver(rt, L, a)) a += 4;
         else if (try_bicgk(rt, L, a)) a += 3;
         else if (try_ns(rt, L, a)) a = L.first[std::size_t(rt.pattern_hi.back()) + 1];
