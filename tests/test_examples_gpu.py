@@ -23,7 +23,7 @@ def _run(args, timeout=300, env=None):
     return r.returncode, r.stdout
 
 
-# "fast": the runtime's registered fast paths (patterns.hpp) run the GEMVER and BiCGK stages as cspb kernels;
+# "fast": the runtime's registered fast paths (patterns.hpp) run the whole gemver chain as one cspb kernel;
 # "generic": every component runs its own body (NAGA_COSPAN_GENERIC); "eager": the fast paths with no CUDA-graph
 # replay of steady forwards (NAGA_COSPAN_NO_GRAPH)
 MODES = {"fast": {}, "generic": {"NAGA_COSPAN_GENERIC": "1"}, "eager": {"NAGA_COSPAN_NO_GRAPH": "1"}}
