@@ -61,19 +61,24 @@ __device__ __forceinline__ float slope(float a, float b) {
 constexpr float kInvGm1 = 1.0f / (kG - 1.0f);
 
 // HLLC with Davis speeds; D = 0 normal x, D = 1 normal y; L / R primitives (ρ, u, v, p). The divisions by ρ of a side
-// are products with its reciprocal (one correctly rounded reciprocal per side), p / (γ - 1) a product with 1 / (γ - 1).
+// are products with its reciprocal, p / (γ - 1) a product with 1 / (γ - 1). The face's reciprocals, square roots and
+// divisions use the hardware's approximate forms (__fdividef, rsqrtf: about 2 ulp): at 4096² they took the kernel
+// from 0.709 to 0.657 ms, and the residual's relative L2 error against the f64 oracle from 4.4e-6 to 4.7e-6 (the f32
+// storage of U dominates it; the reference's bound is 1e-4). The per-cell phases, and so the diagnostics, keep the
+// correctly rounded forms.
 template <int D>
 __device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], float (&F)[4]) {
     const float rl = L[0], rr = R[0], pl = L[3], pr = R[3];
     const float unl = L[1 + D], utl = L[2 - D];
     const float unr = R[1 + D], utr = R[2 - D];
-    const float irl = __frcp_rn(rl), irr = __frcp_rn(rr);
-    const float cl = sqrtf(kG * pl * irl), cr = sqrtf(kG * pr * irr);
+    const float irl = __fdividef(1.0f, rl), irr = __fdividef(1.0f, rr);
+    const float gl = kG * pl * irl, gr = kG * pr * irr;
+    const float cl = gl > 0.0f ? gl * rsqrtf(gl) : 0.0f, cr = gr > 0.0f ? gr * rsqrtf(gr) : 0.0f;
     const float El = pl * kInvGm1 + 0.5f * rl * (unl * unl + utl * utl);
     const float Er = pr * kInvGm1 + 0.5f * rr * (unr * unr + utr * utr);
     const float sl = fmn(unl - cl, unr - cr);
     const float sr = fmx(unl + cl, unr + cr);
-    const float sm = (pr - pl + rl * unl * (sl - unl) - rr * unr * (sr - unr)) / (rl * (sl - unl) - rr * (sr - unr));
+    const float sm = __fdividef(pr - pl + rl * unl * (sl - unl) - rr * unr * (sr - unr), rl * (sl - unl) - rr * (sr - unr));
     float f0, f1, f2, f3;
     if (sl >= 0.0f) {
         f0 = rl * unl; f1 = rl * unl * unl + pl; f2 = rl * unl * utl; f3 = (El + pl) * unl;
@@ -84,8 +89,8 @@ __device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], f
         const float r = left ? rl : rr, un = left ? unl : unr, ut = left ? utl : utr, p = left ? pl : pr;
         const float E = left ? El : Er, s = left ? sl : sr, ir = left ? irl : irr;
         const float a = s - un;
-        const float k = r * a / (s - sm);
-        const float Es = k * (E * ir + (sm - un) * (sm + p * ir / a));
+        const float k = __fdividef(r * a, s - sm);
+        const float Es = k * (E * ir + (sm - un) * (sm + __fdividef(p * ir, a)));
         f0 = r * un + s * (k - r);
         f1 = r * un * un + p + s * (k * sm - r * un);
         f2 = r * un * ut + s * (k * ut - r * ut);
