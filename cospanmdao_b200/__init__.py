@@ -364,6 +364,8 @@ def build_column(src, *, offsets_mode: bool = False, workspace: Workspace | None
     if st != _capi.OK:
         _raise(st, f"shape hook '{path}'")
     total, flag = (int(v) & 0xffffffff for v in tf.cpu().tolist())
+    if flag & _capi.COLUMN_TIMEOUT:
+        raise RuntimeError(f"shape hook '{path}': the device scan's bounded wait gave up; the offsets are not valid")
     if flag & 1:
         raise ValueError(f"naga::cospan: shape hook: '{path}' holds a negative or invalid count or offset")
     if flag & 2:

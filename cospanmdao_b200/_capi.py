@@ -31,6 +31,11 @@ DEV_EXCEEDS32 = 4
 DEV_CAPACITY = 8
 DEV_ARGUMENT = 16
 
+# the flag word of a ragged-column build (total_flag[1])
+COLUMN_NEGATIVE = 1
+COLUMN_EXCEEDS32 = 2
+COLUMN_TIMEOUT = 4
+
 F32 = 0
 BF16 = 1
 GEMVER_PANEL = 1

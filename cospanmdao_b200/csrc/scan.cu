@@ -14,8 +14,6 @@
 // kernel: the narrowing of the source values (negative -> flag 1, past 32 bits -> flag 2) happens as the tile loads,
 // the running sum is carried in 64 bits so that a total past 2^32 - 1 is known exactly (the reference detects the same
 // thing as a decrease of the wrapped u32 offsets), and the last tile writes [total, flag].
-#include <mutex>
-
 #include "common.cuh"
 
 namespace cspb {
@@ -168,6 +166,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
                         if (status_bad(g.ctrl)) give_up = 1;
                         else if (globaltimer_ns() - t0 > kWaitBudgetNs) {
                             set_status(g.ctrl, CSPB_DEV_TIMEOUT);
+                            // a column build also reports it beside its other flags: a caller without the
+                            // workspace (cspb_build_column_static) has no other way to see it
+                            if (g.total_flag) atomicOr(g.total_flag + 1, CSPB_COLUMN_TIMEOUT);
                             give_up = 1;
                         }
                     }
@@ -421,21 +422,15 @@ static_assert(kStaticScratchBytes <= 160 * 1024 + 256, "the fixed scratch stays 
 
 static __device__ __align__(256) unsigned char g_column_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// The device address of g_column_scratch on the current device, looked up once per device.
+// The device address of g_column_scratch in the current device's context. The name is only a host-side stand-in, so
+// the address is asked for on every call rather than cached: after a cudaDeviceReset (or under another context) a
+// cached address would point at memory that no longer exists. The first call with a device current loads this
+// library's device image on that device, which is why it belongs before any stream capture; later lookups are a
+// table read.
 int column_scratch(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CSPB_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_column_scratch) != cudaSuccess || !p) return CSPB_ERR_CUDA;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_column_scratch) != cudaSuccess || !p) return CSPB_ERR_CUDA;
+    *out = p;
     return CSPB_OK;
 }
 }  // namespace

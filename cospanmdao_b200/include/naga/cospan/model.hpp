@@ -319,6 +319,9 @@ public:
         if (rc != 0) throw std::runtime_error("naga::cospan: " + who + ": cspb_build_column: " + cspb_status_string(rc));
         cuda_check(cudaStreamSynchronize(stream), who);
         const std::uint32_t total = c.tf[0], flag = c.tf[1];
+        if (flag & CSPB_COLUMN_TIMEOUT)
+            throw std::runtime_error("naga::cospan: " + who + ": '" + path + "': the device scan's bounded wait gave up "
+                                     "(" + std::string(cspb_status_string(CSPB_ERR_TIMEOUT)) + ")");
         if ((flag & 1u) == 0 && (flag & 2u) != 0)
             throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds a value or a total past 2^32 - 1; "
                                         "ragged totals are limited to 2^32 - 1 elements");

@@ -5,7 +5,10 @@
  * takes caller-owned device buffers and a caller-owned workspace, and never allocates. A call returns a host status
  * (CSPB_OK or a CSPB_ERR_* code) for what can be checked before the launch; what only the device can see (a bounded
  * wait that gave up, a ragged count that is negative or too large) is written to the status word at the start of the
- * workspace and read back by cspb_read_status() after the work has run.
+ * workspace and read back by cspb_read_status() after the work has run. The one exception is
+ * cspb_build_column_static, which takes no workspace: its scratch is a fixed array inside the library, and every
+ * device-side condition it can meet (a negative count, a total past 2^32 - 1, a bounded wait that gave up) is reported
+ * in the flag word it writes beside the total (CSPB_COLUMN_* bits below).
  *
  * The reference (NAGAGroup/CospanMDAO) has no C ABI: its kernels are SYCL bodies that AdaptiveCpp JIT-compiles and
  * launches from GroupLauncher::launch (cospanmdao/include/naga/cospan/component.hpp:779-970) through launch_group
@@ -46,6 +49,13 @@ enum {
 #define CSPB_DEV_EXCEEDS32 4u
 #define CSPB_DEV_CAPACITY 8u
 #define CSPB_DEV_ARGUMENT 16u  /* a task contradicts a flag of the call (CSPB_BATCH_NO_B); read as CSPB_ERR_ARGUMENT */
+
+/* bits of the flag word a ragged-column build writes to total_flag[1] (cspb_build_column, cspb_build_column_static).
+ * 1 and 2 are the reference's own flags (cospanmdao/include/naga/cospan/shape_hook.hpp:455-463); 4 is this library's:
+ * the device scan's bounded look-back gave up, so the offsets and the total are not valid. */
+#define CSPB_COLUMN_NEGATIVE 1u
+#define CSPB_COLUMN_EXCEEDS32 2u
+#define CSPB_COLUMN_TIMEOUT 4u
 
 /* storage dtypes of the big operands (the matrix of a GEMVER, the fields of a stencil) */
 enum { CSPB_F32 = 0, CSPB_BF16 = 1 };
@@ -401,8 +411,9 @@ int cspb_exclusive_scan_u64(const uint64_t* in, uint64_t* out, int64_t n, void* 
  * source, k = 1 for rank 1), writes extents[i] = max(value, 0) narrowed to u32 and offs = their exclusive scan
  * (count + 1 entries); offsets mode (offsets_mode = 1) reads count = N + 1 offsets, writes offs = the values and
  * extents[i] = offs[i+1] - offs[i]. The flag bits follow the reference: 1 = a negative value, offs[0] != 0 or a
- * decrease; 2 = a value or a total past 2^32 - 1. total_flag (device or mapped host memory, 2 words) receives
- * [offs[N], flag]. Single pass: narrow + scan + wrap check in one launch.
+ * decrease; 2 = a value or a total past 2^32 - 1; 4 (CSPB_COLUMN_TIMEOUT, no counterpart in the reference) = the
+ * bounded look-back of the scan gave up and the offsets are not valid. total_flag (device or mapped host memory,
+ * 2 words) receives [offs[N], flag]. Single pass: narrow + scan + wrap check in one launch.
  * ================================================================================================================== */
 int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
                       uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* workspace,
@@ -412,11 +423,15 @@ int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t
  * cspb_build_column_static: cspb_build_column with no workspace argument, for callers that cannot allocate device
  * memory at the call site (a foreign-language binding that holds only the column's pointers and no allocator, code
  * running where an allocation would stall or be refused). It allocates nothing: its scratch is a fixed 164,096-byte array
- * in the library's device image (one per device), found once per device by the first call made with that device
- * current; make that first call before any stream capture begins. Results are bit-identical to cspb_build_column.
+ * in the library's device image (one per device), looked up in the current device's context by each call;
+ * make the first call on a device before any stream capture begins. Results are bit-identical to cspb_build_column.
  * Limit: at most CSPB_BUILD_COLUMN_STATIC_MAX extents (count in counts mode, count - 1 in offsets mode); larger inputs
  * return CSPB_ERR_TOO_LARGE before any device work. The scratch is shared by every call on a device, so calls on one
- * device must not overlap in time (same stream, or ordered by events); overlapping calls race on it.
+ * device must not overlap in time (same stream, or ordered by events); overlapping calls race on it. The device status
+ * word of this call lives in that scratch, out of the caller's reach, so everything the device finds goes to the flag
+ * word total_flag[1]: CSPB_COLUMN_NEGATIVE, CSPB_COLUMN_EXCEEDS32, and CSPB_COLUMN_TIMEOUT when the scan's bounded wait
+ * gave up (offsets not valid). The scratch's device address is asked of the CUDA runtime on every call (a cached
+ * address would outlive a cudaDeviceReset); the first call on a device also loads the library's device image there.
  * No counterpart in the reference (its build_column allocates its temporaries on every call).
  * ================================================================================================================== */
 #define CSPB_BUILD_COLUMN_STATIC_MAX (1 << 24)

@@ -33,7 +33,8 @@ def test_header_flags_match_the_python_view():
     text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
     defs = dict(re.findall(r"#define CSPB_([A-Z0-9_]+) \(?([0-9a-fx <u]+?)\)?\s*$", text, flags=re.M))
     want = {"DEV_TIMEOUT", "DEV_NEGATIVE", "DEV_EXCEEDS32", "DEV_CAPACITY", "DEV_ARGUMENT", "GEMVER_PANEL",
-            "GEMVER_BULK", "GEMVER_LOWRANK", "BATCH_LOWRANK", "BATCH_NO_B"}
+            "GEMVER_BULK", "GEMVER_LOWRANK", "BATCH_LOWRANK", "BATCH_NO_B", "COLUMN_NEGATIVE", "COLUMN_EXCEEDS32",
+            "COLUMN_TIMEOUT"}
     assert want <= set(defs), want - set(defs)
     for name in want:
         assert eval(defs[name].replace("u", "")) == getattr(_capi, name), name
