@@ -273,9 +273,10 @@ NS_DIAG = ("Dt", "Ws", "Sq0", "Sq1", "Sq2", "Sq3", "detn0", "detn1", "detn2", "d
 
 
 def ns_compressible(U, *, limiter: str = "minmod", bc: str = "walls", R=None, diag=None, det_sq64=None,
-                    workspace: Workspace | None = None, stream=None):
+                    reference_rounding: bool = False, workspace: Workspace | None = None, stream=None):
     """The reference's compressible residual and diagnostics. U: (4, ny, nx) float32. Returns (R, diag, det_sq64)
-    with diag the 18 floats of include/cspb.h (NS_DIAG names them)."""
+    with diag the 18 floats of include/cspb.h (NS_DIAG names them). reference_rounding=True selects the kernel that
+    rounds every operation as a sequential f32 evaluation of the reference's physics.hpp does (the same bits)."""
     torch = _torch()
     if limiter not in ("minmod", "vanleer"):
         raise ValueError("--limiter must be minmod|vanleer")
@@ -291,7 +292,8 @@ def ns_compressible(U, *, limiter: str = "minmod", bc: str = "walls", R=None, di
     det_sq64 = torch.empty(4, dtype=torch.float64, device=dev) if det_sq64 is None else det_sq64
     ws = workspace or default_workspace(dev, stream)
     wp, wb = ws.ptr(lib().cspb_ns_comp_workspace_bytes(nx, ny))
-    d = _capi.NsCompDesc(nx, ny, 0 if limiter == "minmod" else 1, 1 if bc == "walls" else 0, _ptr(U), _ptr(R),
+    d = _capi.NsCompDesc(nx, ny, 0 if limiter == "minmod" else 1, 1 if bc == "walls" else 0,
+                         _capi.NS_REFERENCE_ROUNDING if reference_rounding else 0, 0, _ptr(U), _ptr(R),
                          _ptr(diag), _ptr(det_sq64), wp, wb)
     _raise(lib().cspb_ns_compressible(C.byref(d), C.c_void_p(_stream(stream))), "ns-residual")
     return R, diag, det_sq64

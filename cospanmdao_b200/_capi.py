@@ -43,6 +43,7 @@ GEMVER_BULK = 2
 GEMVER_LOWRANK = 4
 BATCH_LOWRANK = 1 << 16
 BATCH_NO_B = 1 << 17
+NS_REFERENCE_ROUNDING = 1
 I32, U32, I64, U64 = 0, 1, 2, 3
 
 vp = C.c_void_p
@@ -104,7 +105,8 @@ class NsIncompTask(C.Structure):
 
 
 class NsCompDesc(C.Structure):
-    _fields_ = [("nx", i32), ("ny", i32), ("limiter", i32), ("walls", i32), ("U", vp), ("R", vp), ("diag", vp),
+    _fields_ = [("nx", i32), ("ny", i32), ("limiter", i32), ("walls", i32), ("flags", i32), ("reserved", i32),
+                ("U", vp), ("R", vp), ("diag", vp),
                 ("det_sq64", vp), ("workspace", vp), ("workspace_bytes", sz)]
 
 

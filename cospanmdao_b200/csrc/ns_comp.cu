@@ -22,7 +22,7 @@
 namespace cspb {
 namespace nsc {
 
-constexpr int TX = 32, TY = 16;              // tile of cells
+constexpr int TX = 32, TY = 15;              // tile of cells: 16 rows of y-faces, two per thread (rows f, f + 8)
 constexpr int LX = TX + 4, LY = TY + 4;      // with the 2-cell halo
 constexpr int LC = LX * LY;                  // 720
 constexpr int NXF = (TX + 1) * TY;           // x-faces of the tile's rows
@@ -30,134 +30,244 @@ constexpr int NYF = TX * (TY + 1);           // y-faces of the tile's columns
 constexpr int kThreads = 256;
 
 constexpr float kG = 1.4f, kMu = 0.01f, kPr = 0.72f, kCfl = 0.5f;
+constexpr float kGm1 = kG - 1.0f;                   // γ - 1 in f32, as the reference's T(kGamma) - T(1)
+constexpr float kInvGm1 = 1.0f / kGm1;              // its reciprocal, rounded once (fast arithmetic only)
+constexpr float kKt = kMu * kG / (kGm1 * kPr);      // the heat conductivity μγ / ((γ - 1) Pr), as visc_flux forms it
+constexpr float kTwo3 = 2.0f / 3.0f;
+constexpr float kNuMax = (4.0f / 3.0f) > (kG / kPr) ? (4.0f / 3.0f) : (kG / kPr);  // tmax(4/3, γ / Pr)
 
 // The tile's state in shared memory: primitives and temperature of the tile with its 2-cell halo, and both fluxes of
-// every face. A face forms the gradients and limited slopes of its two cells from W and T itself, with the formulas
-// a per-cell table would hold (the same bits): a table of both for the 612 cells [-1, T] took 34 KB more, which left
-// room for 2 tiles per SM instead of 4.
+// every face. A face forms the gradients and limited slopes of its two cells from W and T itself.
 struct Smem {
-    float W[4][LC];  // primitives ρ u v p
-    float T[LC];     // p / ρ
+    float W[4][LC];    // primitives ρ u v p
+    float T[LC];       // p / ρ
     float FX[8][NXF];  // HLLC 0..3, viscous 4..7
     float FY[8][NYF];
 };
 
-__device__ __forceinline__ float fmn(float a, float b) { return a < b ? a : b; }
-__device__ __forceinline__ float fmx(float a, float b) { return a > b ? a : b; }
+// ---- arithmetic on pairs of faces (or cells) ------------------------------------------------------------------------
+// A thread evaluates two faces at once: every value is a float2 whose lanes belong to the two faces, and the adds,
+// multiplies and fused multiply-adds are Blackwell's packed f32x2 instructions (FADD2 / FMUL2 / FFMA2), each lane
+// rounded exactly as the scalar instruction would round it. Divisions, square roots, comparisons and selects act per
+// lane. Ar<X> is the arithmetic policy:
+//   X = false  the fast form: fused multiply-adds where they fit, approximate reciprocal / division / reciprocal square
+//              root in the face fluxes (about 2 ulp);
+//   X = true   the reference's rounding: the formulas of physics.hpp in their written order, every multiply and add
+//              rounded separately (no fused multiply-add), IEEE division and square root. The residual is then
+//              bit-identical to a sequential f32 evaluation of physics.hpp (the oracle's ns_comp_f32). This form
+//              works lane by lane with __fadd_rn / __fsub_rn / __fmul_rn, which the compiler never merges into a
+//              fused multiply-add; a subtraction written as a packed a + b·(-1) was merged with the multiply that
+//              produced b in some faces, which changed the last bit.
+using V = float2;
+__device__ __forceinline__ V v2(float a, float b) { return make_float2(a, b); }
+// the hardware's approximate reciprocal and square root (one MUFU instruction each; sqrt(0) = 0)
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ V sp(float a) { return make_float2(a, a); }
 
-template <int LIM>
-__device__ __forceinline__ float slope(float a, float b) {
-    if (LIM == 0) {
-        if (a * b <= 0.0f) return 0.0f;
-        return a > 0.0f ? fmn(a, b) : fmx(a, b);
-    } else {
-        const float ab = a * b;
+template <bool X>
+struct Ar {
+    static __device__ __forceinline__ V add(V a, V b) {
+        if constexpr (X) return v2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+        else return __fadd2_rn(a, b);
+    }
+    // fast form: a - b as a + b·(-1) (one rounding; the compiler may fuse a multiply that produced b into it)
+    static __device__ __forceinline__ V sub(V a, V b) {
+        if constexpr (X) return v2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+        else return __ffma2_rn(b, sp(-1.0f), a);
+    }
+    static __device__ __forceinline__ V mul(V a, V b) {
+        if constexpr (X) return v2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+        else return __fmul2_rn(a, b);
+    }
+    static __device__ __forceinline__ V fma(V a, V b, V c) {  // a·b + c
+        if constexpr (X) return add(mul(a, b), c);
+        else return __ffma2_rn(a, b, c);
+    }
+    // division: IEEE per lane, or (fast) the approximate reciprocal per lane times a, packed
+    static __device__ __forceinline__ V div(V a, V b) {
+        if constexpr (X) return v2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y));
+        else return mul(a, rcp(b));
+    }
+    static __device__ __forceinline__ V rcp(V b) { return v2(rcp_approx(b.x), rcp_approx(b.y)); }
+    // tmin / tmax of physics.hpp (a < b ? a : b); the fast form takes the min / max instructions
+    static __device__ __forceinline__ float mn1(float a, float b) {
+        if constexpr (X) return a < b ? a : b;
+        else return fminf(a, b);
+    }
+    static __device__ __forceinline__ float mx1(float a, float b) {
+        if constexpr (X) return a > b ? a : b;
+        else return fmaxf(a, b);
+    }
+    static __device__ __forceinline__ V mn(V a, V b) { return v2(mn1(a.x, b.x), mn1(a.y, b.y)); }
+    static __device__ __forceinline__ V mx(V a, V b) { return v2(mx1(a.x, b.x), mx1(a.y, b.y)); }
+};
+
+// The limited slope from the backward difference a and the forward difference b (MinMod / VanLeer, physics.hpp:62-80):
+// zero at an extremum. MinMod returns whichever of a, b is nearer zero: the fast form as min(|a|, |b|) with a's sign.
+template <int LIM, bool X>
+__device__ __forceinline__ float minmod1(float a, float b, float ab) {
+    if constexpr (X) {
         if (ab <= 0.0f) return 0.0f;
-        return 2.0f * ab / (a + b);
-    }
-}
-
-// 1 / (γ - 1), rounded once
-constexpr float kInvGm1 = 1.0f / (kG - 1.0f);
-
-// HLLC with Davis speeds; D = 0 normal x, D = 1 normal y; L / R primitives (ρ, u, v, p). The divisions by ρ of a side
-// are products with its reciprocal, p / (γ - 1) a product with 1 / (γ - 1). The face's reciprocals, square roots and
-// divisions use the hardware's approximate forms (__fdividef, rsqrtf: about 2 ulp): at 4096² they took the kernel
-// from 0.709 to 0.657 ms, and the residual's relative L2 error against the f64 oracle from 4.4e-6 to 4.7e-6 (the f32
-// storage of U dominates it; the reference's bound is 1e-4). The per-cell phases, and so the diagnostics, keep the
-// correctly rounded forms.
-template <int D>
-__device__ __forceinline__ void hllc(const float (&L)[4], const float (&R)[4], float (&F)[4]) {
-    const float rl = L[0], rr = R[0], pl = L[3], pr = R[3];
-    const float unl = L[1 + D], utl = L[2 - D];
-    const float unr = R[1 + D], utr = R[2 - D];
-    const float irl = __fdividef(1.0f, rl), irr = __fdividef(1.0f, rr);
-    const float gl = kG * pl * irl, gr = kG * pr * irr;
-    const float cl = gl > 0.0f ? gl * rsqrtf(gl) : 0.0f, cr = gr > 0.0f ? gr * rsqrtf(gr) : 0.0f;
-    const float El = pl * kInvGm1 + 0.5f * rl * (unl * unl + utl * utl);
-    const float Er = pr * kInvGm1 + 0.5f * rr * (unr * unr + utr * utr);
-    const float sl = fmn(unl - cl, unr - cr);
-    const float sr = fmx(unl + cl, unr + cr);
-    const float sm = __fdividef(pr - pl + rl * unl * (sl - unl) - rr * unr * (sr - unr), rl * (sl - unl) - rr * (sr - unr));
-    float f0, f1, f2, f3;
-    if (sl >= 0.0f) {
-        f0 = rl * unl; f1 = rl * unl * unl + pl; f2 = rl * unl * utl; f3 = (El + pl) * unl;
-    } else if (sr <= 0.0f) {
-        f0 = rr * unr; f1 = rr * unr * unr + pr; f2 = rr * unr * utr; f3 = (Er + pr) * unr;
+        return a > 0.0f ? (a < b ? a : b) : (a > b ? a : b);
     } else {
-        const bool left = sm >= 0.0f;
-        const float r = left ? rl : rr, un = left ? unl : unr, ut = left ? utl : utr, p = left ? pl : pr;
-        const float E = left ? El : Er, s = left ? sl : sr, ir = left ? irl : irr;
-        const float a = s - un;
-        const float k = __fdividef(r * a, s - sm);
-        const float Es = k * (E * ir + (sm - un) * (sm + __fdividef(p * ir, a)));
-        f0 = r * un + s * (k - r);
-        f1 = r * un * un + p + s * (k * sm - r * un);
-        f2 = r * un * ut + s * (k * ut - r * ut);
-        f3 = (E + p) * un + s * (Es - E);
+        return ab <= 0.0f ? 0.0f : copysignf(fminf(fabsf(a), fabsf(b)), a);
     }
-    F[0] = f0;
-    F[1 + D] = f1;
-    F[2 - D] = f2;
-    F[3] = f3;
+}
+template <int LIM, bool X>
+__device__ __forceinline__ V slope2(V a, V b) {
+    using A = Ar<X>;
+    const V ab = A::mul(a, b);
+    if constexpr (LIM == 0) {
+        return v2(minmod1<LIM, X>(a.x, b.x, ab.x), minmod1<LIM, X>(a.y, b.y, ab.y));
+    } else {
+        const V q = A::div(A::mul(sp(2.0f), ab), A::add(a, b));
+        return v2(ab.x <= 0.0f ? 0.0f : q.x, ab.y <= 0.0f ? 0.0f : q.y);
+    }
 }
 
-// The viscous flux through a face of normal D: the normal derivatives are the differences of the two cells; the
-// tangential ones (ut_u, ut_v, ut_T) the means of the two cells' central differences.
-template <int D>
-__device__ __forceinline__ void visc(const float (&L)[4], const float (&R)[4], float TL, float TR, float du_t,
-                                     float dv_t, float dT_t, float (&F)[4]) {
-    const float uf = 0.5f * (L[1] + R[1]), vf = 0.5f * (L[2] + R[2]);
-    float ux, uy, vx, vy, Tx, Ty;
+__device__ __forceinline__ V sel(bool cx, bool cy, V a, V b) { return v2(cx ? a.x : b.x, cy ? a.y : b.y); }
+
+// HLLC with Davis speeds through faces of normal D (0: x, 1: y); L / R the reconstructed primitives (ρ, u, v, p) of
+// the two sides (physics.hpp:109-152). Per lane the region is chosen as the reference chooses it (sl >= 0: left state;
+// sr <= 0: right state; else the star state of the side sm points to); the side state's flux is the first term of the
+// star flux, so both regions share it and the star increment s·(…) is added where the face is in the star region.
+template <int D, bool X>
+__device__ __forceinline__ void hllc2(const V (&L)[4], const V (&R)[4], V (&F)[4]) {
+    using A = Ar<X>;
+    const V rl = L[0], rr = R[0], pl = L[3], pr = R[3];
+    const V unl = L[1 + D], utl = L[2 - D];
+    const V unr = R[1 + D], utr = R[2 - D];
+    const V half = sp(0.5f);
+    V cl, cr, El, Er, irl, irr;
+    if constexpr (X) {
+        const V gl = A::div(A::mul(sp(kG), pl), rl), gr = A::div(A::mul(sp(kG), pr), rr);
+        cl = v2(__fsqrt_rn(gl.x), __fsqrt_rn(gl.y));
+        cr = v2(__fsqrt_rn(gr.x), __fsqrt_rn(gr.y));
+        El = A::add(A::div(pl, sp(kGm1)), A::mul(A::mul(half, rl), A::add(A::mul(unl, unl), A::mul(utl, utl))));
+        Er = A::add(A::div(pr, sp(kGm1)), A::mul(A::mul(half, rr), A::add(A::mul(unr, unr), A::mul(utr, utr))));
+        irl = irr = sp(0.0f);
+    } else {
+        irl = A::rcp(rl);
+        irr = A::rcp(rr);
+        const V gl = A::mul(A::mul(sp(kG), pl), irl), gr = A::mul(A::mul(sp(kG), pr), irr);
+        cl = v2(sqrt_approx(gl.x), sqrt_approx(gl.y));
+        cr = v2(sqrt_approx(gr.x), sqrt_approx(gr.y));
+        El = A::fma(A::mul(half, rl), A::fma(unl, unl, A::mul(utl, utl)), A::mul(pl, sp(kInvGm1)));
+        Er = A::fma(A::mul(half, rr), A::fma(unr, unr, A::mul(utr, utr)), A::mul(pr, sp(kInvGm1)));
+    }
+    const V sl = A::mn(A::sub(unl, cl), A::sub(unr, cr));
+    const V sr = A::mx(A::add(unl, cl), A::add(unr, cr));
+    const V al = A::sub(sl, unl), ar = A::sub(sr, unr);
+    const V num = A::sub(A::fma(A::mul(rl, unl), al, A::sub(pr, pl)), A::mul(A::mul(rr, unr), ar));
+    const V sm = A::div(num, A::sub(A::mul(rl, al), A::mul(rr, ar)));
+
+    const bool supx = sl.x >= 0.0f, supy = sl.y >= 0.0f;        // supersonic to the right: the left state
+    const bool subx = sr.x <= 0.0f, suby = sr.y <= 0.0f;        // supersonic to the left: the right state
+    const bool lx = supx || (!subx && sm.x >= 0.0f), ly = supy || (!suby && sm.y >= 0.0f);
+    const bool starx = !supx && !subx, stary = !supy && !suby;
+    const V r = sel(lx, ly, rl, rr), un = sel(lx, ly, unl, unr), ut = sel(lx, ly, utl, utr);
+    const V p = sel(lx, ly, pl, pr), E = sel(lx, ly, El, Er), s = sel(lx, ly, sl, sr);
+    const V ru = A::mul(r, un);
+    const V f0 = ru, f1 = A::fma(ru, un, p), f2 = A::mul(ru, ut), f3 = A::mul(A::add(E, p), un);
+    const V a = A::sub(s, un);
+    const V k = A::div(A::mul(r, a), A::sub(s, sm));
+    V Es;
+    if constexpr (X) {
+        Es = A::mul(k, A::add(A::div(E, r), A::mul(A::sub(sm, un), A::add(sm, A::div(p, A::mul(r, a))))));
+    } else {
+        const V ir = sel(lx, ly, irl, irr);
+        Es = A::mul(k, A::fma(A::sub(sm, un), A::add(sm, A::div(A::mul(p, ir), a)), A::mul(E, ir)));
+    }
+    const V g0 = A::fma(s, A::sub(k, r), f0);
+    const V g1 = A::fma(s, A::sub(A::mul(k, sm), ru), f1);
+    const V g2 = A::fma(s, A::sub(A::mul(k, ut), A::mul(r, ut)), f2);
+    const V g3 = A::fma(s, A::sub(Es, E), f3);
+    F[0] = sel(starx, stary, g0, f0);
+    F[1 + D] = sel(starx, stary, g1, f1);
+    F[2 - D] = sel(starx, stary, g2, f2);
+    F[3] = sel(starx, stary, g3, f3);
+}
+
+// The viscous flux through faces of normal D (physics.hpp:157-192): the normal derivatives are the differences of the
+// two cells; the tangential ones (dut, dvt, dTt) the means of the two cells' central differences.
+template <int D, bool X>
+__device__ __forceinline__ void visc2(const V (&L)[4], const V (&R)[4], V TL, V TR, V dut, V dvt, V dTt,
+                                      V (&F)[4]) {
+    using A = Ar<X>;
+    const V half = sp(0.5f);
+    const V uf = A::mul(half, A::add(L[1], R[1])), vf = A::mul(half, A::add(L[2], R[2]));
+    V ux, uy, vx, vy, Tx, Ty;
     if (D == 0) {
-        ux = R[1] - L[1]; vx = R[2] - L[2]; Tx = TR - TL;
-        uy = du_t; vy = dv_t; Ty = dT_t;
+        ux = A::sub(R[1], L[1]); vx = A::sub(R[2], L[2]); Tx = A::sub(TR, TL);
+        uy = dut; vy = dvt; Ty = dTt;
     } else {
-        uy = R[1] - L[1]; vy = R[2] - L[2]; Ty = TR - TL;
-        ux = du_t; vx = dv_t; Tx = dT_t;
+        uy = A::sub(R[1], L[1]); vy = A::sub(R[2], L[2]); Ty = A::sub(TR, TL);
+        ux = dut; vx = dvt; Tx = dTt;
     }
-    const float mu = kMu;
-    const float k = mu * kG / ((kG - 1.0f) * kPr);
-    const float dv = ux + vy;
-    const float txx = mu * (2.0f * ux - 2.0f / 3.0f * dv);
-    const float tyy = mu * (2.0f * vy - 2.0f / 3.0f * dv);
-    const float txy = mu * (uy + vx);
-    F[0] = 0.0f;
+    const V mu = sp(kMu), two = sp(2.0f);
+    const V dv = A::add(ux, vy);
+    const V t3 = A::mul(sp(kTwo3), dv);
+    const V txx = A::mul(mu, A::sub(A::mul(two, ux), t3));
+    const V tyy = A::mul(mu, A::sub(A::mul(two, vy), t3));
+    const V txy = A::mul(mu, A::add(uy, vx));
+    F[0] = sp(0.0f);
     if (D == 0) {
-        F[1] = txx; F[2] = txy; F[3] = uf * txx + vf * txy + k * Tx;
+        F[1] = txx; F[2] = txy; F[3] = A::fma(sp(kKt), Tx, A::fma(vf, txy, A::mul(uf, txx)));
     } else {
-        F[1] = txy; F[2] = tyy; F[3] = uf * txy + vf * tyy + k * Ty;
+        F[1] = txy; F[2] = tyy; F[3] = A::fma(sp(kKt), Ty, A::fma(vf, tyy, A::mul(uf, txy)));
     }
 }
 
-// One face of normal D between cells cl and cl + st (st the neighbour along the normal): the limited slopes of both
-// cells along the normal, the reconstructed states, the HLLC flux, the tangential gradients of both cells and the
-// viscous flux; the 8 fluxes go to out[v * stride] (HLLC 0..3, viscous 4..7).
-template <int LIM, int D, int stride>
-__device__ __forceinline__ void face(const Smem& s, int cl, float* out) {
+// Two faces of normal D, the first between smem cells ca and ca + st, the second between cb and cb + st (st the
+// neighbour along the normal): the limited slopes of the four cells along the normal, the reconstructed states, the
+// HLLC fluxes, the tangential gradients and the viscous fluxes; HLLC to Fc, viscous to Fv.
+template <int LIM, int D, bool X>
+__device__ __forceinline__ void face2(const Smem& s, int ca, int cb, V (&Fc)[4], V (&Fv)[4]) {
+    using A = Ar<X>;
     constexpr int st = D == 0 ? 1 : LX;  // along the normal
     constexpr int tn = D == 0 ? LX : 1;  // along the face
-    const int cr = cl + st;
-    float pl[4], pr[4], wl[4], wr[4], Fc[4], Fv[4];
+    V pl[4], pr[4], wl[4], wr[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const float a = s.W[v][cl - st], b = s.W[v][cr + st];
-        pl[v] = s.W[v][cl];
-        pr[v] = s.W[v][cr];
-        const float sl = slope<LIM>(pl[v] - a, pr[v] - pl[v]);
-        const float sr = slope<LIM>(pr[v] - pl[v], b - pr[v]);
-        wl[v] = pl[v] + 0.5f * sl;
-        wr[v] = pr[v] - 0.5f * sr;
+        const float* w = s.W[v];
+        const V a = v2(w[ca - st], w[cb - st]);
+        pl[v] = v2(w[ca], w[cb]);
+        pr[v] = v2(w[ca + st], w[cb + st]);
+        const V b = v2(w[ca + 2 * st], w[cb + 2 * st]);
+        const V dc = A::sub(pr[v], pl[v]);
+        const V sl = slope2<LIM, X>(A::sub(pl[v], a), dc);
+        const V sr = slope2<LIM, X>(dc, A::sub(b, pr[v]));
+        wl[v] = A::fma(sp(0.5f), sl, pl[v]);   // w + slope / 2
+        wr[v] = A::fma(sp(-0.5f), sr, pr[v]);  // w - slope / 2
     }
-    hllc<D>(wl, wr, Fc);
+    hllc2<D, X>(wl, wr, Fc);
+    const V half = sp(0.5f);
     auto tangential = [&](const float* q) {  // the mean of the two cells' central differences along the face
-        return 0.5f * (0.5f * (q[cl + tn] - q[cl - tn]) + 0.5f * (q[cr + tn] - q[cr - tn]));
+        const V gl = A::mul(half, A::sub(v2(q[ca + tn], q[cb + tn]), v2(q[ca - tn], q[cb - tn])));
+        const V gr = A::mul(half, A::sub(v2(q[ca + st + tn], q[cb + st + tn]), v2(q[ca + st - tn], q[cb + st - tn])));
+        return A::mul(half, A::add(gl, gr));
     };
-    visc<D>(pl, pr, s.T[cl], s.T[cr], tangential(s.W[1]), tangential(s.W[2]), tangential(s.T), Fv);
+    visc2<D, X>(pl, pr, v2(s.T[ca], s.T[cb]), v2(s.T[ca + st], s.T[cb + st]), tangential(s.W[1]),
+                tangential(s.W[2]), tangential(s.T), Fv);
+}
+
+template <int D, int stride>
+__device__ __forceinline__ void store_face(float* out, int ia, int ib, const V (&Fc)[4], const V (&Fv)[4]) {
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        out[v * stride] = Fc[v];
-        out[(4 + v) * stride] = Fv[v];
+        out[v * stride + ia] = Fc[v].x;
+        out[v * stride + ib] = Fc[v].y;
+        out[(4 + v) * stride + ia] = Fv[v].x;
+        out[(4 + v) * stride + ib] = Fv[v].y;
     }
 }
 
@@ -178,11 +288,30 @@ constexpr int kDtKey = 16, kWsBits = 17, kSq0 = 18;
 
 __device__ __forceinline__ int wrapi(int k, int n) { return ((k % n) + n) % n; }
 
-template <int LIM>
+// dt and wave speed of one cell from its primitives (cell_diag, physics.hpp:196-202)
+template <bool X>
+__device__ __forceinline__ void cell_dt_ws(float rho, float u, float v, float p, float T, float& dt, float& ws) {
+    if constexpr (X) {
+        const float c = __fsqrt_rn(__fdiv_rn(__fmul_rn(kG, p), rho));
+        const float ax = __fadd_rn(fabsf(u), c), ay = __fadd_rn(fabsf(v), c);
+        const float nu = __fmul_rn(__fdiv_rn(kMu, rho), kNuMax);
+        dt = __fdiv_rn(kCfl, __fadd_rn(__fadd_rn(ax, ay), __fmul_rn(4.0f, nu)));
+        ws = ax > ay ? ax : ay;
+    } else {
+        const float c = sqrtf(kG * T);  // T = p / ρ
+        const float ax = fabsf(u) + c, ay = fabsf(v) + c;
+        const float nu = kMu * __frcp_rn(rho) * kNuMax;
+        dt = kCfl / (ax + ay + 4.0f * nu);
+        ws = fmaxf(ax, ay);
+    }
+}
+
+template <int LIM, bool X>
 __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
+    using A = Ar<X>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& s = *reinterpret_cast<Smem*>(smem_raw);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tile = blockIdx.x;
     const int tx0 = (tile % g.tiles_x) * TX, ty0 = (tile / g.tiles_x) * TY;
     const int64_t plane = int64_t(g.nx) * g.ny;
@@ -204,104 +333,136 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
         }
         const int64_t c = int64_t(js) * g.nx + is;
         const float r = __ldg(g.U + c);
-        const float mu = __ldg(g.U + plane + c) * sg;
+        const float mu = __ldg(g.U + plane + c) * sg;  // a sign flip: exact
         const float mv = __ldg(g.U + 2 * plane + c) * sg;
         const float E = __ldg(g.U + 3 * plane + c);
-        const float ir = __frcp_rn(r);
-        const float u = mu * ir, v = mv * ir;
-        const float p = (kG - 1.0f) * (E - 0.5f * r * (u * u + v * v));
+        float u, v, p, T;
+        if constexpr (X) {
+            u = __fdiv_rn(mu, r);
+            v = __fdiv_rn(mv, r);
+            p = __fmul_rn(kGm1, __fsub_rn(E, __fmul_rn(__fmul_rn(0.5f, r), __fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)))));
+            T = __fdiv_rn(p, r);
+        } else {
+            const float ir = __frcp_rn(r);
+            u = mu * ir;
+            v = mv * ir;
+            p = kGm1 * (E - 0.5f * r * (u * u + v * v));
+            T = p * ir;
+        }
         s.W[0][idx] = r;
         s.W[1][idx] = u;
         s.W[2][idx] = v;
         s.W[3][idx] = p;
-        s.T[idx] = p * ir;
+        s.T[idx] = T;
     }
     __syncthreads();
 
-    // 2. every face of the tile's cells, once (tile_gradients, tile_reconstruct, tile_conv_flux, tile_visc_flux).
-    // Work items in warp-uniform runs: the 17 rows of y-faces, the 16 rows of x-faces west of each tile cell (a warp
-    // per row, so the reads are conflict-free), then the 16 x-faces on the tile's east edge.
-    for (int f = tid; f < NXF + NYF; f += kThreads) {
-        if (f < NYF) {
-            const int r = f / TX, k = f - r * TX;  // between tile cells (r-1, k) and (r, k)
-            face<LIM, 1, NYF>(s, (r + 1) * LX + (k + 2), &s.FY[0][f]);
-        } else {
-            int r, k;  // between tile cells (r, k-1) and (r, k)
-            const int q = f - NYF;
-            if (q < TY * TX) {
-                r = q / TX;
-                k = q - r * TX;
-            } else {
-                r = q - TY * TX;
-                k = TX;
-            }
-            face<LIM, 0, NXF>(s, (r + 2) * LX + (k + 1), &s.FX[0][r * (TX + 1) + k]);
-        }
-    }
-    __syncthreads();
-
-    // 3. R = -div F_conv + div F_visc per cell (cell_divergence), and the per-cell diagnostics
-    float dtmin = 3.0e38f, wsmax = 0.0f;
-    float sqf[4] = {0.f, 0.f, 0.f, 0.f};
-    double sqd[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int idx = tid; idx < TX * TY; idx += kThreads) {
-        const int r = idx / TX, k = idx - r * TX;
-        const int j = ty0 + r, i = tx0 + k;
-        if (j >= g.ny || i >= g.nx) continue;
-        const int xw = r * (TX + 1) + k, xe = xw + 1, ys = r * TX + k, yn = ys + TX;
-        const int64_t o = int64_t(j) * g.nx + i;
+    // 2. every face of the tile's cells, once, two per thread (tile_gradients, tile_reconstruct, tile_conv_flux,
+    // tile_visc_flux). A warp takes one row of 32 faces for each lane of its pairs, so its shared-memory reads are
+    // conflict-free. y-faces: face rows f = warp and f + 8 (face row f is the south face of tile row f; row 15 the
+    // north face of row 14). x-faces: rows warp and warp + 8 (warps 0..6); warp 7 takes row 7 and, in its second
+    // lanes, the 15 east faces of column 31. Every thread evaluates two y-faces and two x-faces: no warp waits for
+    // another at the barrier, and each direction is one copy of the face code, so a face on the tile's north or
+    // east edge, which the neighbouring tile evaluates too, gets the same bits from both.
+    {
+        V Fc[4], Fv[4];
+        const int f = warp, k = lane;
+        // y: between smem cells (f + 1, k + 2) and (f + 2, k + 2)
+        face2<LIM, 1, X>(s, (f + 1) * LX + (k + 2), (f + 9) * LX + (k + 2), Fc, Fv);
+        store_face<1, NYF>(&s.FY[0][0], f * TX + k, (f + 8) * TX + k, Fc, Fv);
+        // x: the west face of tile cell (r, c) lies between smem cells (r + 2, c + 1) and (r + 2, c + 2)
+        const bool east = warp == 7;
+        const int rb = east ? (lane < TY ? lane : lane - TY) : f + 8, cb_ = east ? TX : k;
+        face2<LIM, 0, X>(s, (f + 2) * LX + (k + 1), (rb + 2) * LX + (cb_ + 1), Fc, Fv);
+        const int ia = f * (TX + 1) + k, ib = rb * (TX + 1) + cb_;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const float divc = (s.FX[v][xe] - s.FX[v][xw]) + (s.FY[v][yn] - s.FY[v][ys]);
-            const float divv = (s.FX[4 + v][xe] - s.FX[4 + v][xw]) + (s.FY[4 + v][yn] - s.FY[4 + v][ys]);
-            const float rv = -divc + divv;
-            g.R[v * plane + o] = rv;
-            sqf[v] += rv * rv;
-            sqd[v] = __fma_rn(double(rv), double(rv), sqd[v]);
+            s.FX[v][ia] = Fc[v].x;
+            s.FX[4 + v][ia] = Fv[v].x;
         }
-        const int c = (r + 2) * LX + (k + 2);
-        const float rho = s.W[0][c], u = s.W[1][c], vv = s.W[2][c];
-        const float cs = sqrtf(kG * s.T[c]);  // T = p / ρ
-        const float ax = fabsf(u) + cs, ay = fabsf(vv) + cs;
-        const float nu = kMu * __frcp_rn(rho) * fmx(4.0f / 3.0f, kG / kPr);
-        const float dt = kCfl / (ax + ay + 4.0f * nu);
-        const float ws = fmx(ax, ay);
-        dtmin = fmn(dtmin, dt);
-        wsmax = fmx(wsmax, ws);
+        if (!east || lane < TY) {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                s.FX[v][ib] = Fc[v].y;
+                s.FX[4 + v][ib] = Fv[v].y;
+            }
+        }
+    }
+    __syncthreads();
+
+    // 3. R = -div F_conv + div F_visc per cell (cell_divergence: conv, then visc added), two cells per thread (rows r and
+    // r + 8 of column k; warp 7 has row 7 only), and the per-cell diagnostics
+    float dtmin = 3.0e38f, wsmax = 0.0f;
+    double sqd[4] = {0.0, 0.0, 0.0, 0.0};
+    {
+        const int r = warp, k = lane;
+        const int r1 = warp < 7 ? r + 8 : r;  // warp 7: the second lane repeats the first (not stored)
+        const int j0 = ty0 + r, j1 = ty0 + r1, i = tx0 + k;
+        const bool in0 = j0 < g.ny && i < g.nx, in1 = warp < 7 && j1 < g.ny && i < g.nx;
+        const int xw0 = r * (TX + 1) + k, xw1 = r1 * (TX + 1) + k;
+        const int ys0 = r * TX + k, ys1 = r1 * TX + k;
+        const int64_t o0 = int64_t(j0) * g.nx + i, o1 = int64_t(j1) * g.nx + i;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const float* fx = s.FX[v];
+            const float* fy = s.FY[v];
+            const float* gx = s.FX[4 + v];
+            const float* gy = s.FY[4 + v];
+            const V divc = A::add(A::sub(v2(fx[xw0 + 1], fx[xw1 + 1]), v2(fx[xw0], fx[xw1])),
+                                  A::sub(v2(fy[ys0 + TX], fy[ys1 + TX]), v2(fy[ys0], fy[ys1])));
+            const V divv = A::add(A::sub(v2(gx[xw0 + 1], gx[xw1 + 1]), v2(gx[xw0], gx[xw1])),
+                                  A::sub(v2(gy[ys0 + TX], gy[ys1 + TX]), v2(gy[ys0], gy[ys1])));
+            const V rv = A::sub(divv, divc);  // -divc + divv: the same bits
+            if (in0) {
+                g.R[v * plane + o0] = rv.x;
+                sqd[v] = __fma_rn(double(rv.x), double(rv.x), sqd[v]);
+            }
+            if (in1) {
+                g.R[v * plane + o1] = rv.y;
+                sqd[v] = __fma_rn(double(rv.y), double(rv.y), sqd[v]);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h == 0 ? !in0 : !in1) continue;
+            const int c = ((h == 0 ? r : r1) + 2) * LX + (k + 2);
+            float dt, ws;
+            cell_dt_ws<X>(s.W[0][c], s.W[1][c], s.W[2][c], s.W[3][c], s.T[c], dt, ws);
+            dtmin = fminf(dtmin, dt);
+            wsmax = fmaxf(wsmax, ws);
+        }
     }
 
-    // 4. the tile's reductions (fixed order: xor tree in the warp, warps in order)
-    __shared__ float r_dt[kThreads / 32], r_ws[kThreads / 32], r_sqf[kThreads / 32][4];
+    // 4. the tile's reductions (fixed order: xor tree in the warp, warps in order). The tile's Σ R² is summed once, in
+    // f64: the deterministic path keeps it, the atomic path adds it rounded to f32 (the reference's atomic stage adds
+    // each tile's f32 group sum; either way the atomic total depends on the order the tiles finish in).
+    __shared__ float r_dt[kThreads / 32], r_ws[kThreads / 32];
     __shared__ double r_sqd[kThreads / 32][4];
     __shared__ int s_last;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
-        dtmin = fmn(dtmin, __shfl_xor_sync(0xffffffffu, dtmin, off));
-        wsmax = fmx(wsmax, __shfl_xor_sync(0xffffffffu, wsmax, off));
+        dtmin = fminf(dtmin, __shfl_xor_sync(0xffffffffu, dtmin, off));
+        wsmax = fmaxf(wsmax, __shfl_xor_sync(0xffffffffu, wsmax, off));
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            sqf[v] += __shfl_xor_sync(0xffffffffu, sqf[v], off);
-            sqd[v] += __shfl_xor_sync(0xffffffffu, sqd[v], off);
-        }
+        for (int v = 0; v < 4; ++v) sqd[v] += __shfl_xor_sync(0xffffffffu, sqd[v], off);
     }
-    const int warp = tid >> 5, lane = tid & 31;
     if (lane == 0) {
         r_dt[warp] = dtmin;
         r_ws[warp] = wsmax;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) { r_sqf[warp][v] = sqf[v]; r_sqd[warp][v] = sqd[v]; }
+        for (int v = 0; v < 4; ++v) r_sqd[warp][v] = sqd[v];
     }
     __syncthreads();
     if (tid == 0) {
-        float dm = r_dt[0], wm = r_ws[0], sf[4];
+        float dm = r_dt[0], wm = r_ws[0];
         double sd[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) { sf[v] = r_sqf[0][v]; sd[v] = r_sqd[0][v]; }
+        for (int v = 0; v < 4; ++v) sd[v] = r_sqd[0][v];
         for (int w = 1; w < kThreads / 32; ++w) {
-            dm = fmn(dm, r_dt[w]);
-            wm = fmx(wm, r_ws[w]);
+            dm = fminf(dm, r_dt[w]);
+            wm = fmaxf(wm, r_ws[w]);
 #pragma unroll
-            for (int v = 0; v < 4; ++v) { sf[v] += r_sqf[w][v]; sd[v] += r_sqd[w][v]; }
+            for (int v = 0; v < 4; ++v) sd[v] += r_sqd[w][v];
         }
         g.part_dt[tile] = dm;
         g.part_ws[tile] = wm;
@@ -311,27 +472,27 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
         atomicMax(g.ctrl + kDtKey, 0xffffffffu - __float_as_uint(dm));
         atomicMax(g.ctrl + kWsBits, __float_as_uint(wm));
 #pragma unroll
-        for (int v = 0; v < 4; ++v) atomicAdd(reinterpret_cast<float*>(g.ctrl + kSq0 + v), sf[v]);
+        for (int v = 0; v < 4; ++v) atomicAdd(reinterpret_cast<float*>(g.ctrl + kSq0 + v), float(sd[v]));
         __threadfence();
         s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(g.tiles - 1);
     }
     __syncthreads();
     if (!s_last) return;
 
-    // 6. the last tile: deterministic reductions of the per-tile partials in tile order, and the error stage
+    // 5. the last tile: deterministic reductions of the per-tile partials in tile order, and the error stage
     __threadfence();
     float dm = 3.0e38f, wm = 0.0f;
     double sd[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t t = tid; t < g.tiles; t += kThreads) {
-        dm = fmn(dm, __ldcg(g.part_dt + t));
-        wm = fmx(wm, __ldcg(g.part_ws + t));
+        dm = fminf(dm, __ldcg(g.part_dt + t));
+        wm = fmaxf(wm, __ldcg(g.part_ws + t));
 #pragma unroll
         for (int v = 0; v < 4; ++v) sd[v] += __ldcg(g.part_sq + t * 4 + v);
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
-        dm = fmn(dm, __shfl_xor_sync(0xffffffffu, dm, off));
-        wm = fmx(wm, __shfl_xor_sync(0xffffffffu, wm, off));
+        dm = fminf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
+        wm = fmaxf(wm, __shfl_xor_sync(0xffffffffu, wm, off));
 #pragma unroll
         for (int v = 0; v < 4; ++v) sd[v] += __shfl_xor_sync(0xffffffffu, sd[v], off);
     }
@@ -349,8 +510,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) DetSq[v] = r_sqd[0][v];
         for (int w = 1; w < kThreads / 32; ++w) {
-            DetDt = fmn(DetDt, r_dt[w]);
-            DetWs = fmx(DetWs, r_ws[w]);
+            DetDt = fminf(DetDt, r_dt[w]);
+            DetWs = fmaxf(DetWs, r_ws[w]);
 #pragma unroll
             for (int v = 0; v < 4; ++v) DetSq[v] += r_sqd[w][v];
         }
@@ -441,6 +602,7 @@ int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream) {
     if (int64_t(d->nx) * d->ny > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
     if (d->limiter != 0 && d->limiter != 1) return CSPB_ERR_UNSUPPORTED;
     if (d->walls != 0 && d->walls != 1) return CSPB_ERR_ARGUMENT;
+    if ((d->flags & ~CSPB_NS_REFERENCE_ROUNDING) != 0 || d->reserved != 0) return CSPB_ERR_ARGUMENT;
     const NscLayout L = nsc_layout(d->nx, d->ny);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
     if (L.tiles > 0x7fffffff) return CSPB_ERR_ARGUMENT;
@@ -462,7 +624,9 @@ int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream) {
     g.part_ws = reinterpret_cast<float*>(ws + L.off_ws);
     g.part_sq = reinterpret_cast<double*>(ws + L.off_sq);
     const size_t smem = sizeof(nsc::Smem);
-    auto kern = d->limiter == 0 ? nsc::k_ns_comp<0> : nsc::k_ns_comp<1>;
+    const bool exact = (d->flags & CSPB_NS_REFERENCE_ROUNDING) != 0;
+    auto kern = d->limiter == 0 ? (exact ? nsc::k_ns_comp<0, true> : nsc::k_ns_comp<0, false>)
+                                : (exact ? nsc::k_ns_comp<1, true> : nsc::k_ns_comp<1, false>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return CSPB_ERR_CUDA;
     kern<<<unsigned(L.tiles), nsc::kThreads, smem, st>>>(g);

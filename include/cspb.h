@@ -299,10 +299,18 @@ int cspb_gemver_tasks(const cspb_gemver_task* tasks, int64_t count, int64_t max_
  *   [12..17] err.Err = atomic - deterministic: [dt, ws, sq0..sq3]
  * det_sq64 (device, 4 doubles, may be NULL) receives the f64 sums of R² before rounding.
  * ================================================================================================================== */
+/* flags = CSPB_NS_REFERENCE_ROUNDING: the reference's formulas in their written order with every multiply and add
+ * rounded separately (no fused multiply-add) and IEEE division and square root, so that R, min dt and max wave speed are
+ * bit-identical to a sequential f32 evaluation of physics.hpp. The default (flags = 0) uses fused multiply-adds and
+ * approximate reciprocals, divisions and reciprocal square roots in the face fluxes: faster, as close to the f64
+ * reference, not the same bits. */
+#define CSPB_NS_REFERENCE_ROUNDING 1
 typedef struct cspb_ns_comp_desc {
     int32_t nx, ny;      /* >= 4 each */
     int32_t limiter;     /* 0 minmod, 1 van Leer */
     int32_t walls;       /* 1: no-slip adiabatic walls in y; 0: periodic in y. x is always periodic. */
+    int32_t flags;       /* 0 or CSPB_NS_REFERENCE_ROUNDING */
+    int32_t reserved;    /* 0 */
     const float* U;
     float* R;
     float* diag;         /* 18 floats */
