@@ -410,12 +410,15 @@ def bench_ns(torch, cb, dist, args):
     R = torch.empty_like(Uc)
     diag = torch.empty(18, dtype=torch.float32, device=dev)
     sq = torch.empty(4, dtype=torch.float64, device=dev)
-    for bc in ("walls", "periodic"):
+    for bc, lim, exact in (("walls", "minmod", False), ("periodic", "minmod", False), ("walls", "vanleer", False),
+                           ("walls", "minmod", True), ("walls", "vanleer", True)):
         def stepc():
-            cb.ns_compressible(Uc, limiter="minmod", bc=bc, R=R, diag=diag, det_sq64=sq, workspace=ws)
+            cb.ns_compressible(Uc, limiter=lim, bc=bc, R=R, diag=diag, det_sq64=sq, workspace=ws,
+                               reference_rounding=exact)
         msc = timed(torch, dist, stepc, args.steps, args.warmup)
-        res[f"compressible_{bc}_minmod"] = {"grid": N, "ms": msc, "gbs_nominal": 32.0 * N * N / (msc * 1e-3) / 1e9,
-                                            "reference_rtx4090_handwritten_ms": 3.550 if bc == "walls" else None}
+        key = f"compressible_{bc}_{lim}" + ("_reference_rounding" if exact else "")
+        res[key] = {"grid": N, "ms": msc, "gbs_nominal": 32.0 * N * N / (msc * 1e-3) / 1e9,
+                    "reference_rtx4090_handwritten_ms": 3.550 if (bc == "walls" and lim == "minmod") else None}
     del Uc, R
     torch.cuda.empty_cache()
     return res
@@ -533,17 +536,21 @@ def bench_reference_programs(args):
 
 
 # ---- the CPU path ---------------------------------------------------------------------------------------------
-def cpu_gemver(n: int, target_s: float = 3.0, reps: int = 3) -> dict:
-    """The reference's unfused GEMVER component loops in f32 (oracle port, OpenMP, every host thread) on a bounded
-    sample of the n = 16384 workload: a band of rows sized to ~target_s per run, up to the whole matrix. Returns GB/s
-    of the same algorithmic traffic per row."""
+def cpu_gemver(n: int, target_s: float = 2.0, reps: int = 5, warmup: int = 2) -> dict:
+    """The reference's unfused GEMVER component loops in f32 (oracle port, OpenMP, every host thread, threads bound to
+    cores) on a bounded sample of the n = 16384 workload: a band of rows sized to ~target_s per run, up to the whole
+    matrix. The reference's own protocol (examples/run_benchmarks.nu:9-22): warm-up runs, then `reps` timed runs,
+    median with min and max. Returns GB/s of the same algorithmic traffic per row."""
+    import os
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
     import numpy as np
     import oracle
     lib = oracle.restatement()
     A = np.empty(n * n, dtype=np.float32)
     lib.orc_fill_hash(A.ctypes.data_as(__import__("ctypes").c_void_p), n * n, 0, 1, 0)
     vecs = [oracle.hash_fill(n, s, 1) for s in range(2, 8)]
-    B = np.empty(n * n, dtype=np.float32)
+    B = np.zeros(n * n, dtype=np.float32)  # touched here, not inside a timed run
     x = np.empty(n, dtype=np.float32)
     w = np.empty(n, dtype=np.float32)
     P = lambda a: a.ctypes.data_as(__import__("ctypes").c_void_p)  # noqa: E731
@@ -560,12 +567,17 @@ def cpu_gemver(n: int, target_s: float = 3.0, reps: int = 3) -> dict:
         t = run(rows)
     if t < target_s and rows < n:
         rows = min(n, int(rows * target_s / max(t, 1e-3)) // 64 * 64 or 64)
-    times = [run(rows) for _ in range(reps)]
+    for _ in range(max(0, warmup)):
+        run(rows)
+    times = [run(rows) for _ in range(max(1, reps))]
     tmed = statistics.median(times)
     bytes_ = 12.0 * rows * n + 32.0 * n
     return {"value": bytes_ / tmed / 1e9, "unit": "GB/s", "cores": oracle.threads(), "kind": "port",
-            "sample": f"rows 0..{rows} of the n={n} f32 GEMVER (A, Â, Â re-read of those rows), median of {reps}",
-            "seconds_per_sample": tmed}
+            "sample": f"rows 0..{rows} of the n={n} f32 GEMVER (A, Â, Â re-read of those rows); {warmup} warm-up "
+                      f"runs, median of {len(times)} timed runs",
+            "seconds_per_sample": tmed, "runs": len(times),
+            "min_max_gbs": [bytes_ / max(times) / 1e9, bytes_ / min(times) / 1e9],
+            "omp": {"OMP_PROC_BIND": os.environ.get("OMP_PROC_BIND"), "OMP_PLACES": os.environ.get("OMP_PLACES")}}
 
 
 # ---- main -------------------------------------------------------------------------------------------------------
@@ -600,7 +612,8 @@ def main(argv=None) -> int:
     if args.impl == "reference":
         if dist.rank != 0:
             return 0
-        cpu = cpu_gemver(args.n, target_s=2.0, reps=max(1, min(args.steps, 3)))
+        # K timed samples of ~1 s each after W warm-up samples (W capped at 3): the run stays within a few minutes
+        cpu = cpu_gemver(args.n, target_s=1.0, reps=args.steps, warmup=min(args.warmup, 3))
         line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "GB/s", "n_gpus": dist.world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["seconds_per_sample"] * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -32,8 +32,13 @@ PROGRAMS = {
 }
 
 
+def default_reference() -> Path:
+    """The reference checkout when none is named: a sibling of this repository called `reference`."""
+    return PKG.parent.parent / "reference"
+
+
 def build_examples(reference: str | os.PathLike | None = None, verbose: bool = False) -> dict[str, Path]:
-    ref = Path(reference or os.environ.get("CSPB_REFERENCE_DIR", "/root/reference"))
+    ref = Path(reference or os.environ.get("CSPB_REFERENCE_DIR") or default_reference())
     if not (ref / "examples").is_dir():
         raise FileNotFoundError(f"no reference tree at {ref}")
     built = {}
