@@ -424,6 +424,64 @@ def bench_ns(torch, cb, dist, args):
     return res
 
 
+def bench_scan(torch, cb, dist, args, peak):
+    """The single-pass decoupled-lookback scan (cspb_exclusive_scan_u32 / _u64) and the fused ragged-column builder
+    (cspb_build_column, counts mode from i32) at 2^28 items: algorithmic bytes 8 B/item (u32 in, u32 out), 16 B/item
+    (u64) and 12 B/item (i32 counts in, u32 extents and u32 offsets out). Inputs are 1..2 GiB, larger than L2."""
+    import ctypes
+    from cospanmdao_b200 import _capi
+    n = 1 << 28
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = cb.lib()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ws = cb.Workspace(dev)
+    wp, wb = ws.ptr(lib.cspb_scan_workspace_bytes(n))
+    res = {}
+    g = torch.Generator(device=dev).manual_seed(0)
+    for name, dt, fn, bpi in (("scan_u32", torch.int32, lib.cspb_exclusive_scan_u32, 8.0),
+                              ("scan_u64", torch.int64, lib.cspb_exclusive_scan_u64, 16.0)):
+        vals = torch.randint(0, 1000, (n,), dtype=dt, device=dev, generator=g)
+        out = torch.empty(n + 1, dtype=dt, device=dev)
+
+        def step():
+            rc = fn(ctypes.c_void_p(vals.data_ptr()), ctypes.c_void_p(out.data_ptr()), n, wp, wb, st)
+            if rc != 0:
+                raise RuntimeError(f"{name}: {rc}")
+
+        ms = timed(torch, dist, step, args.steps, args.warmup)
+        # bit-exact check of the last step against torch's cumsum (int64: exact for these values)
+        mask = 0xffffffff if dt == torch.int32 else -1
+        want = torch.cumsum(vals.to(torch.int64), 0)
+        ok = bool(torch.equal(out[1:].to(torch.int64) & mask, want & mask)) and int(out[0]) == 0
+        gbs = bpi * n / (ms * 1e-3) / 1e9
+        res[name] = {"items": n, "ms": ms, "gbs": gbs, "frac_of_measured_hbm": gbs / peak["hbm_gbs"],
+                     "bytes_per_item": bpi, "bit_exact_vs_cumsum": ok}
+        del vals, out, want
+        torch.cuda.empty_cache()
+    counts = torch.randint(0, 16, (n,), dtype=torch.int32, device=dev, generator=g)
+    ext = torch.empty(n, dtype=torch.int32, device=dev)
+    offs = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    tf = torch.empty(2, dtype=torch.int32, device=dev)
+
+    def stepc():
+        rc = lib.cspb_build_column(ctypes.c_void_p(counts.data_ptr()), _capi.I32, n, 1, 0,
+                                   ctypes.c_void_p(ext.data_ptr()), ctypes.c_void_p(offs.data_ptr()),
+                                   ctypes.c_void_p(tf.data_ptr()), wp, wb, st)
+        if rc != 0:
+            raise RuntimeError(f"build_column: {rc}")
+
+    ms = timed(torch, dist, stepc, args.steps, args.warmup)
+    want = torch.cumsum(counts.to(torch.int64), 0)
+    ok = bool(torch.equal(offs[1:].to(torch.int64) & 0xffffffff, want & 0xffffffff)) and \
+        int(tf[0]) & 0xffffffff == int(want[-1]) & 0xffffffff and int(tf[1]) == 0
+    gbs = 12.0 * n / (ms * 1e-3) / 1e9
+    res["build_column_i32"] = {"items": n, "ms": ms, "gbs": gbs, "frac_of_measured_hbm": gbs / peak["hbm_gbs"],
+                               "bytes_per_item": 12.0, "bit_exact_vs_cumsum": ok}
+    del counts, ext, offs, want
+    torch.cuda.empty_cache()
+    return res
+
+
 def bench_ragged(torch, cb, dist, args, peak):
     """4096 independent GEMVERs, n ~ log-U[64, 4096], f32, packed, in one persistent launch with device-scanned u64
     offsets, replayed as a CUDA graph; the tile geometry per size bucket picked by the autotuner."""
@@ -598,7 +656,7 @@ def main(argv=None) -> int:
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving stream")
     ap.add_argument("--max-batch", type=int, default=512, help="serving: requests per batch at most")
     ap.add_argument("--only", default="", help="comma list of secondary workloads to run (gemver_bf16_storage, "
-                    "gemver_chain, ns_residual, ragged_batch, serving, reference_programs); default all, none with "
+                    "gemver_chain, ns_residual, ragged_batch, scan, serving, reference_programs); default all, none with "
                     "--quick")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)
@@ -659,6 +717,7 @@ def main(argv=None) -> int:
         "ns_sharded": lambda: bench_ns_sharded(torch, cb, dist, args),
         "ns_residual": lambda: bench_ns(torch, cb, dist, args),
         "ragged_batch": lambda: bench_ragged(torch, cb, dist, args, pk),
+        "scan": lambda: bench_scan(torch, cb, dist, args, pk),
         "serving": lambda: bench_serving(torch, dist, args),
         "reference_programs": lambda: bench_reference_programs(args),
     }

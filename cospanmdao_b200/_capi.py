@@ -110,6 +110,12 @@ class NsCompDesc(C.Structure):
                 ("det_sq64", vp), ("workspace", vp), ("workspace_bytes", sz)]
 
 
+class NsCompSlabDesc(C.Structure):
+    _fields_ = [("nx", i32), ("rows", i32), ("limiter", i32), ("walls", i32), ("flags", i32), ("edges", i32),
+                ("U", vp), ("halo_lo", vp), ("halo_hi", vp), ("R", vp), ("diag", vp), ("det_sq64", vp),
+                ("workspace", vp), ("workspace_bytes", sz)]
+
+
 class NsIncompDesc(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("dtype", i32), ("flags", i32), ("h", C.c_double), ("nu", C.c_double),
                 ("u", vp), ("v", vp), ("p", vp), ("ru", vp), ("rv", vp), ("rc", vp), ("norms", vp),
@@ -140,6 +146,8 @@ PROTOTYPES = {
     "cspb_ns_incomp_tasks": (C.c_int, [vp, i64, i64, i32, vp, sz, vp]),
     "cspb_ns_comp_workspace_bytes": (sz, [i32, i32]),
     "cspb_ns_compressible": (C.c_int, [C.POINTER(NsCompDesc), vp]),
+    "cspb_ns_comp_slab_workspace_bytes": (sz, [i32, i32]),
+    "cspb_ns_comp_slab": (C.c_int, [C.POINTER(NsCompSlabDesc), vp]),
     "cspb_ns_init_cons": (C.c_int, [vp, i32, i32, C.c_float, vp]),
     "cspb_ns_incomp_workspace_bytes": (sz, [i32, i32]),
     "cspb_ns_incompressible": (C.c_int, [C.POINTER(NsIncompDesc), vp]),

@@ -19,47 +19,13 @@
 #pragma once
 
 #include "rowpass.cuh"
+#include "mbar.cuh"
 
 namespace cspb {
 
 constexpr int kBulkThreads = kPassThreads + 32;  // 8 consumer warps + 1 producer warp
 constexpr int kStageRows = 32;                   // 8 rows of each of the 4 warp rows (WX = 2)
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of `parity`; false when the budget ran out or another thread gave up first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag,
-                                          uint32_t* ctrl) {
-    if (mbar_test(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (;;) {
-        if (mbar_test(bar, parity)) return true;
-        if (*abort_flag || status_bad(ctrl)) return false;
-        if (globaltimer_ns() - t0 > kWaitBudgetNs) {
-            set_status(ctrl, CSPB_DEV_TIMEOUT);
-            return false;
-        }
-    }
-}
 // One bulk copy global -> this CTA's shared memory, completing on `bar` (16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t policy) {
     asm volatile(

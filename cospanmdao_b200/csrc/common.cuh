@@ -52,6 +52,15 @@ __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void st_release64(uint64_t* p, uint64_t v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
+// Single-copy-atomic 64-bit accesses at GPU scope, for words that carry a flag and a value together.
+__device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
     return *reinterpret_cast<const volatile uint32_t*>(p);
 }

@@ -1,0 +1,70 @@
+// mbar.cuh — mbarrier and tensor-map (TMA) helpers shared by the kernels that stage data through shared memory with
+// asynchronous bulk copies. Every wait is bounded (common.cuh).
+#pragma once
+
+#include <cuda.h>
+
+#include "common.cuh"
+
+namespace cspb {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase of `parity`; false when the budget ran out or another thread gave up first.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort_flag,
+                                          uint32_t* ctrl) {
+    if (mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
+        if (mbar_test(bar, parity)) return true;
+        if (*abort_flag || status_bad(ctrl)) return false;
+        if (globaltimer_ns() - t0 > kWaitBudgetNs) {
+            set_status(ctrl, CSPB_DEV_TIMEOUT);
+            return false;
+        }
+    }
+}
+// One tiled tensor copy (TMA) of a 2D box at element coordinates (x, y) of `map` into this CTA's shared memory,
+// completing on `bar`. x times the element size must be a multiple of 16 bytes; the map covers this GPU's own memory.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before later async-proxy (TMA) ones.
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+}  // namespace cspb
+
+namespace cspb_host {
+
+// A 2D tiled tensor map over a row-major (rows, cols) array of 4-byte (f32) or 2-byte (bf16) elements with row pitch
+// `pitch_elems`, boxes of (box_cols, box_rows) elements, zero fill outside the array. Encoded through the driver's
+// cuTensorMapEncodeTiled, found with cudaGetDriverEntryPoint (the library links no driver library). false when the
+// driver refuses the arguments (base not 16-byte aligned, pitch not a multiple of 16 bytes, box too large).
+bool encode_tensor_map_2d(CUtensorMap* map, const void* base, bool bf16, uint64_t cols, uint64_t rows,
+                          uint64_t pitch_elems, uint32_t box_cols, uint32_t box_rows);
+
+}  // namespace cspb_host

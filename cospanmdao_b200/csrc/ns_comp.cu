@@ -280,6 +280,11 @@ struct K {
     int nx, ny, walls, tiles_x;
     int64_t tiles;
     const float* U;
+    // a y-slab of a larger grid: an edge whose bit is set in `edges` (1: below row 0, 2: above row ny - 1) is interior,
+    // and its two rows of each field come from halo_lo / halo_hi, (4, 2, nx) each, instead of the boundary rule
+    const float* halo_lo;
+    const float* halo_hi;
+    int edges;
     float* R;
     float* diag;
     double* det_sq64;
@@ -328,19 +333,26 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
         const int is = unsigned(i) < unsigned(g.nx) ? i : wrapi(i, g.nx);  // only halo columns wrap
         int js = j;
         float sg = 1.0f;
+        const float* src = g.U;
+        int64_t fs = plane;  // between the fields of src
         if (j < 0 || j >= g.ny) {
-            if (g.walls) {
-                js = j < 0 ? -1 - j : 2 * g.ny - 1 - j;
+            const bool lo = j < 0;
+            if (g.edges & (lo ? 1 : 2)) {  // a slab's interior edge: the neighbour's rows
+                src = lo ? g.halo_lo : g.halo_hi;
+                fs = 2 * int64_t(g.nx);
+                js = lo ? j + 2 : j - g.ny;
+            } else if (g.walls) {
+                js = lo ? -1 - j : 2 * g.ny - 1 - j;
                 sg = -1.0f;
             } else {
                 js = wrapi(j, g.ny);
             }
         }
         const int64_t c = int64_t(js) * g.nx + is;
-        const float r = __ldg(g.U + c);
-        const float mu = __ldg(g.U + plane + c) * sg;  // a sign flip: exact
-        const float mv = __ldg(g.U + 2 * plane + c) * sg;
-        const float E = __ldg(g.U + 3 * plane + c);
+        const float r = __ldg(src + c);
+        const float mu = __ldg(src + fs + c) * sg;  // a sign flip: exact
+        const float mv = __ldg(src + 2 * fs + c) * sg;
+        const float E = __ldg(src + 3 * fs + c);
         float u, v, p, T;
         if constexpr (X) {
             u = __fdiv_rn(mu, r);
@@ -601,41 +613,75 @@ size_t cspb_ns_comp_workspace_bytes(int32_t nx, int32_t ny) {
     return nsc_layout(nx, ny).total;
 }
 
-int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream) {
-    if (!d) return CSPB_ERR_ARGUMENT;
-    if (d->nx < 4 || d->ny < 4 || !d->U || !d->R || !d->diag) return CSPB_ERR_ARGUMENT;
-    if (int64_t(d->nx) * d->ny > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
-    if (d->limiter != 0 && d->limiter != 1) return CSPB_ERR_UNSUPPORTED;
-    if (d->walls != 0 && d->walls != 1) return CSPB_ERR_ARGUMENT;
-    if ((d->flags & ~CSPB_NS_REFERENCE_ROUNDING) != 0 || d->reserved != 0) return CSPB_ERR_ARGUMENT;
-    const NscLayout L = nsc_layout(d->nx, d->ny);
-    if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
+}  // extern "C"
+
+namespace {
+
+// One launch over ny × nx cells (a whole grid, or a slab when edges != 0).
+int launch_ns_comp(int nx, int ny, int limiter, int walls, int flags, const float* U, const float* halo_lo,
+                   const float* halo_hi, int edges, float* R, float* diag, double* det_sq64, void* workspace,
+                   size_t workspace_bytes, cudaStream_t st) {
+    if (limiter != 0 && limiter != 1) return CSPB_ERR_UNSUPPORTED;
+    if (walls != 0 && walls != 1) return CSPB_ERR_ARGUMENT;
+    if ((flags & ~CSPB_NS_REFERENCE_ROUNDING) != 0) return CSPB_ERR_ARGUMENT;
+    if (int64_t(nx) * ny > (int64_t(1) << 31)) return CSPB_ERR_ARGUMENT;
+    const NscLayout L = nsc_layout(nx, ny);
+    if (!workspace || !aligned(workspace, 256) || workspace_bytes < L.total) return CSPB_ERR_WORKSPACE;
     if (L.tiles > 0x7fffffff) return CSPB_ERR_ARGUMENT;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    char* ws = static_cast<char*>(d->workspace);
+    char* ws = static_cast<char*>(workspace);
     if (cudaMemsetAsync(ws, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
     nsc::K g{};
-    g.nx = d->nx;
-    g.ny = d->ny;
-    g.walls = d->walls;
+    g.nx = nx;
+    g.ny = ny;
+    g.walls = walls;
     g.tiles_x = L.tiles_x;
     g.tiles = L.tiles;
-    g.U = d->U;
-    g.R = d->R;
-    g.diag = d->diag;
-    g.det_sq64 = d->det_sq64;
+    g.U = U;
+    g.halo_lo = halo_lo;
+    g.halo_hi = halo_hi;
+    g.edges = edges;
+    g.R = R;
+    g.diag = diag;
+    g.det_sq64 = det_sq64;
     g.ctrl = reinterpret_cast<uint32_t*>(ws);
     g.part_dt = reinterpret_cast<float*>(ws + L.off_dt);
     g.part_ws = reinterpret_cast<float*>(ws + L.off_ws);
     g.part_sq = reinterpret_cast<double*>(ws + L.off_sq);
     const size_t smem = sizeof(nsc::Smem);
-    const bool exact = (d->flags & CSPB_NS_REFERENCE_ROUNDING) != 0;
-    auto kern = d->limiter == 0 ? (exact ? nsc::k_ns_comp<0, true> : nsc::k_ns_comp<0, false>)
-                                : (exact ? nsc::k_ns_comp<1, true> : nsc::k_ns_comp<1, false>);
+    const bool exact = (flags & CSPB_NS_REFERENCE_ROUNDING) != 0;
+    auto kern = limiter == 0 ? (exact ? nsc::k_ns_comp<0, true> : nsc::k_ns_comp<0, false>)
+                             : (exact ? nsc::k_ns_comp<1, true> : nsc::k_ns_comp<1, false>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
         return CSPB_ERR_CUDA;
     kern<<<unsigned(L.tiles), nsc::kThreads, smem, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    if (d->nx < 4 || d->ny < 4 || !d->U || !d->R || !d->diag) return CSPB_ERR_ARGUMENT;
+    if (d->reserved != 0) return CSPB_ERR_ARGUMENT;
+    return launch_ns_comp(d->nx, d->ny, d->limiter, d->walls, d->flags, d->U, nullptr, nullptr, 0, d->R, d->diag,
+                          d->det_sq64, d->workspace, d->workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+size_t cspb_ns_comp_slab_workspace_bytes(int32_t nx, int32_t rows) {
+    if (nx < 4 || rows < 2) return 0;
+    return nsc_layout(nx, rows).total;
+}
+
+int cspb_ns_comp_slab(const cspb_ns_comp_slab_desc* d, void* stream) {
+    if (!d) return CSPB_ERR_ARGUMENT;
+    if (d->nx < 4 || d->rows < 2 || !d->U || !d->R || !d->diag) return CSPB_ERR_ARGUMENT;
+    if ((d->edges & ~3) != 0 || ((d->edges & 1) && !d->halo_lo) || ((d->edges & 2) && !d->halo_hi))
+        return CSPB_ERR_ARGUMENT;
+    return launch_ns_comp(d->nx, d->rows, d->limiter, d->walls, d->flags, d->U, d->halo_lo, d->halo_hi, d->edges,
+                          d->R, d->diag, d->det_sq64, d->workspace, d->workspace_bytes,
+                          static_cast<cudaStream_t>(stream));
 }
 
 int cspb_ns_init_cons(float* U, int32_t nx, int32_t ny, float amp, void* stream) {

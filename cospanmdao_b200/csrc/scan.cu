@@ -4,8 +4,11 @@
 // reduce-then-scan of 3 kernels per level with temporary allocations, by ONE launch over tiles of 256 threads × ITEMS:
 //   1. a tile takes a dynamic tile index (so every tile it waits on has started), loads its items coalesced through
 //      shared memory, and scans them in the block;
-//   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 32 at a time, adding
-//      aggregates until it meets a published inclusive prefix (flag 2), and publishes its own inclusive prefix;
+//   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 256 at a time (8 per lane,
+//      flag and value in one 64-bit word, so one round is one L2 round trip), adding aggregates until it meets a
+//      published inclusive prefix (flag 2), and publishes its own inclusive prefix. At B200's bandwidth a tile starts
+//      every few nanoseconds, so a look-back window of 32 tiles (two dependent loads per round: flag, then value)
+//      rarely reached a published prefix and walked back through hundreds of tiles;
 //   3. it writes its outputs coalesced; the last tile writes out[n], the total.
 // Integer addition mod 2^32 / 2^64 is associative, so the result is bit-identical to std::exclusive_scan whatever the
 // order of the lookback. Every wait is bounded (common.cuh).
@@ -33,33 +36,33 @@ struct ScanSrc {
     uint32_t* extents;  // column: the narrowed values are written here
 };
 
-// The value of item i (always < n), and the flag bits it raises.
+// Item i of the source (always < n), read through the read-only global path: a column source's raw value widened to
+// 64 bits, a plain source's value.
 template <typename T>
-__device__ __forceinline__ T scan_item(const ScanSrc& s, int64_t i, uint32_t& flag) {
-    if (!s.column) return static_cast<const T*>(s.in)[i];
-    uint32_t x = 0;
+__device__ __forceinline__ T load_plain(const ScanSrc& s, int64_t i) {
+    return __ldg(static_cast<const T*>(s.in) + i);
+}
+__device__ __forceinline__ uint64_t load_column(const ScanSrc& s, int64_t i) {
     switch (s.dtype) {
-        case CSPB_I32: {
-            const int32_t v = static_cast<const int32_t*>(s.in)[i * s.k];
-            if (v < 0) flag |= 1u; else x = uint32_t(v);
-            break;
-        }
-        case CSPB_U32: x = static_cast<const uint32_t*>(s.in)[i * s.k]; break;
-        case CSPB_I64: {
-            const int64_t v = static_cast<const int64_t*>(s.in)[i * s.k];
-            if (v < 0) flag |= 1u;
-            else if (v > int64_t(0xffffffffll)) flag |= 2u;
-            else x = uint32_t(v);
-            break;
-        }
-        default: {
-            const uint64_t v = static_cast<const uint64_t*>(s.in)[i * s.k];
-            if (v > 0xffffffffull) flag |= 2u; else x = uint32_t(v);
-            break;
-        }
+        case CSPB_I32: return uint64_t(int64_t(__ldg(static_cast<const int32_t*>(s.in) + i * s.k)));
+        case CSPB_U32: return uint64_t(__ldg(static_cast<const uint32_t*>(s.in) + i * s.k));
+        case CSPB_I64: return uint64_t(__ldg(reinterpret_cast<const long long*>(s.in) + i * s.k));
+        default: return uint64_t(__ldg(reinterpret_cast<const unsigned long long*>(s.in) + i * s.k));
     }
-    s.extents[i] = x;
-    return T(x);
+}
+// A column value narrowed to u32 (cs::detail::build_column's rule): negative -> 0 and flag 1, past 32 bits -> 0 and
+// flag 2 (the signed dtypes were sign-extended by load_column).
+__device__ __forceinline__ uint32_t narrow(int32_t dtype, uint64_t raw, uint32_t& flag) {
+    const bool sgn = dtype == CSPB_I32 || dtype == CSPB_I64;
+    if (sgn && int64_t(raw) < 0) {
+        flag |= 1u;
+        return 0u;
+    }
+    if (raw > 0xffffffffull) {
+        flag |= 2u;
+        return 0u;
+    }
+    return uint32_t(raw);
 }
 
 template <typename T>
@@ -70,11 +73,44 @@ struct ScanK {
     int64_t n;
     int64_t tiles;
     uint32_t* ctrl;
-    uint32_t* tflag;    // per tile: 0 nothing, 1 aggregate, 2 inclusive prefix
-    T* tagg;
-    T* tinc;
+    uint64_t* tstat;    // per tile: its status words (TileStat<T>)
     uint32_t* total_flag;  // column mode: [total, flag]
 };
+
+// A tile's published state: flag (0 nothing, 1 aggregate, 2 inclusive prefix) and value in single 64-bit words, so a
+// reader gets both with one load and needs no fence between them. u32: one word, flag in the high half. u64: two
+// words (the value's low and high halves), each with the flag in its high half; a reader takes the pair only when both
+// flags agree (a pair caught between two stores is read again).
+template <typename T> struct TileStat;
+template <> struct TileStat<uint32_t> {
+    static constexpr int kWords = 1;
+    static __device__ __forceinline__ void put(uint64_t* w, uint32_t flag, uint32_t v) {
+        st_relaxed64(w, (uint64_t(flag) << 32) | v);
+    }
+    static __device__ __forceinline__ uint32_t get(const uint64_t* w, uint32_t& v) {
+        const uint64_t a = ld_relaxed64(w);
+        v = uint32_t(a);
+        return uint32_t(a >> 32);
+    }
+};
+template <> struct TileStat<uint64_t> {
+    static constexpr int kWords = 2;
+    static __device__ __forceinline__ void put(uint64_t* w, uint32_t flag, uint64_t v) {
+        st_relaxed64(w, (uint64_t(flag) << 32) | (v & 0xffffffffull));
+        st_relaxed64(w + 1, (uint64_t(flag) << 32) | (v >> 32));
+    }
+    static __device__ __forceinline__ uint32_t get(const uint64_t* w, uint64_t& v) {
+        const uint64_t a = ld_relaxed64(w), b = ld_relaxed64(w + 1);
+        v = (b << 32) | (a & 0xffffffffull);
+        const uint32_t fa = uint32_t(a >> 32), fb = uint32_t(b >> 32);
+        return fa == fb ? fa : 0u;
+    }
+};
+
+// Predecessors each lane of the looking-back warp reads per round: one round covers 32·kLook tiles, so the
+// look-back reaches a published prefix in one L2 round trip even when hundreds of tiles are in flight (u64 reads two
+// words per tile: 4 tiles a lane keep its registers at the u32 count).
+template <typename T> inline constexpr int kLook = 8 / TileStat<T>::kWords;
 
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
@@ -88,7 +124,7 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
+__global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
     constexpr int IT = ScanItems<T>::N;
     constexpr int TILE = kScanThreads * IT;
     constexpr int PAD = TILE + TILE / 32;
@@ -103,13 +139,40 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
     if (t == 0) s_flag = 0;
     const int64_t base = int64_t(tile) * TILE;
 
-    // 1. striped coalesced load -> shared (padded) -> blocked items
+    // 1. striped coalesced load -> shared (padded) -> blocked items. Every load of the tile is issued before the first
+    // store: the loads go through the read-only global path into registers, then the stores follow (a load through a
+    // generic pointer, stored to shared memory in the same loop, could not be moved past the previous store).
     uint32_t flag = 0;
+    if (!g.src.column) {
+        T x[IT];
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-        const int idx = k * kScanThreads + t;
-        const int64_t i = base + idx;
-        sm[idx + idx / 32] = i < g.n ? scan_item<T>(g.src, i, flag) : T(0);
+        for (int k = 0; k < IT; ++k) {
+            const int64_t i = base + k * kScanThreads + t;
+            x[k] = i < g.n ? load_plain<T>(g.src, i) : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int idx = k * kScanThreads + t;
+            sm[idx + idx / 32] = x[k];
+        }
+    } else {
+        uint64_t raw[IT];
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int64_t i = base + k * kScanThreads + t;
+            raw[k] = i < g.n ? load_column(g.src, i) : 0ull;
+        }
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+            const int idx = k * kScanThreads + t;
+            const int64_t i = base + idx;
+            uint32_t x = 0;
+            if (i < g.n) {
+                x = narrow(g.src.dtype, raw[k], flag);
+                __stcg(g.src.extents + i, x);
+            }
+            sm[idx + idx / 32] = T(x);
+        }
     }
     __syncthreads();
     if (flag) atomicOr(&s_flag, flag);
@@ -134,33 +197,58 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
     const T thread_excl = s_warp[warp] + incl - run;
     __shared__ T s_agg;
     if (t == kScanThreads - 1) s_agg = thread_excl + run;
+    // the tile's exclusive values wait in shared memory (blocked order) during the look-back, not in registers (every
+    // thread's last read of sm was before the barriers above)
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+        const int idx = t * IT + k;
+        sm[idx + idx / 32] = thread_excl + v[k];
+    }
     __syncthreads();
     const T agg = s_agg;
 
     // 2. publish the aggregate, look back, publish the inclusive prefix
     if (warp == 0) {
-        T prefix = 0;
+        using TS = TileStat<T>;
+        constexpr int W = TS::kWords;
+        constexpr int kLook = cspb::kLook<T>;
         if (tile == 0) {
             if (lane == 0) {
-                g.tinc[0] = agg;
-                __threadfence();
-                st_release(g.tflag, 2u);
+                TS::put(g.tstat, 2u, agg);
+                s_prefix = 0;
             }
         } else {
-            if (lane == 0) {
-                g.tagg[tile] = agg;
-                __threadfence();
-                st_release(g.tflag + tile, 1u);
-            }
-            int64_t look = int64_t(tile) - 1;  // the nearest predecessor this window starts at
-            bool done = false;
+            if (lane == 0) TS::put(g.tstat + int64_t(tile) * W, 1u, agg);
+            T prefix = 0;
+            int64_t base = int64_t(tile) - 1;  // the nearest predecessor of this round
             const unsigned long long t0 = globaltimer_ns();
+            bool done = false, gave_up = false;
             while (!done) {
-                const int64_t p = look - lane;  // lane 0 is the nearest
-                uint32_t f = p >= 0 ? ld_acquire(g.tflag + p) : 2u;
-                // wait until every lane of the window has something published (lane 0 decides to give up)
+                // lane l reads predecessors base - (l·kLook + j), j = 0 .. kLook-1 (lane 0 the nearest); a
+                // predecessor before tile 0 reads as an inclusive prefix of 0
+                uint32_t f[kLook];
+                T v[kLook];
+                int first, stop;
                 for (;;) {
-                    if (__all_sync(0xffffffffu, f != 0u)) break;
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j) {
+                        const int64_t p = base - (lane * kLook + j);
+                        if (p >= 0) f[j] = TS::get(g.tstat + p * W, v[j]);
+                        else { f[j] = 2u; v[j] = T(0); }
+                    }
+                    first = kLook;  // this lane's nearest inclusive prefix
+                    bool zero = false;
+#pragma unroll
+                    for (int j = kLook - 1; j >= 0; --j)
+                        if (f[j] == 2u) first = j;
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j)
+                        if (j < first && f[j] == 0u) zero = true;
+                    const unsigned incl = __ballot_sync(0xffffffffu, first < kLook);
+                    stop = incl ? __ffs(incl) - 1 : 32;  // the lane holding the nearest inclusive prefix
+                    // every predecessor up to that prefix must have published at least its aggregate
+                    const bool wait = lane <= stop && zero;
+                    if (!__any_sync(0xffffffffu, wait)) break;
                     int give_up = 0;
                     if (lane == 0) {
                         if (status_bad(g.ctrl)) give_up = 1;
@@ -173,52 +261,45 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanK<T> g) {
                         }
                     }
                     if (__shfl_sync(0xffffffffu, give_up, 0)) {
-                        done = true;
+                        gave_up = true;
                         break;
                     }
-                    __nanosleep(64);
-                    if (f == 0u) f = ld_acquire(g.tflag + p);
+                    __nanosleep(32);
                 }
-                if (done) break;
-                const unsigned incl_mask = __ballot_sync(0xffffffffu, f == 2u);
-                // the nearest lane holding an inclusive prefix: lanes before it contribute aggregates
-                const int stop = incl_mask ? __ffs(incl_mask) - 1 : 32;
+                if (gave_up) break;
                 T c = 0;
-                if (lane < stop) c = p >= 0 ? __ldcg(g.tagg + p) : T(0);
-                else if (lane == stop) c = p >= 0 ? __ldcg(g.tinc + p) : T(0);
+                if (lane < stop) {
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j) c += v[j];
+                } else if (lane == stop) {
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j)
+                        if (j <= first) c += v[j];
+                }
 #pragma unroll
                 for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
                 prefix += c;
-                if (incl_mask) done = true;
-                else look -= 32;
+                if (stop < 32) done = true;
+                else base -= 32 * kLook;
             }
             if (lane == 0) {
-                g.tinc[tile] = prefix + agg;
-                __threadfence();
-                st_release(g.tflag + tile, 2u);
+                if (!gave_up) TS::put(g.tstat + int64_t(tile) * W, 2u, prefix + agg);
                 s_prefix = prefix;
             }
         }
-        if (tile == 0 && lane == 0) s_prefix = 0;
     }
     __syncthreads();
     const T prefix = s_prefix;
 
-    // 3. blocked exclusive values -> shared -> striped coalesced stores
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-        const int idx = t * IT + k;
-        sm[idx + idx / 32] = prefix + thread_excl + v[k];
-    }
-    __syncthreads();
+    // 3. the tile's prefix plus its exclusive values, from shared memory in striped order: coalesced stores
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
         const int idx = k * kScanThreads + t;
         const int64_t i = base + idx;
         if (i < g.n) {
-            const T o = sm[idx + idx / 32];
-            if (g.out32) g.out32[i] = uint32_t(o);
-            else g.out[i] = o;
+            const T o = prefix + sm[idx + idx / 32];
+            if (g.out32) __stcg(g.out32 + i, uint32_t(o));
+            else __stcg(g.out + i, o);
         }
     }
     if (s_flag && t == 0) {
@@ -295,7 +376,7 @@ namespace {
 template <typename T>
 struct ScanLayout {
     int64_t tiles = 0;
-    size_t off_flag = 0, off_agg = 0, off_inc = 0, total = 0;
+    size_t off_stat = 0, total = 0;
 };
 
 template <typename T>
@@ -303,14 +384,8 @@ ScanLayout<T> scan_layout(int64_t n) {
     ScanLayout<T> L;
     const int64_t TILE = int64_t(kScanThreads) * ScanItems<T>::N;
     L.tiles = n <= 0 ? 0 : (n + TILE - 1) / TILE;
-    size_t o = kCtrlBytes;
-    L.off_flag = o;
-    o = align_up(o + size_t(L.tiles) * 4, 256);
-    L.off_agg = o;
-    o = align_up(o + size_t(L.tiles) * sizeof(T), 256);
-    L.off_inc = o;
-    o = align_up(o + size_t(L.tiles) * sizeof(T), 256);
-    L.total = o;
+    L.off_stat = kCtrlBytes;
+    L.total = align_up(kCtrlBytes + size_t(L.tiles) * 8 * TileStat<T>::kWords, 256);
     return L;
 }
 
@@ -320,7 +395,7 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
     const ScanLayout<T> L = scan_layout<T>(n);
     if (!ws || !aligned(ws, 256) || ws_bytes < L.total) return CSPB_ERR_WORKSPACE;
     char* w = static_cast<char*>(ws);
-    cudaError_t e = cudaMemsetAsync(w, 0, L.off_agg, st);  // ctrl + tile flags
+    cudaError_t e = cudaMemsetAsync(w, 0, L.total, st);  // ctrl + tile status words
     if (e != cudaSuccess) return CSPB_ERR_CUDA;
     ScanK<T> g{};
     g.src = src;
@@ -329,9 +404,7 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
     g.n = n;
     g.tiles = L.tiles;
     g.ctrl = reinterpret_cast<uint32_t*>(w);
-    g.tflag = reinterpret_cast<uint32_t*>(w + L.off_flag);
-    g.tagg = reinterpret_cast<T*>(w + L.off_agg);
-    g.tinc = reinterpret_cast<T*>(w + L.off_inc);
+    g.tstat = reinterpret_cast<uint64_t*>(w + L.off_stat);
     g.total_flag = total_flag;
     k_scan<T><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
@@ -417,7 +490,7 @@ namespace {
 constexpr int64_t kStaticTiles = (int64_t(CSPB_BUILD_COLUMN_STATIC_MAX) + kScanThreads * ScanItems<uint64_t>::N - 1) /
                                  (kScanThreads * ScanItems<uint64_t>::N);
 constexpr size_t kStaticScratchBytes =
-    kCtrlBytes + ((size_t(kStaticTiles) * 4 + 255) / 256 * 256) + 2 * ((size_t(kStaticTiles) * 8 + 255) / 256 * 256);
+    kCtrlBytes + (size_t(kStaticTiles) * 8 * TileStat<uint64_t>::kWords + 255) / 256 * 256;
 static_assert(kStaticScratchBytes <= 160 * 1024 + 256, "the fixed scratch stays modest");
 
 static __device__ __align__(256) unsigned char g_column_scratch[kStaticScratchBytes];

@@ -158,3 +158,107 @@ def ns_incompressible_sharded(u, v, p, *, h, nu, ranks=None, workspace=None, str
     up, dn = exchange_halos((u[0], v[0], p[0]), (u[-1], v[-1], p[-1]), ranks)
     ru, rv, rc, sums = ns_incompressible_slab(u, v, p, up, dn, h=h, nu=nu, workspace=workspace, stream=stream)
     return ru, rv, rc, combine_sums(sums, ranks)
+
+
+# ---- the compressible NS residual in y-slabs ----------------------------------------------------------------------
+# Rank r holds rows [r0, r1) of U (4, rows, nx), rows >= 2. The reference's tiles read a 2-cell halo
+# (examples/ns-residual/tile.hpp:39-49), so every rank contributes its first two and its last two rows of the four
+# fields to ONE all-gather (2 · 4 · 2 · nx floats per rank) and takes the previous rank's last two rows (halo_lo) and
+# the next rank's first two (halo_hi). In a periodic grid every edge between ranks is interior, the ranks wrapping
+# around; with walls the first rank's lower edge and the last rank's upper edge take the mirror instead. Each rank runs
+# cspb_ns_comp_slab, whose residual rows are bit-identical to the whole grid's. The diagnostics combine in rank order:
+# min dt and max wave speed exactly, the squared sums added in rank order (an all-gather of each slab's 18
+# diagnostics and 4 f64 sums).
+
+def comp_slab_edges(rank: int, world: int, walls: bool) -> int:
+    """The interior edges of rank `rank`'s slab (bit 1 below, bit 2 above): none for a single slab (the whole grid
+    takes its own boundary rule); with walls, not the grid's first and last edges."""
+    if world == 1:
+        return 0
+    lo = 1 if (not walls or rank > 0) else 0
+    hi = 2 if (not walls or rank < world - 1) else 0
+    return lo | hi
+
+
+def exchange_comp_halos(U, ranks, walls: bool):
+    """U: this rank's slab (4, rows, nx). Returns (halo_lo, halo_hi, edges): the neighbours' two rows of each field
+    ((4, 2, nx) tensors, None where the edge is not interior) and the edge bits for cspb_ns_comp_slab."""
+    import torch
+    if ranks is None or ranks.world == 1:
+        return None, None, 0
+    if U.shape[1] < 2:
+        raise ValueError("a compressible slab needs at least 2 rows")
+    mine = torch.stack([U[:, :2, :], U[:, -2:, :]]).contiguous()  # (2, 4, 2, nx): first rows, last rows
+    parts = ranks.all_gather_tensor(mine)
+    edges = comp_slab_edges(ranks.rank, ranks.world, walls)
+    lo = parts[(ranks.rank - 1) % ranks.world][1].contiguous() if edges & 1 else None
+    hi = parts[(ranks.rank + 1) % ranks.world][0].contiguous() if edges & 2 else None
+    return lo, hi, edges
+
+
+def ns_compressible_slab(U, halo_lo=None, halo_hi=None, edges: int = 0, *, limiter: str = "minmod",
+                         bc: str = "walls", reference_rounding: bool = False, R=None, diag=None, det_sq64=None,
+                         workspace=None, stream=None):
+    """The residual of one slab (cspb_ns_comp_slab): returns (R, diag, det_sq64) over the slab's cells."""
+    import torch
+    import cospanmdao_b200 as cb
+    if limiter not in ("minmod", "vanleer") or bc not in ("walls", "periodic"):
+        raise ValueError("limiter must be minmod|vanleer and bc walls|periodic")
+    if U.dim() != 3 or U.shape[0] != 4 or U.dtype != torch.float32 or not U.is_contiguous():
+        raise ValueError("'U' must be a contiguous (4, rows, nx) float32 tensor")
+    _, rows, nx = U.shape
+    dev = U.device
+    for name, h, bit in (("halo_lo", halo_lo, 1), ("halo_hi", halo_hi, 2)):
+        if edges & bit and (h is None or tuple(h.shape) != (4, 2, nx) or not h.is_contiguous()):
+            raise ValueError(f"'{name}' must be a contiguous (4, 2, {nx}) tensor for an interior edge")
+    R = torch.empty_like(U) if R is None else R
+    diag = torch.empty(18, dtype=torch.float32, device=dev) if diag is None else diag
+    det_sq64 = torch.empty(4, dtype=torch.float64, device=dev) if det_sq64 is None else det_sq64
+    ws = workspace or cb.default_workspace(dev, stream)
+    wp, wb = ws.ptr(int(lib().cspb_ns_comp_slab_workspace_bytes(nx, rows)))
+    d = _capi.NsCompSlabDesc(nx, rows, 0 if limiter == "minmod" else 1, 1 if bc == "walls" else 0,
+                             _capi.NS_REFERENCE_ROUNDING if reference_rounding else 0, int(edges), _ptr(U),
+                             _ptr(halo_lo) if edges & 1 else None, _ptr(halo_hi) if edges & 2 else None, _ptr(R),
+                             _ptr(diag), _ptr(det_sq64), wp, wb)
+    cb._raise(lib().cspb_ns_comp_slab(C.byref(d), C.c_void_p(cb._stream(stream))), "ns compressible slab")
+    return R, diag, det_sq64
+
+
+def combine_comp_diag(diags, sums):
+    """The whole grid's 18 diagnostics from every slab's (diags: per-slab (18,) float32 tensors in rank order, sums:
+    their (4,) f64 squared sums): the atomic and deterministic min dt / max wave speed exactly, the atomic sums in f32
+    and the deterministic ones in f64, each added in rank order; the error stage atomic - deterministic."""
+    import torch
+    D = torch.stack([d.float().cpu() for d in diags])
+    S = torch.stack([s.double().cpu() for s in sums])
+    out = torch.empty(18, dtype=torch.float32)
+    out[0] = D[:, 0].min()
+    out[1] = D[:, 1].max()
+    sq = D[0, 2:6].clone()
+    det = S[0].clone()
+    for q in range(1, D.shape[0]):
+        sq += D[q, 2:6]
+        det += S[q]
+    out[2:6] = sq
+    out[6:10] = det.float()
+    out[10] = D[:, 10].min()
+    out[11] = D[:, 11].max()
+    out[12] = out[0] - out[10]
+    out[13] = out[1] - out[11]
+    out[14:18] = out[2:6] - out[6:10]
+    return out, det
+
+
+def ns_compressible_sharded(U, *, limiter: str = "minmod", bc: str = "walls", ranks=None,
+                            reference_rounding: bool = False, workspace=None, stream=None):
+    """This rank's slab of one compressible residual: (R of its rows, the whole grid's 18 diagnostics, the whole
+    grid's 4 f64 squared sums)."""
+    lo, hi, edges = exchange_comp_halos(U, ranks, bc == "walls")
+    R, diag, sq = ns_compressible_slab(U, lo, hi, edges, limiter=limiter, bc=bc,
+                                       reference_rounding=reference_rounding, workspace=workspace, stream=stream)
+    if ranks is None or ranks.world == 1:
+        return R, diag, sq
+    d_all = ranks.all_gather_tensor(diag)
+    s_all = ranks.all_gather_tensor(sq)
+    out, det = combine_comp_diag(d_all, s_all)
+    return R, out.to(diag.device), det.to(sq.device)

@@ -322,6 +322,35 @@ typedef struct cspb_ns_comp_desc {
 size_t cspb_ns_comp_workspace_bytes(int32_t nx, int32_t ny);
 int cspb_ns_compressible(const cspb_ns_comp_desc* d, void* stream);
 
+/* One y-slab of a larger compressible grid (one process per GPU): rows [r0, r0 + rows) of U, rows >= 2. An edge whose
+ * bit is set in `edges` is interior: bit 1, below the slab's row 0, reads the two rows r0 - 2, r0 - 1 of every field
+ * from halo_lo; bit 2, above its last row, reads r0 + rows, r0 + rows + 1 from halo_hi; both are (4, 2, nx) f32,
+ * the neighbouring slabs' rows (wrapped over the whole grid when it is periodic). An edge whose bit is clear takes the
+ * whole grid's boundary rule there: the walls' mirror for the grid's first and last slab, or, with one slab, the
+ * periodic wrap. R over the slab's cells is bit-identical to cspb_ns_compressible's rows of the whole grid, and so are
+ * the per-cell dt and wave speed; diag and det_sq64 hold this slab's diagnostics (its min dt, max wave speed and
+ * squared sums), which the caller combines across slabs in a fixed order (min, max, sum). The reference runs its
+ * residual on one device (no counterpart); the exchange this implies is the 2-cell halo of its tiles
+ * (examples/ns-residual/tile.hpp:39-49) across slabs, 2 rows x 4 fields per neighbour. */
+typedef struct cspb_ns_comp_slab_desc {
+    int32_t nx, rows;    /* nx >= 4, rows >= 2 */
+    int32_t limiter;     /* 0 minmod, 1 van Leer */
+    int32_t walls;       /* the whole grid's boundary rule in y: 1 walls, 0 periodic */
+    int32_t flags;       /* 0 or CSPB_NS_REFERENCE_ROUNDING */
+    int32_t edges;       /* bit 1: the edge below row 0 is interior; bit 2: the edge above row rows - 1 */
+    const float* U;      /* (4, rows, nx) */
+    const float* halo_lo;  /* (4, 2, nx) when edges & 1 */
+    const float* halo_hi;  /* (4, 2, nx) when edges & 2 */
+    float* R;            /* (4, rows, nx) */
+    float* diag;         /* 18 floats, as cspb_ns_compressible, over this slab's cells */
+    double* det_sq64;    /* 4 doubles, may be NULL */
+    void* workspace;
+    size_t workspace_bytes;
+} cspb_ns_comp_slab_desc;
+
+size_t cspb_ns_comp_slab_workspace_bytes(int32_t nx, int32_t rows);
+int cspb_ns_comp_slab(const cspb_ns_comp_slab_desc* d, void* stream);
+
 /* The reference's initial field (examples/ns-residual/physics.hpp:203-215, make_init main.cpp:100-112) on the
  * device: U(v, j, i) for amplitude amp. */
 int cspb_ns_init_cons(float* U, int32_t nx, int32_t ny, float amp, void* stream);
@@ -430,7 +459,7 @@ int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t
 /* ==================================================================================================================
  * cspb_build_column_static: cspb_build_column with no workspace argument, for callers that cannot allocate device
  * memory at the call site (a foreign-language binding that holds only the column's pointers and no allocator, code
- * running where an allocation would stall or be refused). It allocates nothing: its scratch is a fixed 164,096-byte array
+ * running where an allocation would stall or be refused). It allocates nothing: its scratch is a fixed 131,328-byte array
  * in the library's device image (one per device), looked up in the current device's context by each call;
  * make the first call on a device before any stream capture begins. Results are bit-identical to cspb_build_column.
  * Limit: at most CSPB_BUILD_COLUMN_STATIC_MAX extents (count in counts mode, count - 1 in offsets mode); larger inputs

@@ -113,3 +113,66 @@ def test_three_ranks_exchange_halo_rows(tmp_path):
     want = np.sqrt(np.array([1.0 + 2.0 + 3.0, 2.0 * 3, 3.0 * (0 + 1 + 2)]))
     for q in range(world):
         assert np.array_equal(np.load(tmp_path / f"norms{q}.npy"), want)
+
+
+# ---- the compressible residual's slabs --------------------------------------------------------------------------
+NXC, NYC = 20, 23
+
+
+def _comp_rank(rank, world, port, out_dir, walls):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    import torch
+    import oracle
+    from cospanmdao_b200.replicas import Ranks
+    from cospanmdao_b200.sharded import combine_comp_diag, exchange_comp_halos, shard_rows
+    r = Ranks().init("gloo", timeout_s=60)
+    U = torch.from_numpy(oracle.ns_init(NXC, NYC, 1.0))
+    r0, r1 = shard_rows(NYC, world, 2)[rank]
+    lo, hi, edges = exchange_comp_halos(U[:, r0:r1].contiguous(), r, walls)
+    blank = torch.full((4, 2, NXC), float("nan"))
+    np.save(Path(out_dir) / f"c{rank}.npy", np.stack([(lo if lo is not None else blank).numpy(),
+                                                      (hi if hi is not None else blank).numpy()]))
+    # stand-in slab diagnostics: [dt, ws, sq0..3, detn0..3, detd, detw, err..] and f64 sums, distinct per rank
+    diag = torch.arange(18, dtype=torch.float32) + 100 * rank
+    diag[0] = diag[10] = 5.0 - rank
+    diag[1] = diag[11] = 1.0 + rank
+    sums = torch.tensor([1.0, 2.0, 3.0, 4.0], dtype=torch.float64) * (rank + 1) + 0.1
+    out, det = combine_comp_diag(r.all_gather_tensor(diag), r.all_gather_tensor(sums))
+    np.save(Path(out_dir) / f"d{rank}.npy", np.concatenate([out.numpy().astype(np.float64), det.numpy()]))
+    Path(out_dir, f"e{rank}.json").write_text(json.dumps({"edges": edges, "r0": r0, "r1": r1}))
+    r.barrier()
+    r.close()
+
+
+@pytest.mark.parametrize("world,walls", [(2, True), (3, True), (3, False)])
+def test_ranks_exchange_compressible_halos(tmp_path, world, walls):
+    import torch.multiprocessing as mp
+    import oracle
+    mp.start_processes(_comp_rank, args=(world, _free_port(), str(tmp_path), walls), nprocs=world, join=True,
+                       start_method="spawn")
+    U = oracle.ns_init(NXC, NYC, 1.0)
+    outs = []
+    for q in range(world):
+        lo, hi = np.load(tmp_path / f"c{q}.npy")
+        e = json.loads((tmp_path / f"e{q}.json").read_text())
+        r0, r1 = e["r0"], e["r1"]
+        want_lo = not walls or q > 0
+        want_hi = not walls or q < world - 1
+        assert e["edges"] == (1 if want_lo else 0) | (2 if want_hi else 0)
+        if want_lo:  # global rows r0 - 2, r0 - 1, wrapped
+            assert np.array_equal(lo, U[:, [(r0 - 2) % NYC, (r0 - 1) % NYC], :])
+        else:
+            assert np.isnan(lo).all()
+        if want_hi:
+            assert np.array_equal(hi, U[:, [r1 % NYC, (r1 + 1) % NYC], :])
+        else:
+            assert np.isnan(hi).all()
+        outs.append(np.load(tmp_path / f"d{q}.npy"))
+    for q in range(1, world):
+        assert np.array_equal(outs[q], outs[0])  # every rank combines to the same bits
+    d = outs[0]
+    assert d[0] == 5.0 - (world - 1) and d[10] == d[0]  # min dt
+    assert d[1] == 1.0 + (world - 1) and d[11] == d[1]  # max wave speed
+    det = sum(np.array([1.0, 2.0, 3.0, 4.0]) * (q + 1) + 0.1 for q in range(world))
+    assert np.allclose(d[18:], det, rtol=0, atol=1e-12)

@@ -114,3 +114,45 @@ def test_ns_slabs_match_the_whole_grid(cuda, nx, ny, world):
     for s in sums[1:]:
         total += s
     assert torch.allclose(total.sqrt(), norms, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("walls", [True, False])
+@pytest.mark.parametrize("lim,exact", [("minmod", False), ("vanleer", False), ("minmod", True)])
+def test_compressible_slabs_bit_identical_to_whole_grid(cuda, walls, lim, exact):
+    # three slabs of one grid, run one after the other on one GPU with the halos each would receive: R bit-identical
+    # to the whole grid's, min dt / max wave speed exactly, the f64 squared sums to rounding of their grouping
+    import torch
+    import numpy as np
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200.sharded import combine_comp_diag, comp_slab_edges, ns_compressible_slab, shard_rows
+    nx, ny, world = 256, 301, 3
+    bc = "walls" if walls else "periodic"
+    U = cb.ns_init_cons(nx, ny, 1.0, device=cuda)
+    R, diag, sq = cb.ns_compressible(U, limiter=lim, bc=bc, reference_rounding=exact)
+    Rs, ds, ss = [], [], []
+    for q, (r0, r1) in enumerate(shard_rows(ny, world, 16)):
+        edges = comp_slab_edges(q, world, walls)
+        lo = U[:, [(r0 - 2) % ny, (r0 - 1) % ny], :].contiguous()
+        hi = U[:, [r1 % ny, (r1 + 1) % ny], :].contiguous()
+        Rq, dq, sq_q = ns_compressible_slab(U[:, r0:r1].contiguous(), lo, hi, edges, limiter=lim, bc=bc,
+                                            reference_rounding=exact)
+        Rs.append(Rq)
+        ds.append(dq.clone())
+        ss.append(sq_q.clone())
+    torch.cuda.synchronize()
+    assert torch.equal(torch.cat(Rs, dim=1), R)
+    out, det = combine_comp_diag(ds, ss)
+    d = diag.cpu()
+    assert out[10] == d[10] and out[11] == d[11] and out[0] == d[0] and out[1] == d[1]
+    assert np.allclose(det.numpy(), sq.cpu().numpy(), rtol=1e-12, atol=0)
+
+
+def test_compressible_single_slab_equals_whole_grid(cuda):
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200.sharded import ns_compressible_slab
+    U = cb.ns_init_cons(128, 64, 1.0, device=cuda)
+    for bc in ("walls", "periodic"):
+        R, diag, sq = cb.ns_compressible(U, bc=bc)
+        R1, d1, s1 = ns_compressible_slab(U, None, None, 0, bc=bc)
+        assert torch.equal(R, R1) and torch.equal(diag[6:12], d1[6:12]) and torch.equal(sq, s1)

@@ -111,7 +111,7 @@ def test_ns_tasks_match_single_calls(cuda, dtype_name):
     from cospanmdao_b200 import workloads
     from cospanmdao_b200.tasks import TaskRunner, ns_task
     dtype = getattr(torch, dtype_name)
-    grids = [256, 512, 64, 1024, 130]
+    grids = [256, 512, 64, 1024, 130, 200, 24]  # 200, 24: partial tiles at the grid's east and south edges
     cases = []
     for i, N in enumerate(grids):
         u, v, p, h = workloads.ns_fields(N, seed=i, dtype=dtype, device=cuda)
