@@ -64,7 +64,8 @@ def build_examples(reference: str | os.PathLike | None = None, verbose: bool = F
     return built
 
 
-RUNTIME_TESTS = {"runtime-fused-groups": "fused_groups.cu", "runtime-ragged": "ragged.cu", "runtime-replay": "replay.cu"}
+RUNTIME_TESTS = {"runtime-fused-groups": "fused_groups.cu", "runtime-ragged": "ragged.cu", "runtime-replay": "replay.cu",
+                 "runtime-decoy": "decoy.cu"}
 
 
 def build_runtime_tests(verbose: bool = False) -> dict[str, Path]:

@@ -150,6 +150,11 @@ public:
     std::vector<int> pattern_at;             // leaf index -> pattern index or -1 (-2: covered, skip)
     std::vector<std::size_t> pattern_hi;     // per pattern: the last leaf it covers
     std::vector<std::shared_ptr<void>> pattern_state;  // what the fast paths keep between runs (workspaces, scales)
+    // per pattern: the outputs its kernel writes, each with the relative L2 distance it may keep from the components'
+    // own bodies, and whether it was checked against them (0 not yet, 1 agreed: the kernel runs, -1 disagreed: the
+    // bodies run)
+    std::vector<std::vector<std::pair<int, double>>> pattern_checks;
+    std::vector<int> pattern_verified;
     int sms = 0;
     bool trace = false;  // NAGA_COSPAN_TRACE set: every launch and initializer is printed to stderr
     void* scan_ws = nullptr;  // cspb_build_column's workspace (ragged hooks), grown as needed
@@ -181,6 +186,7 @@ public:
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         pattern_runs.clear();
         pattern_state.clear();
+        pattern_checks.clear();
         for (auto& v : vars)
             if (v.data) cudaFree(v.data);
         if (ctrl) cudaFree(ctrl);
@@ -1030,6 +1036,7 @@ private:
 // ---- the model --------------------------------------------------------------------------------------------------------
 namespace detail {
 void register_patterns(Runtime& rt);  // patterns.hpp
+int verify_pattern(Runtime& rt, std::size_t pat);  // patterns.hpp
 }
 
 class Model {
@@ -1142,10 +1149,22 @@ private:
             const int pat = rt.pattern_at.empty() ? -1 : rt.pattern_at[i];
             if (pat == -2) continue;
             if (pat >= 0) {
-                std::size_t next = i;
-                if (rt.pattern_runs[std::size_t(pat)](rt, next)) continue;
-                // the fast path declined this run: the leaves it covers run their own bodies
                 const std::size_t hi = rt.pattern_hi[std::size_t(pat)];
+                int& verified = rt.pattern_verified[std::size_t(pat)];
+                if (verified == 0) {
+                    // A run is recognised by its components' type names and wiring; before its kernel replaces the
+                    // bodies, one forward runs both and compares what they write (never inside a graph capture: the
+                    // comparison waits on the host)
+                    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+                    cudaStreamIsCapturing(rt.stream, &cs);
+                    for (std::size_t k = i; k <= hi; ++k) run_leaf(k);
+                    if (cs == cudaStreamCaptureStatusNone) verified = detail::verify_pattern(rt, std::size_t(pat));
+                    i = hi;
+                    continue;
+                }
+                std::size_t next = i;
+                if (verified > 0 && rt.pattern_runs[std::size_t(pat)](rt, next)) continue;
+                // the fast path declined this run or disagreed with the bodies: the leaves it covers run their own
                 for (std::size_t k = i; k <= hi; ++k) run_leaf(k);
                 i = hi;
                 continue;

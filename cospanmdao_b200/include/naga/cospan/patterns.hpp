@@ -21,9 +21,16 @@
 // Ps) are not written, so a run whose partials something else reads, or whose scale is itself computed, is left to
 // the generic path. The scales (the reference's `scale` inputs: α = β = 1/√n in the chain) are read from their device
 // variables once per initialisation. NAGA_COSPAN_GENERIC set in the environment turns every fast path off.
+//
+// Types and wiring say what a run is built from, not what its bodies compute: a user component with the reference's
+// type name and ports could do other arithmetic. So the first forward of every recognised run executes the bodies,
+// then the kernel, and compares the outputs the kernel writes (verify_pattern, tolerances kTol*); the kernel replaces
+// the bodies only when they agree, and otherwise the bodies' results are kept and the bodies run from then on.
 #pragma once
 
 #include <algorithm>
+#include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <memory>
 #include <string>
@@ -209,7 +216,108 @@ inline std::int64_t gemver_n(Runtime& rt, const GemverMatch& g) {
     return (A.rank == 2 && A.shape[0] == A.shape[1]) ? std::int64_t(A.shape[0]) : 0;
 }
 
-inline void claim(Runtime& rt, int pat, std::size_t lo, std::size_t hi) {
+// Tolerances of a fast path's outputs against the components' own bodies (relative L2). Two f32 evaluations that
+// round differently (the bodies compile with fused multiply-adds, the kernels round each operation of Â; sums in
+// another order) stay well inside them: Â about 1e-7, x and w about 1e-7 at n = 16384, an NS residual about 2e-5 at
+// 4096². A component that computes something else differs at O(1).
+constexpr double kTolMatrix = 1e-6, kTolVector = 1e-5, kTolField = 1e-4;
+
+// Σ (a - b)², Σ b² and the number of positions where b is finite and a is not, in f64, one atomic per block.
+template <int kUnused = 0>
+__global__ void k_fast_check(const float* a, const float* b, std::size_t n, double* acc) {
+    double d = 0.0, s = 0.0, bad = 0.0;
+    for (std::size_t i = std::size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += std::size_t(gridDim.x) * blockDim.x) {
+        const float x = a[i], y = b[i];
+        if (isfinite(y) && !isfinite(x)) bad += 1.0;
+        const double t = double(x) - double(y);
+        d += t * t;
+        s += double(y) * double(y);
+    }
+    for (int off = 16; off >= 1; off >>= 1) {
+        d += __shfl_xor_sync(0xffffffffu, d, off);
+        s += __shfl_xor_sync(0xffffffffu, s, off);
+        bad += __shfl_xor_sync(0xffffffffu, bad, off);
+    }
+    __shared__ double r[3][32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { r[0][w] = d; r[1][w] = s; r[2][w] = bad; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        for (int k = 0; k < int(blockDim.x >> 5); ++k) t += r[threadIdx.x][k];
+        atomicAdd(acc + threadIdx.x, t);
+    }
+}
+
+// Runs pattern `pat`'s kernel after the components' own bodies wrote its outputs, and compares. 1: every output within
+// its tolerance (the kernel runs from now on); -1: an output differs, the bodies' values are put back and the bodies
+// run from now on (a component with the same type name and wiring but other arithmetic is never replaced); 0: the fast
+// path declined this forward (checked again on the next).
+inline int verify_pattern(Runtime& rt, std::size_t pat) {
+    const auto& checks = rt.pattern_checks[pat];
+    std::vector<void*> snap(checks.size(), nullptr);
+    std::vector<std::size_t> count(checks.size(), 0);
+    for (std::size_t k = 0; k < checks.size(); ++k) {
+        Var& v = rt.vars[std::size_t(checks[k].first)];
+        if (v.dtype != DType::f32 || !v.data || v.elements() == 0) continue;
+        count[k] = v.elements();
+        ++rt.allocs;
+        cuda_check(cudaMalloc(&snap[k], count[k] * sizeof(float)), "fast-path check");
+        cuda_check(cudaMemcpyAsync(snap[k], v.data, count[k] * sizeof(float), cudaMemcpyDeviceToDevice, rt.stream),
+                   "fast-path check");
+    }
+    std::size_t next = 0;
+    int result = 0;
+    if (rt.pattern_runs[pat](rt, next)) {
+        double* acc = nullptr;
+        ++rt.allocs;
+        cuda_check(cudaMalloc(&acc, 3 * sizeof(double) * checks.size()), "fast-path check");
+        cuda_check(cudaMemsetAsync(acc, 0, 3 * sizeof(double) * checks.size(), rt.stream), "fast-path check");
+        for (std::size_t k = 0; k < checks.size(); ++k) {
+            if (!snap[k]) continue;
+            const float* fast = static_cast<const float*>(rt.vars[std::size_t(checks[k].first)].data);
+            const unsigned blocks = unsigned(std::min<std::size_t>((count[k] + 255) / 256, 1024));
+            k_fast_check<<<blocks, 256, 0, rt.stream>>>(fast, static_cast<const float*>(snap[k]), count[k], acc + 3 * k);
+        }
+        std::vector<double> h(3 * checks.size(), 0.0);
+        ++rt.host_syncs;
+        cuda_check(cudaMemcpyAsync(h.data(), acc, h.size() * sizeof(double), cudaMemcpyDeviceToHost, rt.stream),
+                   "fast-path check");
+        cuda_check(cudaStreamSynchronize(rt.stream), "fast-path check");
+        cudaFree(acc);
+        result = 1;
+        std::string bad;
+        for (std::size_t k = 0; k < checks.size(); ++k) {
+            if (!snap[k]) continue;
+            const double d = h[3 * k], s2 = h[3 * k + 1], nonfinite = h[3 * k + 2];
+            const double rel = s2 > 0.0 ? std::sqrt(d / s2) : (d > 0.0 ? 1.0 : 0.0);
+            if (nonfinite > 0.0 || !(rel <= checks[k].second)) {
+                result = -1;
+                bad += " '" + rt.vars[std::size_t(checks[k].first)].name + "' (relative L2 " + std::to_string(rel) + ")";
+            }
+        }
+        if (result < 0) {
+            for (std::size_t k = 0; k < checks.size(); ++k)
+                if (snap[k])
+                    cuda_check(cudaMemcpyAsync(rt.vars[std::size_t(checks[k].first)].data, snap[k],
+                                               count[k] * sizeof(float), cudaMemcpyDeviceToDevice, rt.stream),
+                               "fast-path check");
+            std::fprintf(stderr, "[cospan] fast path %zu not used: the kernel and the components' own bodies differ in%s;"
+                                 " the bodies run\n", pat, bad.c_str());
+        } else if (rt.trace) {
+            std::fprintf(stderr, "[cospan] fast path %zu agrees with the components' own bodies\n", pat);
+        }
+    }
+    cuda_check(cudaStreamSynchronize(rt.stream), "fast-path check");
+    for (void* p : snap)
+        if (p) cudaFree(p);
+    return result;
+}
+
+inline void claim(Runtime& rt, int pat, std::size_t lo, std::size_t hi,
+                  std::vector<std::pair<int, double>> checks) {
+    rt.pattern_checks.push_back(std::move(checks));
+    rt.pattern_verified.push_back(0);
     rt.pattern_hi.push_back(hi);
     rt.pattern_at[lo] = pat;
     for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
@@ -238,7 +346,7 @@ inline bool try_gemver(Runtime& rt, const PatternLeaves& L, std::size_t a) {
         launch_gemver(rt, *st, g, n, st->scale[0], st->scale[1]);
         return true;
     });
-    claim(rt, pat, lo, hi);
+    claim(rt, pat, lo, hi, {{g.vB, kTolMatrix}, {var_id(rt, g.cred, "x"), kTolVector}, {var_id(rt, g.gemv, "y"), kTolVector}});
     return true;
 }
 
@@ -332,7 +440,7 @@ inline bool try_bicgk(Runtime& rt, const PatternLeaves& L, std::size_t a) {
         launch_bicgk(rt, *st, m, std::int64_t(B.shape[0]));
         return true;
     });
-    claim(rt, pat, lo, hi);
+    claim(rt, pat, lo, hi, {{m.vq, kTolVector}, {m.vs, kTolVector}});
     return true;
 }
 
@@ -346,6 +454,12 @@ struct ChainVars {
         return true;
     }
 };
+
+// the outputs a chain kernel writes
+inline std::vector<std::pair<int, double>> chain_checks(const ChainVars& c) {
+    return {{c.B1, kTolMatrix}, {c.x1, kTolVector}, {c.w1, kTolVector}, {c.q, kTolVector}, {c.s, kTolVector},
+            {c.B2, kTolMatrix}, {c.x2, kTolVector}, {c.w2, kTolVector}};
+}
 
 inline void launch_chain(Runtime& rt, FastState& st, const ChainVars& c, std::int64_t n, float alpha, float beta,
                          const ComponentBase* first, const ComponentBase* last) {
@@ -442,7 +556,7 @@ inline bool try_chain(Runtime& rt, const PatternLeaves& L, std::size_t a) {
         launch_chain(rt, *st, cv, n, alpha1, beta1, g1.r2u, g2.gemv);
         return true;
     });
-    claim(rt, pat, lo, hi);
+    claim(rt, pat, lo, hi, chain_checks(cv));
     return true;
 }
 
@@ -503,7 +617,7 @@ inline bool try_crafted_chain(Runtime& rt, const PatternLeaves& L, std::size_t a
         launch_chain(rt, *st, cv, n, alpha1, beta1, run.front(), run.back());
         return true;
     });
-    claim(rt, pat, lo, hi);
+    claim(rt, pat, lo, hi, chain_checks(cv));
     return true;
 }
 
@@ -617,9 +731,8 @@ inline bool try_ns(Runtime& rt, const PatternLeaves& L, std::size_t a) {
             }
             return true;
         });
-        rt.pattern_hi.push_back(hi);
-        rt.pattern_at[lo] = pat;
-        for (std::size_t i = lo + 1; i <= hi; ++i) rt.pattern_at[i] = -2;
+        // R and the deterministic diagnostics (the atomic ones depend on the order the tiles finish in)
+        claim(rt, pat, lo, hi, {{vR, kTolField}, {outs[3], kTolField}, {outs[4], kTolVector}, {outs[5], kTolVector}});
         return true;
     }
     return false;
@@ -628,6 +741,8 @@ inline bool try_ns(Runtime& rt, const PatternLeaves& L, std::size_t a) {
 inline void register_patterns(Runtime& rt) {
     rt.pattern_at.assign(rt.leaves.size(), -1);
     rt.pattern_hi.clear();
+    rt.pattern_checks.clear();
+    rt.pattern_verified.clear();
     if (std::getenv("NAGA_COSPAN_GENERIC")) return;
     const PatternLeaves L = pattern_leaves(rt);
     for (std::size_t a = 0; a < L.comps.size();) {

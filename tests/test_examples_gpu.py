@@ -51,6 +51,15 @@ def test_runtime_replay(cuda):
     assert rc == 0 and "ALL OK" in out, out
 
 
+def test_runtime_decoy_component_not_replaced(cuda):
+    """A component named Gemv with the reference's ports and wiring but other arithmetic is not replaced by the GEMVER
+    kernel: the first forward compares kernel and bodies, and only the honest system keeps the kernel."""
+    rc, out = _run(["runtime-decoy"], env={"NAGA_COSPAN_TRACE": "1"})
+    assert rc == 0 and "ALL OK" in out, out[-3000:]
+    assert "agrees with the components' own bodies" in out, out[-3000:]
+    assert "not used: the kernel and the components' own bodies differ in" in out, out[-3000:]
+
+
 def test_getting_started(cuda):
     rc, out = _run(["getting-started"])
     assert rc == 0, out
