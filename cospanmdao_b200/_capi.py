@@ -156,6 +156,7 @@ PROTOTYPES = {
     "cspb_exclusive_scan_u64": (C.c_int, [vp, vp, i64, vp, sz, vp]),
     "cspb_build_column": (C.c_int, [vp, i32, i64, i64, i32, vp, vp, vp, vp, sz, vp]),
     "cspb_build_column_static": (C.c_int, [vp, i32, i64, i64, i32, vp, vp, vp, vp]),
+    "cspb_build_column64": (C.c_int, [vp, i32, i64, i64, i32, vp, vp, vp, vp, sz, vp]),
     "cspb_fill_hash": (C.c_int, [vp, i32, i64, u64, u32, i32, vp]),
 }
 

@@ -75,6 +75,7 @@ struct ScanK {
     uint32_t* ctrl;
     uint64_t* tstat;    // per tile: its status words (TileStat<T>)
     uint32_t* total_flag;  // column mode: [total, flag]
+    uint64_t* total64;     // a column with u64 offsets: its total (its flag word is total_flag)
 };
 
 // A tile's published state: flag (0 nothing, 1 aggregate, 2 inclusive prefix) and value in single 64-bit words, so a
@@ -320,6 +321,7 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
             }
         } else {
             g.out[g.n] = total;
+            if (g.total64) g.total64[0] = uint64_t(total);
         }
     }
 }
@@ -362,6 +364,43 @@ __global__ void k_column_extents(const uint32_t* offs, int64_t n, uint32_t* exte
     if (blockIdx.x == 0 && threadIdx.x == 0) total_flag[0] = offs[n];
 }
 
+// Offsets mode with u64 offsets: the values need not fit 32 bits; each extent (a difference) still must.
+__global__ void k_column_offsets64(ScanSrc s, int64_t m, uint64_t* offs, uint32_t* ctrl, uint32_t* flagw) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += stride) {
+        const uint64_t raw = load_column(s, i);
+        const bool sgn = s.dtype == CSPB_I32 || s.dtype == CSPB_I64;
+        uint64_t x = raw;
+        uint32_t flag = 0;
+        if (sgn && int64_t(raw) < 0) {
+            flag = 1u;
+            x = 0;
+        }
+        if (i == 0 && x != 0) flag |= 1u;
+        offs[i] = x;
+        if (flag) {
+            atomicOr(flagw, flag);
+            set_status(ctrl, CSPB_DEV_NEGATIVE);
+        }
+    }
+}
+__global__ void k_column_extents64(const uint64_t* offs, int64_t n, uint32_t* extents, uint32_t* ctrl,
+                                   uint32_t* flagw, uint64_t* total64) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t a = offs[i], b = offs[i + 1];
+        uint32_t flag = 0;
+        if (b < a) flag = 1u;
+        else if (b - a > 0xffffffffull) flag = 2u;
+        extents[i] = flag ? 0u : uint32_t(b - a);
+        if (flag) {
+            atomicOr(flagw, flag);
+            set_status(ctrl, flag == 1u ? CSPB_DEV_NEGATIVE : CSPB_DEV_EXCEEDS32);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) total64[0] = offs[n];
+}
+
 __global__ void k_scan_empty32(uint32_t* out) { out[0] = 0; }
 __global__ void k_scan_empty64(uint64_t* out) { out[0] = 0; }
 
@@ -391,7 +430,7 @@ ScanLayout<T> scan_layout(int64_t n) {
 
 template <typename T>
 int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, size_t ws_bytes, uint32_t* total_flag,
-             cudaStream_t st) {
+             cudaStream_t st, uint64_t* total64 = nullptr) {
     const ScanLayout<T> L = scan_layout<T>(n);
     if (!ws || !aligned(ws, 256) || ws_bytes < L.total) return CSPB_ERR_WORKSPACE;
     char* w = static_cast<char*>(ws);
@@ -406,6 +445,7 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
     g.ctrl = reinterpret_cast<uint32_t*>(w);
     g.tstat = reinterpret_cast<uint64_t*>(w + L.off_stat);
     g.total_flag = total_flag;
+    g.total64 = total64;
     k_scan<T><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
@@ -477,6 +517,43 @@ int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t
     const int64_t blocks = count / 256 + 1 > 1024 ? 1024 : count / 256 + 1;
     k_column_offsets<<<unsigned(blocks), 256, 0, st>>>(s, count, offs, ctrl, total_flag);
     k_column_extents<<<unsigned(blocks), 256, 0, st>>>(offs, n, extents, ctrl, total_flag);
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+int cspb_build_column64(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
+                        uint32_t* extents, uint64_t* offs, uint64_t* total_flag, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+    if (src_dtype < CSPB_I32 || src_dtype > CSPB_U64) return CSPB_ERR_UNSUPPORTED;
+    if (count < 0 || !offs || !total_flag || (count > 0 && !src)) return CSPB_ERR_ARGUMENT;
+    if (offsets_mode && count == 0) return CSPB_ERR_ARGUMENT;
+    if (!offsets_mode && k < 1) return CSPB_ERR_ARGUMENT;
+    if (count > (int64_t(1) << 40)) return CSPB_ERR_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = offsets_mode ? count - 1 : count;
+    if (n > 0 && !extents) return CSPB_ERR_ARGUMENT;
+    if (!workspace || !aligned(workspace, 256) || workspace_bytes < cspb_scan_workspace_bytes(n)) return CSPB_ERR_WORKSPACE;
+    cudaError_t e = cudaMemsetAsync(total_flag, 0, 2 * sizeof(uint64_t), st);
+    if (e != cudaSuccess) return CSPB_ERR_CUDA;
+    // the flag word: the low half of total_flag[1] (the same bits as cspb_build_column's total_flag[1])
+    uint32_t* flagw = reinterpret_cast<uint32_t*>(total_flag + 1);
+    ScanSrc s{src, src_dtype, offsets_mode ? 1 : k, true, extents};
+    if (!offsets_mode) {
+        if (n == 0) {
+            e = cudaMemsetAsync(workspace, 0, kCtrlBytes, st);
+            if (e != cudaSuccess) return CSPB_ERR_CUDA;
+            k_scan_empty64<<<1, 1, 0, st>>>(offs);
+            return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+        }
+        // the scan kernel ORs its flags into word 1 of the u32 view it is given: hand it the word before flagw (the
+        // high half of the total, which it does not write when it has a 64-bit total)
+        return run_scan<uint64_t>(s, offs, nullptr, n, workspace, workspace_bytes, flagw - 1, st, total_flag);
+    }
+    e = cudaMemsetAsync(workspace, 0, kCtrlBytes, st);
+    if (e != cudaSuccess) return CSPB_ERR_CUDA;
+    uint32_t* ctrl = static_cast<uint32_t*>(workspace);
+    const int64_t blocks = count / 256 + 1 > 1024 ? 1024 : count / 256 + 1;
+    k_column_offsets64<<<unsigned(blocks), 256, 0, st>>>(s, count, offs, ctrl, flagw);
+    k_column_extents64<<<unsigned(blocks), 256, 0, st>>>(offs, n, extents, ctrl, flagw, total_flag);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 

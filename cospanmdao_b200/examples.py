@@ -65,7 +65,7 @@ def build_examples(reference: str | os.PathLike | None = None, verbose: bool = F
 
 
 RUNTIME_TESTS = {"runtime-fused-groups": "fused_groups.cu", "runtime-ragged": "ragged.cu", "runtime-replay": "replay.cu",
-                 "runtime-decoy": "decoy.cu"}
+                 "runtime-decoy": "decoy.cu", "runtime-ragged-wide": "ragged_wide.cu"}
 
 
 def build_runtime_tests(verbose: bool = False) -> dict[str, Path]:

@@ -68,7 +68,8 @@ struct PortRec {
     // block offsets and per-index extents on the device, or nullptr and the row length for a dense variable)
     bool ragged = false;
     std::optional<std::vector<std::size_t>> counts;
-    std::function<void(void*, std::size_t, const std::uint32_t*, const std::uint32_t*, std::size_t)> bind_ragged;
+    std::function<void(void*, std::size_t, const std::uint32_t*, const std::uint64_t*, const std::uint32_t*, std::size_t)>
+        bind_ragged;
 };
 
 inline std::string list_of(const std::vector<std::size_t>& v) {
@@ -302,10 +303,12 @@ private:
         detail::PortRec& p = ports_.back();
         p.ragged = true;
         p.counts = std::move(counts);
-        p.bind_ragged = [&w](void* d, std::size_t nb, const std::uint32_t* offs, const std::uint32_t* ext, std::size_t row) {
+        p.bind_ragged = [&w](void* d, std::size_t nb, const std::uint32_t* offs, const std::uint64_t* offs64,
+                             const std::uint32_t* ext, std::size_t row) {
             w.data_ = static_cast<std::remove_reference_t<decltype(*w.data_)>*>(d);
             w.n_ = nb;
             w.offs_ = offs;
+            w.offs64_ = offs64;
             w.ext_ = ext;
             w.row_ = row;
         };

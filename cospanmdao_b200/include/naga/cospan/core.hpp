@@ -186,7 +186,8 @@ struct Initializer {
 
 // ---- ragged ports (wrappers.hpp:236-347 of the reference) -------------------------------------------------------
 // A ragged port is rank 2: N blocks, block i holding count(i) elements, the blocks stored end to end. The runtime
-// keeps per-index extents and the N + 1 block offsets (u32, so a ragged total is below 2^32) on the device. A
+// keeps per-index extents and the N + 1 block offsets on the device: u32 (the reference's, so a ragged total is below
+// 2^32), or u64 where the hook asked for them (counts_from<std::uint64_t>). A
 // RaggedInput also reads a DENSE rank-2 variable, whose block i is row i.
 
 /// Per-index counts given on the host, in a declaration: declare_output(m, "m", cs::counts({1, 0, 3})).
@@ -236,11 +237,11 @@ namespace detail {
 /// Block i: extents from the per-index array (a ragged variable) or the row length (a dense one); the start from the
 /// block offsets, or i rows in.
 template <class T>
-CS_HD inline Block<T> ragged_block(T* data, const std::uint32_t* offs, const std::uint32_t* ext, std::size_t row,
-                                   std::size_t i) {
+CS_HD inline Block<T> ragged_block(T* data, const std::uint32_t* offs, const std::uint64_t* offs64,
+                                   const std::uint32_t* ext, std::size_t row, std::size_t i) {
     Block<T> b;
     b.n_ = ext ? std::size_t(ext[i]) : row;
-    b.data_ = data + (offs ? std::size_t(offs[i]) : i * row);
+    b.data_ = data + (offs64 ? std::size_t(offs64[i]) : offs ? std::size_t(offs[i]) : i * row);
     return b;
 }
 }  // namespace detail
@@ -255,11 +256,12 @@ struct RaggedInput {
     static constexpr int rank = Rank;
     static constexpr bool ragged = true;
     CS_HD std::size_t size() const { return n_; }
-    CS_HD Block<const value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, ext_, row_, i); }
+    CS_HD Block<const value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, offs64_, ext_, row_, i); }
 
     std::size_t n_ = 0;
     const value_type* data_ = nullptr;
     const std::uint32_t* offs_ = nullptr;
+    const std::uint64_t* offs64_ = nullptr;  // a column with u64 offsets (counts_from<std::uint64_t>)
     const std::uint32_t* ext_ = nullptr;
     std::size_t row_ = 0;
 };
@@ -274,15 +276,16 @@ struct RaggedOutput {
     static constexpr bool ragged = true;
     CS_HD std::size_t size() const { return n_; }
     template <DType Q = DT, std::enable_if_t<!is_atomic_v<Q>, int> = 0>
-    CS_HD Block<value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, ext_, row_, i); }
+    CS_HD Block<value_type> block(std::size_t i) const { return detail::ragged_block(data_, offs_, offs64_, ext_, row_, i); }
     template <DType Q = DT, std::enable_if_t<is_atomic_v<Q>, int> = 0>
     CS_HD AtomicBlock<value_type> block(std::size_t i) const {
-        return AtomicBlock<value_type>{detail::ragged_block(data_, offs_, ext_, row_, i)};
+        return AtomicBlock<value_type>{detail::ragged_block(data_, offs_, offs64_, ext_, row_, i)};
     }
 
     std::size_t n_ = 0;
     value_type* data_ = nullptr;
     const std::uint32_t* offs_ = nullptr;
+    const std::uint64_t* offs64_ = nullptr;  // a column with u64 offsets (counts_from<std::uint64_t>)
     const std::uint32_t* ext_ = nullptr;
     std::size_t row_ = 0;
 };

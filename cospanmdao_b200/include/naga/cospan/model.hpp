@@ -40,54 +40,71 @@ struct ViewState {
     bool ragged = false, per = false;
     std::size_t n = 0, row = 0;
     std::uint32_t* host_offs = nullptr;
+    std::uint64_t* host_offs64 = nullptr;  // a column with u64 offsets
     std::size_t offs_cap = 0;
+    // block i's start (a column's offsets, u32 or u64, or i rows in)
+    std::uint64_t off(std::size_t i) const {
+        if (!per) return std::uint64_t(i) * row;
+        return host_offs64 ? host_offs64[i] : std::uint64_t(host_offs[i]);
+    }
     ~ViewState() {
         if (host) cudaFreeHost(host);
         if (host_offs) cudaFreeHost(host_offs);
+        if (host_offs64) cudaFreeHost(host_offs64);
         if (ev) cudaEventDestroy(ev);
     }
 };
 
 /// A ragged variable's device counts and block offsets (shape_hook.hpp:215-348 and variable.hpp:252-300 of the
-/// reference): N extents and N + 1 offsets, u32, so that a ragged total is below 2^32. A counts_from / offsets_from
+/// reference): N u32 extents and N + 1 offsets, u32 as in the reference (a total below 2^32) or u64 when the hook asks
+/// for them (counts_from<std::uint64_t>, built by cspb_build_column64). A counts_from / offsets_from
 /// hook builds one with cspb_build_column (one launch; [total, flag] comes back through mapped pinned memory); host
 /// counts (a declaration, or a producer's set_shape) are uploaded into one. Shared between variables by set_shape(out,
 /// shape_of(in)): the wrappers read the pointers at every bind, so a column that grows is seen by all of them.
 struct Column {
     std::uint32_t* ext = nullptr;
-    std::uint32_t* offs = nullptr;
+    std::uint32_t* offs = nullptr;    // u32 offsets (the default)
+    std::uint64_t* offs64 = nullptr;  // u64 offsets, for a column built with wide offsets (counts_from<uint64_t>)
+    bool wide = false;
     std::size_t cap = 0;  // entries of offs (ext has at least cap - 1)
     std::size_t n = 0;
     std::uint64_t total = 0;
     std::uint64_t version = 0;
-    std::uint32_t* tf = nullptr;  // mapped pinned [total, flag]
+    std::uint32_t* tf = nullptr;  // mapped pinned [total, flag] (u32 offsets) or, as two u64, [total, flag] (u64)
     std::uint32_t* tf_dev = nullptr;
     std::vector<std::size_t> uploaded;  // the host counts in the column (a host column)
     bool has_upload = false;
     std::vector<std::uint32_t> staging;
+    std::vector<std::uint64_t> staging64;
     Column() = default;
     Column(const Column&) = delete;
     Column& operator=(const Column&) = delete;
     ~Column() {
         if (ext) cudaFree(ext);
         if (offs) cudaFree(offs);
+        if (offs64) cudaFree(offs64);
         if (tf) cudaFreeHost(tf);
     }
-    /// Room for n blocks. A reallocation waits for the stream first (kernels in flight may read the old arrays).
-    void reserve(std::size_t nb, cudaStream_t s) {
+    /// Room for n blocks, with u32 or (wide) u64 offsets. A reallocation waits for the stream first (kernels in flight
+    /// may read the old arrays).
+    void reserve(std::size_t nb, cudaStream_t s, bool want_wide = false) {
         if (!tf) {
-            if (cudaHostAlloc(reinterpret_cast<void**>(&tf), 8, cudaHostAllocMapped) != cudaSuccess ||
+            if (cudaHostAlloc(reinterpret_cast<void**>(&tf), 16, cudaHostAllocMapped) != cudaSuccess ||
                 cudaHostGetDevicePointer(reinterpret_cast<void**>(&tf_dev), tf, 0) != cudaSuccess)
                 throw std::runtime_error("naga::cospan: a ragged column's host word");
         }
-        if (nb + 1 <= cap) return;
-        const std::size_t want = std::max(nb + 1, cap * 2);
-        if (ext || offs) cudaStreamSynchronize(s);
+        if (nb + 1 <= cap && want_wide == wide) return;
+        const std::size_t want = std::max(nb + 1, want_wide == wide ? cap * 2 : nb + 1);
+        if (ext || offs || offs64) cudaStreamSynchronize(s);
         if (ext) cudaFree(ext);
         if (offs) cudaFree(offs);
+        if (offs64) cudaFree(offs64);
         ext = offs = nullptr;
-        if (cudaMalloc(&ext, std::max<std::size_t>(want - 1, 1) * 4) != cudaSuccess || cudaMalloc(&offs, want * 4) != cudaSuccess)
-            throw std::runtime_error("naga::cospan: allocating a ragged column of " + std::to_string(nb) + " blocks");
+        offs64 = nullptr;
+        wide = want_wide;
+        const bool ok = cudaMalloc(&ext, std::max<std::size_t>(want - 1, 1) * 4) == cudaSuccess &&
+                        (wide ? cudaMalloc(&offs64, want * 8) : cudaMalloc(&offs, want * 4)) == cudaSuccess;
+        if (!ok) throw std::runtime_error("naga::cospan: allocating a ragged column of " + std::to_string(nb) + " blocks");
         cap = want;
     }
 };
@@ -281,6 +298,8 @@ public:
         const bool offsets_mode = std::holds_alternative<ragged::OffsetsFrom>(v.hook[0]);
         const std::string path = offsets_mode ? std::get<ragged::OffsetsFrom>(v.hook[0]).path
                                               : std::get<ragged::CountsFrom>(v.hook[0]).path;
+        const bool wide = offsets_mode ? std::get<ragged::OffsetsFrom>(v.hook[0]).wide
+                                       : std::get<ragged::CountsFrom>(v.hook[0]).wide;
         Var& src = var_of_path(v.hook_sys, path);
         int code = -1;
         switch (value_dtype(src.dtype)) {
@@ -308,7 +327,7 @@ public:
         const std::size_t n = offsets_mode ? count - 1 : count;
         if (!v.hook_column) v.hook_column = std::make_shared<Column>();
         Column& c = *v.hook_column;
-        c.reserve(n, stream);
+        c.reserve(n, stream, wide);
         const std::size_t need = std::size_t(cspb_scan_workspace_bytes(std::int64_t(n)));
         if (need > scan_ws_bytes) {
             ++allocs;
@@ -320,17 +339,26 @@ public:
             cuda_check(cudaMalloc(&scan_ws, need), "a ragged hook's workspace");
             scan_ws_bytes = need;
         }
-        const int rc = cspb_build_column(src.data, code, std::int64_t(count), std::int64_t(k), offsets_mode ? 1 : 0, c.ext,
-                                         c.offs, c.tf_dev, scan_ws, std::int64_t(scan_ws_bytes), stream);
-        if (rc != 0) throw std::runtime_error("naga::cospan: " + who + ": cspb_build_column: " + cspb_status_string(rc));
+        const int rc =
+            wide ? cspb_build_column64(src.data, code, std::int64_t(count), std::int64_t(k), offsets_mode ? 1 : 0, c.ext,
+                                       c.offs64, reinterpret_cast<std::uint64_t*>(c.tf_dev), scan_ws,
+                                       std::int64_t(scan_ws_bytes), stream)
+                 : cspb_build_column(src.data, code, std::int64_t(count), std::int64_t(k), offsets_mode ? 1 : 0, c.ext,
+                                     c.offs, c.tf_dev, scan_ws, std::int64_t(scan_ws_bytes), stream);
+        if (rc != 0) throw std::runtime_error("naga::cospan: " + who + ": building a ragged column: " + cspb_status_string(rc));
         cuda_check(cudaStreamSynchronize(stream), who);
-        const std::uint32_t total = c.tf[0], flag = c.tf[1];
+        // [total, flag]: two u32, or two u64 whose second's low half holds the same flag bits
+        const std::uint64_t total = wide ? reinterpret_cast<const std::uint64_t*>(c.tf)[0] : std::uint64_t(c.tf[0]);
+        const std::uint32_t flag = wide ? c.tf[2] : c.tf[1];
         if (flag & CSPB_COLUMN_TIMEOUT)
             throw std::runtime_error("naga::cospan: " + who + ": '" + path + "': the device scan's bounded wait gave up "
                                      "(" + std::string(cspb_status_string(CSPB_ERR_TIMEOUT)) + ")");
         if ((flag & 1u) == 0 && (flag & 2u) != 0)
-            throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds a value or a total past 2^32 - 1; "
-                                        "ragged totals are limited to 2^32 - 1 elements");
+            throw std::invalid_argument(
+                "naga::cospan: " + who + ": '" + path +
+                (wide ? "' holds a block past 2^32 - 1 elements; a block's extent is a u32"
+                      : "' holds a value or a total past 2^32 - 1; ragged totals with u32 offsets are limited to 2^32 - 1 "
+                        "elements (cs::ragged::counts_from<std::uint64_t> takes u64 offsets)"));
         if (flag != 0)
             throw std::invalid_argument("naga::cospan: " + who + ": '" + path + "' holds " +
                                         std::string(offsets_mode ? "offsets that are negative, do not start at 0, or decrease"
@@ -350,28 +378,39 @@ public:
     /// A ragged shape from host counts: uploaded into the variable's own column when they changed.
     void set_host_counts(Var& v, const std::vector<std::size_t>& counts, const std::string& who) {
         std::uint64_t total = 0;
-        for (auto c : counts) total += c;
-        if (total > 0xFFFFFFFFull)
-            throw std::invalid_argument("naga::cospan: " + who + ": a ragged shape has " + std::to_string(total) +
-                                        " elements; ragged totals are limited to 2^32 - 1 elements");
+        for (auto c : counts) {
+            if (c > 0xFFFFFFFFull)
+                throw std::invalid_argument("naga::cospan: " + who + ": a ragged block has " + std::to_string(c) +
+                                            " elements; a block's extent is limited to 2^32 - 1");
+            total += c;
+        }
+        // the host knows the total: past 2^32 - 1 the column takes u64 offsets by itself
+        const bool wide = total > 0xFFFFFFFFull;
         if (!v.own_column) v.own_column = std::make_shared<Column>();
         Column& c = *v.own_column;
-        if (!c.has_upload || c.uploaded != counts) {
+        if (!c.has_upload || c.uploaded != counts || c.wide != wide) {
             ++host_syncs;  // an upload from pageable memory: never part of a captured run
-            c.reserve(counts.size(), stream);
+            c.reserve(counts.size(), stream, wide);
             c.staging.assign(2 * counts.size() + 1, 0u);
-            std::uint32_t run = 0;
+            c.staging64.assign(wide ? counts.size() + 1 : 0, 0u);
+            std::uint64_t run = 0;
             for (std::size_t i = 0; i < counts.size(); ++i) {
                 c.staging[i] = std::uint32_t(counts[i]);
-                c.staging[counts.size() + i] = run;
-                run += std::uint32_t(counts[i]);
+                if (wide) c.staging64[i] = run;
+                else c.staging[counts.size() + i] = std::uint32_t(run);
+                run += counts[i];
             }
-            c.staging[2 * counts.size()] = run;
+            if (wide) c.staging64[counts.size()] = run;
+            else c.staging[2 * counts.size()] = std::uint32_t(run);
             // staging is pageable: each copy has consumed it when the call returns
             if (!counts.empty())
                 cuda_check(cudaMemcpyAsync(c.ext, c.staging.data(), counts.size() * 4, cudaMemcpyHostToDevice, stream), who);
-            cuda_check(cudaMemcpyAsync(c.offs, c.staging.data() + counts.size(), (counts.size() + 1) * 4,
-                                       cudaMemcpyHostToDevice, stream), who);
+            if (wide)
+                cuda_check(cudaMemcpyAsync(c.offs64, c.staging64.data(), (counts.size() + 1) * 8, cudaMemcpyHostToDevice,
+                                           stream), who);
+            else
+                cuda_check(cudaMemcpyAsync(c.offs, c.staging.data() + counts.size(), (counts.size() + 1) * 4,
+                                           cudaMemcpyHostToDevice, stream), who);
             c.uploaded = counts;
             c.has_upload = true;
             c.n = counts.size();
@@ -495,8 +534,8 @@ public:
     /// the device column (or, on a dense rank-2 variable, the row length).
     void bind(ComponentBase* c, detail::PortRec& p, Var& v) {
         if (p.ragged) {
-            if (v.per) p.bind_ragged(v.data, v.shape[0], v.column->offs, v.column->ext, 0);
-            else p.bind_ragged(v.data, v.shape[0], nullptr, nullptr, v.shape[1]);
+            if (v.per) p.bind_ragged(v.data, v.shape[0], v.column->offs, v.column->offs64, v.column->ext, 0);
+            else p.bind_ragged(v.data, v.shape[0], nullptr, nullptr, nullptr, v.shape[1]);
             return;
         }
         if (v.per)
@@ -1019,13 +1058,13 @@ public:
     /// Block i is data()[offsets[i], offsets[i + 1]).
     std::vector<std::uint64_t> block_offsets() const {
         std::vector<std::uint64_t> o(s_->n + 1, 0);
-        for (std::size_t i = 0; i <= s_->n; ++i) o[i] = s_->per ? std::uint64_t(s_->host_offs[i]) : std::uint64_t(i) * s_->row;
+        for (std::size_t i = 0; i <= s_->n; ++i) o[i] = s_->off(i);
         return o;
     }
     std::span<const value_type> block(std::size_t i) const {
         if (i >= s_->n) throw std::out_of_range("naga::cospan: HostRagged::block past the last block");
-        const std::uint64_t a = s_->per ? s_->host_offs[i] : std::uint64_t(i) * s_->row;
-        const std::uint64_t b = s_->per ? s_->host_offs[i + 1] : std::uint64_t(i + 1) * s_->row;
+        const std::uint64_t a = s_->off(i);
+        const std::uint64_t b = s_->off(i + 1);
         return std::span<const value_type>(data() + a, std::size_t(b - a));
     }
 
@@ -1256,14 +1295,22 @@ private:
         if (!s.ev) detail::cuda_check(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming), "view event");
         if (b) detail::cuda_check(cudaMemcpyAsync(s.host, v.data, b, cudaMemcpyDeviceToHost, rt_->stream), "view push");
         if (s.ragged && v.per) {
-            if (s.offs_cap < s.n + 1) {
+            const bool wide = v.column->wide;
+            if (s.offs_cap < s.n + 1 || wide != (s.host_offs64 != nullptr)) {
                 if (s.host_offs) cudaFreeHost(s.host_offs);
+                if (s.host_offs64) cudaFreeHost(s.host_offs64);
                 s.host_offs = nullptr;
-                detail::cuda_check(cudaMallocHost(reinterpret_cast<void**>(&s.host_offs), (s.n + 1) * 4), "host view");
+                s.host_offs64 = nullptr;
+                void** dst = wide ? reinterpret_cast<void**>(&s.host_offs64) : reinterpret_cast<void**>(&s.host_offs);
+                detail::cuda_check(cudaMallocHost(dst, (s.n + 1) * (wide ? 8 : 4)), "host view");
                 s.offs_cap = s.n + 1;
             }
-            detail::cuda_check(cudaMemcpyAsync(s.host_offs, v.column->offs, (s.n + 1) * 4, cudaMemcpyDeviceToHost, rt_->stream),
-                               "view push");
+            if (wide)
+                detail::cuda_check(cudaMemcpyAsync(s.host_offs64, v.column->offs64, (s.n + 1) * 8, cudaMemcpyDeviceToHost,
+                                                   rt_->stream), "view push");
+            else
+                detail::cuda_check(cudaMemcpyAsync(s.host_offs, v.column->offs, (s.n + 1) * 4, cudaMemcpyDeviceToHost,
+                                                   rt_->stream), "view push");
         }
         detail::cuda_check(cudaEventRecord(s.ev, rt_->stream), "view event");
     }

@@ -33,11 +33,23 @@ inline Custom custom(std::function<std::size_t(ShapeHookCtx&)> fn) { return Cust
 }  // namespace dim
 namespace ragged {
 /// the per-index counts are the values of an integer variable (rank 1 [N], or column 0 of a rank-2 [N, k])
-struct CountsFrom { std::string path; };
+struct CountsFrom { std::string path; bool wide = false; };
 /// the N + 1 block offsets are the values of a rank-1 integer variable
-struct OffsetsFrom { std::string path; };
-inline CountsFrom counts_from(std::string path) { return CountsFrom{std::move(path)}; }
-inline OffsetsFrom offsets_from(std::string path) { return OffsetsFrom{std::move(path)}; }
+struct OffsetsFrom { std::string path; bool wide = false; };
+/// Offset is the column's offset type: std::uint32_t (the reference's, and the default: the total stays below 2^32)
+/// or std::uint64_t (a total past 2^32 - 1, at 8 bytes per offset). Extents are u32 either way.
+template <class Offset = std::uint32_t>
+inline CountsFrom counts_from(std::string path) {
+    static_assert(std::is_same_v<Offset, std::uint32_t> || std::is_same_v<Offset, std::uint64_t>,
+                  "naga::cospan: a ragged column's offsets are std::uint32_t or std::uint64_t");
+    return CountsFrom{std::move(path), sizeof(Offset) == 8};
+}
+template <class Offset = std::uint32_t>
+inline OffsetsFrom offsets_from(std::string path) {
+    static_assert(std::is_same_v<Offset, std::uint32_t> || std::is_same_v<Offset, std::uint64_t>,
+                  "naga::cospan: a ragged column's offsets are std::uint32_t or std::uint64_t");
+    return OffsetsFrom{std::move(path), sizeof(Offset) == 8};
+}
 }  // namespace ragged
 using HookDim = std::variant<dim::AsIs, dim::FixedAtRun, dim::FromShape, dim::FromValue, dim::Custom, ragged::CountsFrom,
                              ragged::OffsetsFrom>;

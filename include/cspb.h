@@ -456,6 +456,16 @@ int cspb_build_column(const void* src, int32_t src_dtype, int64_t count, int64_t
                       uint32_t* extents, uint32_t* offs, uint32_t* total_flag, void* workspace,
                       size_t workspace_bytes, void* stream);
 
+/* The same column with 64-bit offsets (offs: count + 1 u64 in counts mode, N + 1 in offsets mode), for a ragged
+ * variable whose total may pass 2^32 - 1: the runtime's opt-in u64 offset type (cs::ragged::counts_from<uint64_t>),
+ * which the reference's roadmap names as the next step for its u32-only columns (internal/ROADMAP.md:106; today
+ * shape_hook.hpp:455-457 rejects such totals). Each extent is still a u32: flag 2 marks a single value or offset
+ * difference past 2^32 - 1, never the total. total_flag (2 u64) receives [offs[N], flag], the flag word holding the
+ * same bits as cspb_build_column's total_flag[1]. */
+int cspb_build_column64(const void* src, int32_t src_dtype, int64_t count, int64_t k, int32_t offsets_mode,
+                        uint32_t* extents, uint64_t* offs, uint64_t* total_flag, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
 /* ==================================================================================================================
  * cspb_build_column_static: cspb_build_column with no workspace argument, for callers that cannot allocate device
  * memory at the call site (a foreign-language binding that holds only the column's pointers and no allocator, code

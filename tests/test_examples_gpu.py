@@ -51,6 +51,13 @@ def test_runtime_replay(cuda):
     assert rc == 0 and "ALL OK" in out, out
 
 
+def test_runtime_ragged_u64_offsets(cuda):
+    """A ragged variable of 2^32 + 11 elements: counts_from<std::uint64_t> (and host counts past 2^32 - 1) place every
+    block where its u64 offset says; the default u32 column refuses the total with an error naming the u64 form."""
+    rc, out = _run(["runtime-ragged-wide"])
+    assert rc == 0 and "ALL OK" in out, out[-3000:]
+
+
 def test_runtime_decoy_component_not_replaced(cuda):
     """A component named Gemv with the reference's ports and wiring but other arithmetic is not replaced by the GEMVER
     kernel: the first forward compares kernel and bodies, and only the honest system keeps the kernel."""

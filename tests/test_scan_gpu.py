@@ -91,3 +91,53 @@ def test_build_column_flags_raise_like_the_reference(cuda):
         cb.build_column(torch.tensor([1, 2], dtype=torch.int32, device=cuda), offsets_mode=True)
     with pytest.raises(ValueError, match="negative"):
         cb.build_column(torch.tensor([0, 5, 3], dtype=torch.int32, device=cuda), offsets_mode=True)
+
+
+def test_build_column64_total_past_2_32(cuda):
+    """cspb_build_column64: u64 offsets for a column whose total passes 2^32 - 1 (the u32 builder flags it as too large);
+    each extent stays a u32, so a single count or offset difference past 2^32 - 1 is still flag 2."""
+    import ctypes as C
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200 import _capi
+    lib = cb.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def build(src_np, dtype_code, offsets_mode):
+        src = torch.from_numpy(src_np).to(cuda)
+        count = src_np.shape[0]
+        n = count - 1 if offsets_mode else count
+        ext = torch.zeros(max(n, 1), dtype=torch.int32, device=cuda)
+        offs = torch.zeros(n + 1, dtype=torch.int64, device=cuda)
+        tf = torch.full((2,), -1, dtype=torch.int64, device=cuda)
+        wb = lib.cspb_scan_workspace_bytes(n)
+        ws = torch.empty(wb + 256, dtype=torch.uint8, device=cuda)
+        wp = (ws.data_ptr() + 255) // 256 * 256
+        rc = lib.cspb_build_column64(C.c_void_p(src.data_ptr()), dtype_code, count, 1, int(offsets_mode),
+                                     C.c_void_p(ext.data_ptr()), C.c_void_p(offs.data_ptr()), C.c_void_p(tf.data_ptr()),
+                                     C.c_void_p(wp), wb, st)
+        assert rc == 0, rc
+        torch.cuda.synchronize()
+        return (ext[:n].cpu().numpy().view(np.uint32), offs.cpu().numpy().view(np.uint64),
+                tf.cpu().numpy().view(np.uint64))
+
+    rng = np.random.default_rng(11)
+    counts = np.concatenate([[2 ** 31 + 3, 2 ** 31 + 1], rng.integers(0, 1000, 20001)]).astype(np.int64)
+    want = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    ext, offs, tf = build(counts, _capi.I64, False)
+    assert np.array_equal(offs, want) and int(tf[0]) == int(want[-1]) > 2 ** 32 and int(tf[1]) == 0
+    assert np.array_equal(ext.astype(np.int64), counts)
+    # the u32 builder refuses the same counts (flag 2: the total passes 2^32 - 1)
+    with pytest.raises(ValueError, match="2\\^32"):
+        cb.build_column(torch.from_numpy(counts).to(cuda))
+    # offsets mode: the N + 1 offsets themselves, past 2^32
+    ext2, offs2, tf2 = build(want.astype(np.int64), _capi.I64, True)
+    assert np.array_equal(offs2, want) and np.array_equal(ext2.astype(np.int64), counts) and int(tf2[1]) == 0
+    assert int(tf2[0]) == int(want[-1])
+    # a single count past 2^32 - 1, and an offset difference past it, are flag 2; a decrease is flag 1
+    _, _, tf3 = build(np.array([5, 2 ** 32 + 1, 3], dtype=np.int64), _capi.I64, False)
+    assert int(tf3[1]) & 0xffffffff == 2
+    _, _, tf4 = build(np.array([0, 2 ** 32 + 1, 2 ** 32 + 4], dtype=np.int64), _capi.I64, True)
+    assert int(tf4[1]) & 0xffffffff == 2
+    _, _, tf5 = build(np.array([0, 9, 4], dtype=np.int64), _capi.I64, True)
+    assert int(tf5[1]) & 0xffffffff == 1
