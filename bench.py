@@ -534,6 +534,24 @@ def bench_serving(torch, dist, args):
     pl = serving.plain(wl)
     res["plain_f32_saturation"] = {k: v for k, v in pl.items() if k not in ("out", "norms")}
     res["throughput_ratio_batched_over_plain"] = sat["req_per_s"] / pl["req_per_s"]
+    # like for like: the per-request path with the server's storage and bytes (no Â), and a batched FP32 server, so
+    # that each ratio below is the batching alone at equal precision and equal bytes
+    pl_b16 = serving.plain(wl, dtype=torch.bfloat16, want_B=False)
+    pl_f32 = serving.plain(wl, want_B=False)
+    srv32 = serving.Server(wl, budget_bytes=120e9, max_batch=args.max_batch, depth=4, dtype=torch.float32)
+    srv32.run()  # warm-up pass
+    runs32 = sorted((srv32.run() for _ in range(3)), key=lambda r: r["req_per_s"])
+    sat32 = dict(runs32[1], runs_req_per_s=[r["req_per_s"] for r in runs32])
+    del srv32
+    torch.cuda.empty_cache()
+    strip = lambda d: {k: v for k, v in d.items() if k not in ("out", "norms")}  # noqa: E731
+    res["plain_bf16_noB_saturation"] = strip(pl_b16)
+    res["plain_f32_noB_saturation"] = strip(pl_f32)
+    res["batched_f32_noB_saturation"] = sat32
+    res["like_for_like_ratio"] = {
+        "bf16_noB_batched_over_plain": sat["req_per_s"] / pl_b16["req_per_s"],
+        "f32_noB_batched_over_plain": sat32["req_per_s"] / pl_f32["req_per_s"],
+        "bytes_only_plain_bf16_noB_over_plain_f32_withB": pl_b16["req_per_s"] / pl["req_per_s"]}
     rate = 0.5 * sat["req_per_s"]
     wl2 = serving.make_workload(args.requests, rate=rate, seed=1)
     srv2 = serving.Server(wl2, budget_bytes=120e9, max_batch=args.max_batch, depth=4)

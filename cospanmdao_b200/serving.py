@@ -18,7 +18,9 @@ back in one device→host copy per kind, and records an event. Batches on differ
 Completion times come from CUDA events on a common origin, so latency = device completion − arrival.
 
 `plain()` serves the same requests the way a caller without batching would: one request at a time, FP32 storage,
-the fused single-request kernels (Â written, as the reference's gemver does), one stream.
+the fused single-request kernels (Â written, as the reference's gemver does), one stream. Its dtype / want_B options
+give it the server's storage and bytes (BF16 or FP32 without Â), so that a throughput ratio at equal precision and
+equal bytes shows what the batching alone buys.
 
 Per-request results do not depend on the batch a request lands in (task tables compute each task exactly as the
 single call does); `check_mix()` verifies it.
@@ -385,22 +387,25 @@ class Server:
 
 
 # ---- the per-request FP32 path ---------------------------------------------------------------------------------
-def plain(wl: Workload, *, device=None, stream=None) -> dict:
-    """Each request on its own: FP32 models, the single-request kernels, one stream, no batching."""
+def plain(wl: Workload, *, device=None, stream=None, dtype=None, want_B: bool = True) -> dict:
+    """Each request on its own: the single-request kernels, one stream, no batching. By default FP32 models with Â
+    written (what a caller of the reference's gemver gets); dtype=bfloat16 and/or want_B=False give the per-request
+    path the same storage and the same bytes as the batched server, so that the two differ by the batching alone."""
     import cospanmdao_b200 as cb
     from . import workloads
     torch = _torch()
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    gdt = dtype or torch.float32
     models = {}
     for m, (kind, size) in wl.model_size.items():
         if kind == KIND_GEMVER:
-            models[m] = {"A": model_matrix(size, torch.float32, 16 * (1000 + m) + 1, dev)}
+            models[m] = {"A": model_matrix(size, gdt, 16 * (1000 + m) + 1, dev)}
         else:
             u, v, p, h = workloads.ns_fields(size, seed=1000 + m, dtype=torch.float32, device=dev)
             models[m] = {"u": u, "v": v, "p": p, "h": h}
     nmax = max(s for k, s in wl.model_size.values() if k == KIND_GEMVER)
     gmax = max(s for k, s in wl.model_size.values() if k == KIND_NS)
-    B = torch.empty(nmax * nmax, dtype=torch.float32, device=dev)
+    B = torch.empty(nmax * nmax if want_B else 1, dtype=torch.float32, device=dev)
     vin = torch.empty(6 * nmax, dtype=torch.float32, device=dev)
     xw = torch.empty(2 * nmax, dtype=torch.float32, device=dev)
     rns = [torch.empty(gmax * gmax, dtype=torch.float32, device=dev) for _ in range(3)]
@@ -426,8 +431,8 @@ def plain(wl: Workload, *, device=None, stream=None) -> dict:
                 a, b = int(wl.in_off[r]), int(wl.in_off[r + 1])
                 vin[:b - a].copy_(wl.inputs[a:b], non_blocking=True)
                 v = [vin[k * n:(k + 1) * n] for k in range(6)]
-                cb.gemver(md["A"], *v, alpha=wl.alpha, beta=wl.beta, B=B[:n * n].view(n, n), x=xw[:n],
-                          w=xw[n:2 * n], workspace=ws, stream=s)
+                cb.gemver(md["A"], *v, alpha=wl.alpha, beta=wl.beta, want_B=want_B,
+                          B=B[:n * n].view(n, n) if want_B else None, x=xw[:n], w=xw[n:2 * n], workspace=ws, stream=s)
                 o = int(wl.out_off[r])
                 out[o:o + 2 * n].copy_(xw[:2 * n], non_blocking=True)
             else:
