@@ -426,11 +426,12 @@ def bench_ns(torch, cb, dist, args):
 
 def bench_scan(torch, cb, dist, args, peak):
     """The single-pass decoupled-lookback scan (cspb_exclusive_scan_u32 / _u64) and the fused ragged-column builder
-    (cspb_build_column, counts mode from i32) at 2^28 items: algorithmic bytes 8 B/item (u32 in, u32 out), 16 B/item
-    (u64) and 12 B/item (i32 counts in, u32 extents and u32 offsets out). Inputs are 1..2 GiB, larger than L2."""
+    (cspb_build_column, counts mode from i32) at 2^28 items (--scan-log2): algorithmic bytes 8 B/item (u32 in, u32 out),
+    16 B/item (u64) and 12 B/item (i32 counts in, u32 extents and u32 offsets out). Inputs are 1..2 GiB at 2^28, larger
+    than L2 from 2^25 on."""
     import ctypes
     from cospanmdao_b200 import _capi
-    n = 1 << 28
+    n = 1 << args.scan_log2
     dev = torch.device("cuda", torch.cuda.current_device())
     lib = cb.lib()
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -673,6 +674,7 @@ def main(argv=None) -> int:
     ap.add_argument("--ragged", type=int, default=4096, help="instances of the ragged batch")
     ap.add_argument("--requests", type=int, default=20000, help="requests of the serving stream")
     ap.add_argument("--max-batch", type=int, default=512, help="serving: requests per batch at most")
+    ap.add_argument("--scan-log2", type=int, default=28, help="scan: log2 of the items per launch")
     ap.add_argument("--only", default="", help="comma list of secondary workloads to run (gemver_bf16_storage, "
                     "gemver_chain, ns_residual, ragged_batch, scan, serving, reference_programs); default all, none with "
                     "--quick")
