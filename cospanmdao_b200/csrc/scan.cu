@@ -17,6 +17,8 @@
 // kernel: the narrowing of the source values (negative -> flag 1, past 32 bits -> flag 2) happens as the tile loads,
 // the running sum is carried in 64 bits so that a total past 2^32 - 1 is known exactly (the reference detects the same
 // thing as a decrease of the wrapped u32 offsets), and the last tile writes [total, flag].
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace cspb {
@@ -108,10 +110,11 @@ template <> struct TileStat<uint64_t> {
     }
 };
 
-// Predecessors each lane of the looking-back warp reads per round: one round covers 32·kLook tiles, so the
-// look-back reaches a published prefix in one L2 round trip even when hundreds of tiles are in flight (u64 reads two
-// words per tile: 4 tiles a lane keep its registers at the u32 count).
-template <typename T> inline constexpr int kLook = 8 / TileStat<T>::kWords;
+// Predecessors each lane of the looking-back warp reads per round: one round covers 32·kLook tiles. One tile a lane
+// (32 a round) is the fastest on B200 at 2^28 u32 items: 0.76 ms against 0.81 (2 a lane), 0.95 (4) and 1.33 (8), at 6
+// blocks per SM. A round's status words are the lines every looking-back warp polls, and a round of 256 tiles (16
+// lines) made each poll several times slower than the walk back it saved.
+template <typename T> inline constexpr int kLook = 1;
 
 template <typename T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
@@ -124,8 +127,22 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
     return v;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
+// Where a tile's items come from: a plain array, or a column's count values of a 32-bit or a 64-bit dtype.
+enum ScanMode : int { kPlain = 0, kColumn32 = 1, kColumn64 = 2 };
+
+// A column value of a 32-bit dtype, kept in 32 bits until it is narrowed (a signed value is sign-extended then).
+__device__ __forceinline__ uint32_t load_column32(const ScanSrc& s, int64_t i) {
+    return __ldg(static_cast<const uint32_t*>(s.in) + i * s.k);
+}
+__device__ __forceinline__ uint64_t widen_column32(int32_t dtype, uint32_t raw) {
+    return dtype == CSPB_I32 ? uint64_t(int64_t(int32_t(raw))) : uint64_t(raw);
+}
+
+// 8 blocks per SM (32 registers) for the plain and the 32-bit column tiles: the whole SM's warp slots hold tiles, and a
+// tile spends most of its life in the look-back, so the tiles resident decide the bytes in flight (2^28 u32: 0.67 ms
+// against 0.76 ms at 6 blocks). A 64-bit column tile holds 16 raw 64-bit values in flight: 6 blocks.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kScanThreads, MODE == kColumn64 ? 6 : 8) k_scan(ScanK<T> g) {
     constexpr int IT = ScanItems<T>::N;
     constexpr int TILE = kScanThreads * IT;
     constexpr int PAD = TILE + TILE / 32;
@@ -144,7 +161,7 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
     // store: the loads go through the read-only global path into registers, then the stores follow (a load through a
     // generic pointer, stored to shared memory in the same loop, could not be moved past the previous store).
     uint32_t flag = 0;
-    if (!g.src.column) {
+    if constexpr (MODE == kPlain) {
         T x[IT];
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
@@ -157,11 +174,13 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
             sm[idx + idx / 32] = x[k];
         }
     } else {
-        uint64_t raw[IT];
+        using Raw = std::conditional_t<MODE == kColumn32, uint32_t, uint64_t>;
+        Raw raw[IT];
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
             const int64_t i = base + k * kScanThreads + t;
-            raw[k] = i < g.n ? load_column(g.src, i) : 0ull;
+            if constexpr (MODE == kColumn32) raw[k] = i < g.n ? load_column32(g.src, i) : 0u;
+            else raw[k] = i < g.n ? load_column(g.src, i) : 0ull;
         }
 #pragma unroll
         for (int k = 0; k < IT; ++k) {
@@ -169,7 +188,8 @@ __global__ void __launch_bounds__(kScanThreads, 6) k_scan(ScanK<T> g) {
             const int64_t i = base + idx;
             uint32_t x = 0;
             if (i < g.n) {
-                x = narrow(g.src.dtype, raw[k], flag);
+                if constexpr (MODE == kColumn32) x = narrow(g.src.dtype, widen_column32(g.src.dtype, raw[k]), flag);
+                else x = narrow(g.src.dtype, raw[k], flag);
                 __stcg(g.src.extents + i, x);
             }
             sm[idx + idx / 32] = T(x);
@@ -446,7 +466,10 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
     g.tstat = reinterpret_cast<uint64_t*>(w + L.off_stat);
     g.total_flag = total_flag;
     g.total64 = total64;
-    k_scan<T><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+    if (!src.column) k_scan<T, kPlain><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+    else if (src.dtype == CSPB_I32 || src.dtype == CSPB_U32)
+        k_scan<T, kColumn32><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+    else k_scan<T, kColumn64><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
