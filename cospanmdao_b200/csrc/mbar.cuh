@@ -52,6 +52,23 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
+// One untiled bulk copy (TMA) of `bytes` from this GPU's global memory into this CTA's shared memory, completing on
+// `bar`: both addresses 16-byte aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Bounded wait for the phase of `parity` that looks at nothing but the time: for a copy this thread's CTA has in
+// flight, which must land before the CTA may leave even when another tile has given up. false after the budget.
+__device__ __forceinline__ bool mbar_wait_own_copy(uint64_t* bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_test(bar, parity))
+        if (globaltimer_ns() - t0 > kWaitBudgetNs) return false;
+    return true;
+}
 // Orders this thread's earlier generic-proxy accesses of shared memory before later async-proxy (TMA) ones.
 __device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }

@@ -44,6 +44,29 @@ def test_scan_u64(cuda, n):
     assert np.array_equal(out.cpu().numpy().view(np.uint64), oracle.exclusive_scan(v))
 
 
+@pytest.mark.parametrize("misaligned", [False, True], ids=["bulk-tiles", "register-tiles"])
+@pytest.mark.parametrize("wide", [False, True], ids=["u32", "u64"])
+@pytest.mark.parametrize("n", [1, 5, 3071, 3072, 3073, 6143, 6144, 6145, 12289, (1 << 22) + 3])
+def test_scan_bulk_and_register_tiles(cuda, n, wide, misaligned):
+    """16-byte aligned input and output take the bulk-copy tiles (6144 u32 / 3072 u64 items); an array that starts one
+    element off a 16-byte boundary takes the register-loaded tiles. Both are bit-exact, at and around the tile sizes."""
+    import torch
+    import cospanmdao_b200 as cb
+    rng = np.random.default_rng(n * 2 + wide)
+    npdt, tdt = (np.uint64, torch.int64) if wide else (np.uint32, torch.int32)
+    v = rng.integers(0, np.iinfo(npdt).max, size=n + 1, dtype=np.uint64).astype(npdt)
+    src = torch.from_numpy(v.view(np.int64 if wide else np.int32)).to(cuda)
+    vals = src[1:] if misaligned else src[:n]
+    store = torch.full((n + 2,), -1, dtype=tdt, device=cuda)
+    out = store[1:] if misaligned else store[:n + 1]
+    assert (vals.data_ptr() % 16 == 0) != misaligned and (out.data_ptr() % 16 == 0) != misaligned
+    cb.exclusive_scan(vals, out=out)
+    want = oracle.exclusive_scan(v[1:] if misaligned else v[:n])
+    assert np.array_equal(out.cpu().numpy().view(npdt), want)
+    if not misaligned:
+        assert int(store[n + 1]) == -1  # nothing past out[n]
+
+
 def test_scan_repeat_is_identical(cuda):
     import torch
     import cospanmdao_b200 as cb
