@@ -67,6 +67,11 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
 
 __device__ __forceinline__ void set_status(uint32_t* ctrl, uint32_t bits) { atomicOr(ctrl + kStatus, bits); }
 __device__ __forceinline__ bool status_bad(const uint32_t* ctrl) { return ld_volatile(ctrl + kStatus) != 0u; }
+// Only a wait that gave up (CSPB_DEV_TIMEOUT): for kernels whose data flags (a negative count, a total past 2^32 - 1)
+// share the status word but must not end the other tiles' waits.
+__device__ __forceinline__ bool status_timed_out(const uint32_t* ctrl) {
+    return (ld_volatile(ctrl + kStatus) & CSPB_DEV_TIMEOUT) != 0u;
+}
 
 // Wait until *flag != old (acquire). Returns false (and sets CSPB_DEV_TIMEOUT) if the budget runs out or another
 // waiter has already given up. Called by ONE thread.

@@ -176,7 +176,7 @@ __device__ __forceinline__ void tile_lookback(const ScanK<T>& g, uint32_t tile, 
                 if (!__any_sync(0xffffffffu, wait)) break;
                 int give_up = 0;
                 if (lane == 0) {
-                    if (status_bad(g.ctrl)) give_up = 1;
+                    if (status_timed_out(g.ctrl)) give_up = 1;
                     else if (globaltimer_ns() - t0 > kWaitBudgetNs) {
                         set_status(g.ctrl, CSPB_DEV_TIMEOUT);
                         // a column build also reports it beside its other flags: a caller without the
@@ -472,6 +472,145 @@ __global__ void __launch_bounds__(kBulkThreads, 9) k_scan_bulk(ScanK<T> g) {
     if (tile == g.tiles - 1 && t == kBulkThreads - 1) out[g.n] = carry;  // the total
 }
 
+// Counts mode of build_column on bulk tiles: a 32-bit count source with stride 1. Pass 1 narrows the counts (a
+// negative i32 is 0 and flag 1), writes the extents and the narrowed values back to the tile, and sums them in 64 bits;
+// pass 2 scans them from the tile's prefix into u32 offsets (out32) or u64 offsets (out). The extents, the offsets and
+// the flags are those of k_scan's column mode.
+template <bool SIGNED>
+__global__ void __launch_bounds__(kBulkThreads, 9) k_column_bulk(ScanK<uint64_t> g) {
+    constexpr int TILE = BulkTile<uint32_t>::kItems;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint64_t s_wsum[4];
+    __shared__ uint64_t s_prefix;
+    __shared__ uint32_t s_flag;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        s_flag = 0;
+    }
+    const uint32_t tile = grab_work(g.ctrl, kWork0);
+    if (tile >= g.tiles) return;
+    const int64_t base = int64_t(tile) * TILE;
+    const int64_t cnt = g.n - base < TILE ? g.n - base : TILE;
+    const uint32_t* in = static_cast<const uint32_t*>(g.src.in);
+    if (cnt == TILE) {
+        if (t == 0) {
+            mbar_arrive_tx(&bar, BulkTile<uint32_t>::kBytes);
+            bulk_load_1d(dsm, in + base, BulkTile<uint32_t>::kBytes, &bar);
+        }
+        if (!mbar_wait_own_copy(&bar, 0)) {
+            set_status(g.ctrl, CSPB_DEV_TIMEOUT);
+            if (g.total_flag) atomicOr(g.total_flag + 1, CSPB_COLUMN_TIMEOUT);
+            return;
+        }
+    } else {
+        uint32_t* b32 = reinterpret_cast<uint32_t*>(dsm);
+        for (int i = t; i < TILE; i += kBulkThreads) b32[i] = i < cnt ? __ldg(in + base + i) : 0u;
+        __syncthreads();
+    }
+    uint4* buf = reinterpret_cast<uint4*>(dsm);
+    uint32_t* ext = g.src.extents;
+    // pass 1: narrow, extents, the warp's sum
+    uint64_t s = 0;
+    uint32_t flag = 0;
+#pragma unroll 4
+    for (int j = 0; j < kBulkRows; ++j) {
+        const int row = warp * kBulkRows + j;
+        uint4 v = buf[row * 32 + lane];
+        if constexpr (SIGNED) {
+            const auto nz = [&flag](uint32_t x) {
+                if (int32_t(x) < 0) {
+                    flag |= 1u;
+                    return 0u;
+                }
+                return x;
+            };
+            v.x = nz(v.x);
+            v.y = nz(v.y);
+            v.z = nz(v.z);
+            v.w = nz(v.w);
+            buf[row * 32 + lane] = v;
+        }
+        const int64_t i0 = base + int64_t(row) * 128 + lane * 4;
+        if (cnt == TILE) {
+            asm volatile("st.global.cg.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(ext + i0), "r"(v.x), "r"(v.y), "r"(v.z),
+                         "r"(v.w)
+                         : "memory");
+        } else {
+            const uint32_t o4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (i0 + k < g.n) __stcg(ext + i0 + k, o4[k]);
+        }
+        s += (uint64_t(v.x) + v.y) + (uint64_t(v.z) + v.w);
+    }
+    if (flag) atomicOr(&s_flag, flag);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) s_wsum[warp] = s;
+    __syncthreads();
+    const uint64_t agg = (s_wsum[0] + s_wsum[1]) + (s_wsum[2] + s_wsum[3]);
+    if (warp == 0) tile_lookback<uint64_t>(g, tile, agg, &s_prefix);
+    __syncthreads();
+    // pass 2: the offsets
+    uint64_t carry = s_prefix;
+#pragma unroll
+    for (int w = 0; w < 3; ++w)
+        if (w < warp) carry += s_wsum[w];
+#pragma unroll
+    for (int j = 0; j < kBulkRows; ++j) {
+        const int row = warp * kBulkRows + j;
+        const uint4 v = buf[row * 32 + lane];
+        const uint64_t c0 = v.x, c1 = c0 + v.y, c2 = c1 + v.z, c3 = c2 + v.w;
+        const uint64_t inc = warp_incl_scan(c3);
+        const uint64_t e = carry + inc - c3;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+        const uint64_t o[4] = {e, e + c0, e + c1, e + c2};
+        const int64_t i0 = base + int64_t(row) * 128 + lane * 4;
+        if (cnt == TILE) {
+            if (g.out32) {
+                asm volatile("st.global.cg.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(g.out32 + i0), "r"(uint32_t(o[0])),
+                             "r"(uint32_t(o[1])), "r"(uint32_t(o[2])), "r"(uint32_t(o[3]))
+                             : "memory");
+            } else {
+                asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(g.out + i0), "l"(o[0]), "l"(o[1]) : "memory");
+                asm volatile("st.global.cg.v2.u64 [%0], {%1, %2};" ::"l"(g.out + i0 + 2), "l"(o[2]), "l"(o[3])
+                             : "memory");
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (i0 + k < g.n) {
+                    if (g.out32) __stcg(g.out32 + i0 + k, uint32_t(o[k]));
+                    else __stcg(g.out + i0 + k, o[k]);
+                }
+        }
+    }
+    __syncthreads();  // every thread's flag is in s_flag
+    if (s_flag && t == 0) {
+        if (g.total_flag) atomicOr(g.total_flag + 1, s_flag);
+        set_status(g.ctrl, CSPB_DEV_NEGATIVE);
+    }
+    if (tile == g.tiles - 1 && t == kBulkThreads - 1) {
+        const uint64_t total = carry;
+        if (g.out32) {
+            g.out32[g.n] = uint32_t(total);
+            if (g.total_flag) {
+                g.total_flag[0] = uint32_t(total);
+                if (total > 0xffffffffull) {
+                    atomicOr(g.total_flag + 1, 2u);
+                    set_status(g.ctrl, CSPB_DEV_EXCEEDS32);
+                }
+            }
+        } else {
+            g.out[g.n] = total;
+            if (g.total64) g.total64[0] = total;
+        }
+    }
+}
+
 // Offsets mode of build_column: offs[i] = narrowed value (bad: negative, offs[0] != 0), extents from differences.
 __global__ void k_column_offsets(ScanSrc s, int64_t m, uint32_t* offs, uint32_t* ctrl, uint32_t* total_flag) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
@@ -597,7 +736,17 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
         g.tiles = (n + BulkTile<T>::kItems - 1) / BulkTile<T>::kItems;
         k_scan_bulk<T><<<unsigned(g.tiles), kBulkThreads, BulkTile<T>::kBytes, st>>>(g);
     } else if (!src.column) k_scan<T, kPlain><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
-    else if (src.dtype == CSPB_I32 || src.dtype == CSPB_U32)
+    else if constexpr (std::is_same_v<T, uint64_t>) {
+        if ((src.dtype == CSPB_I32 || src.dtype == CSPB_U32) && src.k == 1 && aligned(src.in, 16) &&
+            aligned(src.extents, 16) && aligned(out32 ? static_cast<const void*>(out32) : out, 16)) {
+            g.tiles = (n + BulkTile<uint32_t>::kItems - 1) / BulkTile<uint32_t>::kItems;
+            if (src.dtype == CSPB_I32)
+                k_column_bulk<true><<<unsigned(g.tiles), kBulkThreads, BulkTile<uint32_t>::kBytes, st>>>(g);
+            else k_column_bulk<false><<<unsigned(g.tiles), kBulkThreads, BulkTile<uint32_t>::kBytes, st>>>(g);
+        } else if (src.dtype == CSPB_I32 || src.dtype == CSPB_U32)
+            k_scan<T, kColumn32><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+        else k_scan<T, kColumn64><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
+    } else if (src.dtype == CSPB_I32 || src.dtype == CSPB_U32)
         k_scan<T, kColumn32><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     else k_scan<T, kColumn64><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;

@@ -164,3 +164,52 @@ def test_build_column64_total_past_2_32(cuda):
     assert int(tf4[1]) & 0xffffffff == 2
     _, _, tf5 = build(np.array([0, 9, 4], dtype=np.int64), _capi.I64, True)
     assert int(tf5[1]) & 0xffffffff == 1
+
+
+@pytest.mark.parametrize("misaligned", [False, True], ids=["bulk-tiles", "register-tiles"])
+@pytest.mark.parametrize("wide", [False, True], ids=["u32-offsets", "u64-offsets"])
+@pytest.mark.parametrize("dtype", ["int32", "uint32"])
+@pytest.mark.parametrize("n", [1, 6143, 6144, 6145, (1 << 20) + 7])
+def test_build_column_bulk_and_register_tiles(cuda, n, dtype, wide, misaligned):
+    """Counts from a 16-byte aligned 32-bit source take the bulk-copy tiles, a source one element off the boundary the
+    register-loaded tiles; extents, offsets, total and flag agree with the oracle either way, for u32 offsets
+    (cspb_build_column) and u64 offsets (cspb_build_column64), with and without negative counts (flag 1)."""
+    import ctypes as C
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200 import _capi
+    lib = cb.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(n + 3 * wide + 5 * misaligned)
+    for negative in (False, True):
+        v = rng.integers(0, 3000, size=n + 1).astype(np.int64)
+        if negative and dtype == "int32":
+            v[rng.integers(0, n + 1, size=3)] = -7
+        src_np = v.astype(dtype)
+        big = torch.from_numpy(src_np).to(cuda)
+        src = big[1:] if misaligned else big[:n]
+        assert (src.data_ptr() % 16 == 0) != misaligned
+        host = src_np[1:] if misaligned else src_np[:n]
+        ext = torch.zeros(n, dtype=torch.int32, device=cuda)
+        offs = torch.zeros(n + 1, dtype=torch.int64 if wide else torch.int32, device=cuda)
+        tf = torch.zeros(2, dtype=torch.int64 if wide else torch.int32, device=cuda)
+        wb = lib.cspb_scan_workspace_bytes(n)
+        ws = torch.empty(wb + 256, dtype=torch.uint8, device=cuda)
+        wp = C.c_void_p((ws.data_ptr() + 255) // 256 * 256)
+        code = _capi.I32 if dtype == "int32" else _capi.U32
+        f = lib.cspb_build_column64 if wide else lib.cspb_build_column
+        rc = f(C.c_void_p(src.data_ptr()), code, n, 1, 0, C.c_void_p(ext.data_ptr()), C.c_void_p(offs.data_ptr()),
+               C.c_void_p(tf.data_ptr()), wp, wb, st)
+        assert rc == 0, rc
+        torch.cuda.synchronize()
+        counts = np.where(host.astype(np.int64) < 0, 0, host.astype(np.int64))
+        want_offs = np.concatenate([[0], np.cumsum(counts)])
+        flag = 1 if (host.astype(np.int64) < 0).any() else 0
+        assert np.array_equal(ext.cpu().numpy().view(np.uint32).astype(np.int64), counts)
+        got = offs.cpu().numpy().view(np.uint64 if wide else np.uint32).astype(np.int64)
+        assert np.array_equal(got, want_offs)
+        tfh = tf.cpu().numpy().view(np.uint64 if wide else np.uint32)
+        assert int(tfh[0]) == int(want_offs[-1]) and int(tfh[1]) == flag
+        if not wide:
+            e2, o2, tot2, f2 = oracle.build_column(host)
+            assert np.array_equal(ext.cpu().numpy().view(np.uint32), e2) and tot2 == int(tfh[0]) and f2 == flag
