@@ -1,15 +1,14 @@
 // scan.cu — single-pass exclusive scan (decoupled lookback) of u32 / u64, and the fused ragged-column builder.
 //
 // Replaces cs::detail::exclusive_scan_u32 (cospanmdao/include/naga/cospan/device_scan.hpp:46-110), a recursive
-// reduce-then-scan of 3 kernels per level with temporary allocations, by ONE launch over tiles of 256 threads × ITEMS:
-//   1. a tile takes a dynamic tile index (so every tile it waits on has started), loads its items coalesced through
-//      shared memory, and scans them in the block;
-//   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 256 at a time (8 per lane,
-//      flag and value in one 64-bit word, so one round is one L2 round trip), adding aggregates until it meets a
-//      published inclusive prefix (flag 2), and publishes its own inclusive prefix. At B200's bandwidth a tile starts
-//      every few nanoseconds, so a look-back window of 32 tiles (two dependent loads per round: flag, then value)
-//      rarely reached a published prefix and walked back through hundreds of tiles;
-//   3. it writes its outputs coalesced; the last tile writes out[n], the total.
+// reduce-then-scan of 3 kernels per level with temporary allocations, by ONE launch over tiles:
+//   1. a tile takes a dynamic tile index (so every tile it waits on has started) and brings its items into shared
+//      memory: 16-byte aligned arrays with one untiled bulk copy of 24 KB per 128-thread tile (k_scan_bulk,
+//      k_column_bulk), other arrays with coalesced loads of 256 threads × ITEMS (k_scan);
+//   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 32 at a time (flag and value
+//      in one 64-bit word, so one round is one L2 round trip), adding aggregates until it meets a published inclusive
+//      prefix (flag 2), and publishes its own inclusive prefix;
+//   3. it scans its items from that prefix and writes them coalesced; the last tile writes out[n], the total.
 // Integer addition mod 2^32 / 2^64 is associative, so the result is bit-identical to std::exclusive_scan whatever the
 // order of the lookback. Every wait is bounded (common.cuh).
 //
