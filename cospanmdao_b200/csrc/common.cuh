@@ -28,6 +28,7 @@ enum CtrlWord : int {
     kBarrierGen = 2,
     kWork0 = 4,  // dynamic work counters kWork0 .. kWork0 + 7
     kDone0 = 12, // completion counters kDone0 .. kDone0 + 7
+    kDots0 = 32, // 4 f64 (words 32 .. 39): dot products one block forms for every block of the grid
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {

@@ -71,8 +71,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
 // GEMVER without Â (flag CSPB_GEMVER_LOWRANK, B not requested): the rank-2 update is applied as four dot products,
 //   Âᵀy = Aᵀy + v1(u1·y) + v2(u2·y),   Â·x = A·x + u1(v1·x) + u2(v2·x),
 // so the two passes over A are plain streaming GEMVs (column sums of A·y, then row dots of A·x) with no per-element
-// update, and the finishes add the rank-2 terms. The dots are formed by every block in the same order (block_dot2),
-// in f64. Measured at n = 16384 with bf16 storage, forming Â per element made each pass issue-bound at 3.3 TB/s.
+// update, and the finishes add the rank-2 terms. The dots are formed in f64 by block 0 (block_dot2, one fixed order)
+// and handed to every block through the control block. Measured at n = 16384 with bf16 storage, forming Â per element made each pass issue-bound at 3.3 TB/s.
 // Other rounding than the schedules that form Â (closer to the f64 result, not the same bits).
 struct LowRankK {
     PassArgs p1, p2;
@@ -94,6 +94,20 @@ template <typename T, bool STORE>
 __global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_lr(LowRankK g, int vec_ok) {
     constexpr int RB = kLrRB<T, STORE>;
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+    // The dot products of the finishes are formed by block 0 alone (block_dot2: one order, whatever the grid) and read
+    // by every block after the next grid barrier; every block forming them read 3 vectors each time (85 MB of L2 reads
+    // per finish at n = 16384 and 444 blocks).
+    double* dots = reinterpret_cast<double*>(g.ctrl + kDots0);
+    if constexpr (!STORE) {
+        if (blockIdx.x == 0) {  // u1·y, u2·y: inputs only
+            double s1, s2;
+            block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
+            if (threadIdx.x == 0) {
+                dots[0] = s1;
+                dots[1] = s2;
+            }
+        }
+    }
     for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0);
         if constexpr (STORE) pass_unit<T, kWX, true, true, false, true, false, 0>(g.p1, u, vec_ok != 0, smem);
@@ -104,20 +118,24 @@ __global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_
     if constexpr (STORE) {
         colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
     } else {
-        double s1, s2;
-        block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
-        colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, s1, s2, g.x);
+        colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, __ldcg(dots), __ldcg(dots + 1), g.x);
     }
     if (!grid_barrier(g.ctrl)) return;
+    if (blockIdx.x == 0) {  // v1·x, v2·x: x is complete after the barrier
+        double t1, t2;
+        block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
+        if (threadIdx.x == 0) {
+            dots[2] = t1;
+            dots[3] = t2;
+        }
+    }
     for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
         const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
         pass_unit<T, kWX, true, false, false, false, true, RB, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, smem);
         u = share_work(next);
     }
     if (!grid_barrier(g.ctrl)) return;
-    double t1, t2;
-    block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
-    rowsum_finish_lr(g.p2, g.u1, g.u2, t1, t2);
+    rowsum_finish_lr(g.p2, g.u1, g.u2, __ldcg(dots + 2), __ldcg(dots + 3));
 }
 
 // The same three passes with the matrix streamed through a shared-memory ring by bulk copies (bulkpass.cuh): one
