@@ -485,7 +485,8 @@ def bench_scan(torch, cb, dist, args, peak):
 
 def bench_ragged(torch, cb, dist, args, peak):
     """4096 independent GEMVERs, n ~ log-U[64, 4096], f32, packed, in one persistent launch with device-scanned u64
-    offsets, replayed as a CUDA graph; the tile geometry per size bucket picked by the autotuner."""
+    offsets, replayed as a CUDA graph; the tile geometry per size bucket, the work items per grab and the blocks
+    per SM picked by the autotuner."""
     from cospanmdao_b200 import workloads
     from cospanmdao_b200.batched import RaggedBatch, autotune
     sizes = workloads.ragged_sizes(args.ragged)
@@ -511,7 +512,8 @@ def bench_ragged(torch, cb, dist, args, peak):
     torch.cuda.empty_cache()
     return {"instances": int(sizes.size), "sum_n2": float((sizes.astype(np.float64) ** 2).sum()),
             "ms": ms, "gbs": gbs, "frac": gbs / peak["hbm_gbs"], "offsets_bit_exact": bool(offsets_ok),
-            "tune": tune, "tune_codes": tuned["codes"], "cuda_graph": True}
+            "tune": tune, "tune_codes": tuned["codes"], "tune_group": tuned["group"], "tune_blocks": tuned["blocks"],
+            "tune_trials": len(tuned["trials"]), "cuda_graph": True}
 
 
 def bench_serving(torch, dist, args):

@@ -145,8 +145,14 @@ def gemver_batched(sizes, *, seed: int = 0, dtype=None, want_B: bool = True, tun
 
 
 # ---- the autotuner --------------------------------------------------------------------------------------------------
-def tune_word(codes) -> int:
-    return int(sum((int(c) & 3) << (2 * b) for b, c in enumerate(codes)))
+GROUPS = (0, 1, 2, 3)  # work items per grab: 4, 1, 2, 8
+BLOCKS = (0, 1, 2, 3)  # blocks per SM: as many as fit, one fewer, two, one
+
+
+def tune_word(codes, group: int = 0, blocks: int = 0) -> int:
+    """The tuning word: 2 bits of tile geometry per size bucket, then the grab-group and blocks-per-SM codes."""
+    w = int(sum((int(c) & 3) << (2 * b) for b, c in enumerate(codes)))
+    return w | ((int(group) & 3) << 8) | ((int(blocks) & 3) << 10)
 
 
 def _cache_path() -> Path:
@@ -189,9 +195,11 @@ def _time_ms(batch: RaggedBatch, tune: int, reps: int) -> float:
 
 
 def autotune(batch: RaggedBatch, reps: int = 3, save: bool = True) -> dict:
-    """Coordinate descent over the four size buckets' geometry codes, device-timed on `batch`. Returns
-    {'tune': word, 'codes': [...], 'ms': best, 'trials': [...]} and caches it."""
+    """Coordinate descent, device-timed on `batch`, over the four size buckets' geometry codes, then the work items a
+    block takes per grab, then the blocks per SM. Returns {'tune': word, 'codes': [...], 'group': g, 'blocks': b,
+    'ms': best, 'trials': [...]} and caches it."""
     codes = [0, 0, 0, 0]
+    group = blocks = 0
     present = set(int(np.searchsorted(BUCKETS, n, side="right")) for n in batch.sizes)
     best = _time_ms(batch, tune_word(codes), reps)
     trials = [(tune_word(codes), best)]
@@ -207,7 +215,22 @@ def autotune(batch: RaggedBatch, reps: int = 3, save: bool = True) -> dict:
             trials.append((tune_word(trial), ms))
             if ms < best:
                 best, codes = ms, trial
-    res = {"tune": tune_word(codes), "codes": codes, "ms": best, "trials": trials}
+    for g in GROUPS:
+        if g == group:
+            continue
+        ms = _time_ms(batch, tune_word(codes, g, blocks), reps)
+        trials.append((tune_word(codes, g, blocks), ms))
+        if ms < best:
+            best, group = ms, g
+    for k in BLOCKS:
+        if k == blocks:
+            continue
+        ms = _time_ms(batch, tune_word(codes, group, k), reps)
+        trials.append((tune_word(codes, group, k), ms))
+        if ms < best:
+            best, blocks = ms, k
+    res = {"tune": tune_word(codes, group, blocks), "codes": codes, "group": group, "blocks": blocks, "ms": best,
+           "trials": trials}
     if save:
         with _cache_lock:
             p = _cache_path()
@@ -218,6 +241,7 @@ def autotune(batch: RaggedBatch, reps: int = 3, save: bool = True) -> dict:
                     data = json.loads(p.read_text())
                 except ValueError:
                     data = {}
-            data[_cache_key(batch)] = {"tune": res["tune"], "codes": codes, "ms": best}
+            data[_cache_key(batch)] = {"tune": res["tune"], "codes": codes, "group": group, "blocks": blocks,
+                                       "ms": best}
             p.write_text(json.dumps(data, indent=1))
     return res

@@ -22,7 +22,18 @@ namespace cspb {
 namespace batch {
 
 constexpr int kThreads = kPassThreads;
-constexpr uint32_t kGroup = 4;  // consecutive work items a block takes at once
+// tuning word bits 8..9: consecutive work items a block takes at once (0: 4, 1: 1, 2: 2, 3: 8); bits 10..11: blocks
+// per SM (0: as many as fit, 1: one fewer, 2: two, 3: one). Neither changes a result: every sum's order is fixed by
+// (n, dtype, the bucket codes) alone.
+__host__ __device__ inline uint32_t group_of(uint32_t tune) {
+    const uint32_t c = (tune >> 8) & 3u;
+    return c == 1 ? 1u : (c == 2 ? 2u : (c == 3 ? 8u : 4u));
+}
+__host__ __device__ inline int blocks_per_sm_of(uint32_t tune, int fit) {
+    const uint32_t c = (tune >> 10) & 3u;
+    const int b = c == 1 ? fit - 1 : (c == 2 ? 2 : (c == 3 ? 1 : fit));
+    return b < 1 ? 1 : (b > fit ? fit : b);
+}
 constexpr int kSets = 7;  // a, v, p, w, s, u, c
 enum { SA = 0, SV = 1, SP = 2, SW = 3, SS = 4, SU = 5, SC = 6 };
 
@@ -86,6 +97,7 @@ struct RunK {
     uint32_t* x_ready;     // [Σ units]: likewise, one flag per column chunk
     uint64_t cap_units;
     uint32_t* ctrl;
+    uint32_t group;  // work items per grab (group_of)
 };
 
 // the instance holding unit u (u_off[k] <= u < u_off[k+1]); instances with no units are skipped by construction
@@ -323,10 +335,11 @@ __global__ void __launch_bounds__(kThreads, (kRunBlocks<T, LEAN>)) k_run(RunK g)
         __syncthreads();
         return s_ok != 0;
     };
-    for (uint32_t base = grab_work(g.ctrl, kWork0, kGroup); uint64_t(base) < e4;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0, kGroup);
+    const uint32_t group = g.group;
+    for (uint32_t base = grab_work(g.ctrl, kWork0, group); uint64_t(base) < e4;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0, group);
         bool stop = false;
-        for (uint32_t q = 0; q < kGroup && !stop; ++q) {
+        for (uint32_t q = 0; q < group && !stop; ++q) {
             const uint64_t item = uint64_t(base) + q;
             if (item >= e4) break;
             if (item < e1 || (item >= e2 && item < e3)) {  // a unit of pass 1 or pass 2
@@ -460,7 +473,7 @@ size_t cspb_gemver_batched_workspace_bytes(int64_t count, int64_t max_elems, int
     return batch_layout(count, max_elems, max_vec).total;
 }
 
-int cspb_gemver_batched_tunings(void) { return 1 << 8; }
+int cspb_gemver_batched_tunings(void) { return 1 << 12; }
 
 }  // extern "C"
 
@@ -550,6 +563,8 @@ int run_batch(int64_t count, int64_t max_elems, int64_t max_vec, int32_t a_dtype
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, batch::kThreads, 0) != cudaSuccess || per_sm < 1)
         return CSPB_ERR_LAUNCH;
+    per_sm = batch::blocks_per_sm_of(uint32_t(tune), per_sm);
+    g.group = batch::group_of(uint32_t(tune));
     void* args[] = {&g};
     if (cudaLaunchKernel(kern, dim3(unsigned(per_sm * di.sms)), dim3(batch::kThreads), args, 0, st) != cudaSuccess)
         return CSPB_ERR_LAUNCH;

@@ -224,7 +224,9 @@ int cspb_gemver_chain(const cspb_chain_desc* d, void* stream);
  * kernel checks the device-computed totals against them before touching memory and sets CSPB_DEV_CAPACITY when they
  * do not fit (an invalid n[k] sets CSPB_DEV_NEGATIVE). Per-instance alpha[k], beta[k] are device arrays.
  * `tune` holds 2 bits per size bucket (n < 512, < 1024, < 2048, >= 2048) choosing the tile geometry of that bucket
- * (0: 8 warps as 2 × 4, 1: 1 × 8, 2: 4 × 2); results depend only on (n, dtype, tune), never on the rest of the batch.
+ * (0: 8 warps as 2 × 4, 1: 1 × 8, 2: 4 × 2); results depend only on (n, dtype, these bits), never on the rest of the
+ * batch. Bits 8..9 set the work items a block takes per grab (0: 4, 1: 1, 2: 2, 3: 8) and bits 10..11 the blocks per
+ * SM (0: as many as fit, 1: one fewer, 2: two, 3: one); neither changes a result.
  * Replaces the per-request launches a caller of the gemver example would make; ragged offsets follow
  * cs::ragged::counts_from (cospanmdao/include/naga/cospan/shape_hook.hpp:215-348) with u64 element offsets, since
  * 4096 instances of n up to 4096 overflow the reference's 32-bit offsets (device_scan.hpp:20-23).

@@ -77,6 +77,23 @@ def test_batched_every_tuning_within_tolerance(cuda):
             assert oracle.rel_l2(w, ref) < 2 * TOL
 
 
+def test_batched_group_and_blocks_do_not_change_bits(cuda):
+    """The work items a block takes per grab and the blocks per SM (tuning bits 8..11) move work between blocks only:
+    x, w and Â are bit-identical for every value."""
+    import torch
+    from cospanmdao_b200.batched import RaggedBatch, tune_word, GROUPS, BLOCKS
+    b = RaggedBatch(SIZES).fill(seed=2)
+    b.run(tune=tune_word([1, 2, 0, 1]))
+    torch.cuda.synchronize()
+    ref = (b.x.clone(), b.w.clone(), b.B.clone())
+    for g in GROUPS:
+        for k in BLOCKS:
+            b.x.fill_(float("nan"))
+            b.run(tune=tune_word([1, 2, 0, 1], g, k))
+            torch.cuda.synchronize()
+            assert torch.equal(b.x, ref[0]) and torch.equal(b.w, ref[1]) and torch.equal(b.B, ref[2]), (g, k)
+
+
 def test_batched_config_sizes_offsets_bit_exact(cuda):
     # the configuration's 4096 log-uniform sizes: the u64 offsets pass 2^32 and match the host's exactly
     import torch
