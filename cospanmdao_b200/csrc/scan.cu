@@ -2,13 +2,15 @@
 //
 // Replaces cs::detail::exclusive_scan_u32 (cospanmdao/include/naga/cospan/device_scan.hpp:46-110), a recursive
 // reduce-then-scan of 3 kernels per level with temporary allocations, by ONE launch over tiles:
-//   1. a tile takes a dynamic tile index (so every tile it waits on has started) and brings its items into shared
-//      memory: 16-byte aligned arrays with one untiled bulk copy of 24 KB per 128-thread tile (k_scan_bulk,
-//      k_column_bulk), other arrays with coalesced loads of 256 threads × ITEMS (k_scan);
+//   1. a tile takes a dynamic tile index (so every tile it waits on has started) and sums its items: 16-byte aligned
+//      plain arrays with 16-byte loads kept in L2 (k_scan_l2, 32 KB per 128-thread tile), a column from aligned 32-bit
+//      counts with one untiled bulk copy of 24 KB into shared memory (k_column_bulk), other arrays with coalesced
+//      loads of 256 threads × ITEMS through shared memory (k_scan);
 //   2. it publishes its aggregate (flag 1), then warp 0 looks back over its predecessors 32 at a time (flag and value
 //      in one 64-bit word, so one round is one L2 round trip), adding aggregates until it meets a published inclusive
 //      prefix (flag 2), and publishes its own inclusive prefix;
-//   3. it scans its items from that prefix and writes them coalesced; the last tile writes out[n], the total.
+//   3. it scans its items from that prefix (k_scan_l2 reads them again, from L2) and writes them coalesced; the last
+//      tile writes out[n], the total.
 // Integer addition mod 2^32 / 2^64 is associative, so the result is bit-identical to std::exclusive_scan whatever the
 // order of the lookback. Every wait is bounded (common.cuh).
 //
@@ -16,6 +18,7 @@
 // kernel: the narrowing of the source values (negative -> flag 1, past 32 bits -> flag 2) happens as the tile loads,
 // the running sum is carried in 64 bits so that a total past 2^32 - 1 is known exactly (the reference detects the same
 // thing as a decrease of the wrapped u32 offsets), and the last tile writes [total, flag].
+#include <cstring>
 #include <type_traits>
 
 #include "common.cuh"
@@ -353,12 +356,13 @@ __global__ void __launch_bounds__(kScanThreads, MODE == kColumn64 ? 6 : 8) k_sca
     }
 }
 
-// ---- bulk tiles: the plain scans of 16-byte aligned arrays ----------------------------------------------------------
-// A tile of 128 threads arrives with ONE untiled bulk copy (TMA) of 24 KB into shared memory: no registers hold
-// loads in flight, so 9 tiles fit an SM (216 KB) against 8 × 16 KB for the register-loaded tiles, and a tile in its
-// look-back holds only shared memory. Pass 1 sums each warp's 12 rows (a row = 32 lanes × 16 bytes, read
-// conflict-free), warp 0 looks back with the tile's aggregate, and pass 2 scans the rows again from the tile's prefix
-// and stores them with 16-byte stores. 2^28 u32 items: 0.515 ms against 0.67 ms for the register-loaded tiles.
+// ---- bulk tiles: build_column from 16-byte aligned 32-bit counts ----------------------------------------------------
+// A tile of 128 threads arrives with ONE untiled bulk copy (TMA) of 24 KB into shared memory: no registers hold loads
+// in flight, so 9 tiles fit an SM (216 KB), and a tile in its look-back holds only shared memory. Pass 1 narrows and
+// sums each warp's 12 rows (a row = 32 lanes × 16 bytes, read conflict-free), warp 0 looks back with the tile's
+// aggregate, and pass 2 scans the rows again from the tile's prefix and stores them with 16-byte stores. 2^28 i32
+// counts: 0.587 ms (84 % of the measured copy bandwidth; it writes twice the bytes it reads). The plain scans took
+// these tiles too (2^28 u32: 0.512 ms) before the L2 re-read tiles below.
 constexpr int kBulkThreads = 128;
 constexpr int kBulkRows = 12;  // rows per warp
 template <typename T> struct BulkTile {
@@ -387,48 +391,89 @@ template <> struct Vec16<uint64_t> {
     }
 };
 
+// ---- L2 re-read tiles: the plain scans of 16-byte aligned arrays -----------------------------------------------------
+// A tile of 128 threads reads its 32 KB from DRAM once in pass 1 (16-byte loads kept in L2 with an evict-last policy)
+// and sums it, warp 0 looks back with the tile's aggregate, and pass 2 reads the tile again (from L2, evict-first) and
+// scans and stores it. The tile holds no shared memory while it waits in the look-back, so 12 tiles fit an SM (3 ×
+// the bytes a bulk-copy tile could hold there) and their DRAM reads stay in flight; ~57 MB of tiles sit in L2 at a
+// time. 2^28 u32 items: 0.441 ms against 0.512 ms for the bulk-copy tiles and 0.52 ms for the same tiles without the
+// L2 policies.
+constexpr int kL2Threads = 128;
+constexpr int kL2Rows = 16;   // rows of 32 lanes × 16 bytes per warp
+constexpr int kL2Flight = 4;  // rows each lane keeps in flight
+template <typename T> struct L2Tile {
+    static constexpr int kVec = 16 / int(sizeof(T));
+    static constexpr int kItems = 4 * kL2Rows * 32 * kVec;  // 8192 u32 / 4096 u64
+};
+
+__device__ __forceinline__ uint4 ld_policy_u4(const void* p, uint64_t pol) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint64_t evict_last_l2_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+template <typename T> struct VecCs;
+template <> struct VecCs<uint32_t> {
+    static __device__ __forceinline__ void store(uint32_t* p, const uint32_t (&o)[4]) {
+        asm volatile("st.global.cs.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(o[0]), "r"(o[1]), "r"(o[2]), "r"(o[3])
+                     : "memory");
+    }
+};
+template <> struct VecCs<uint64_t> {
+    static __device__ __forceinline__ void store(uint64_t* p, const uint64_t (&o)[2]) {
+        asm volatile("st.global.cs.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(o[0]), "l"(o[1]) : "memory");
+    }
+};
+
+// A row of the tile as one 16-byte vector per lane: the whole vector when the tile is full, else element by element
+// (zero past n).
 template <typename T>
-__global__ void __launch_bounds__(kBulkThreads, 9) k_scan_bulk(ScanK<T> g) {
-    constexpr int E = BulkTile<T>::kVec;
-    constexpr int TILE = BulkTile<T>::kItems;
-    extern __shared__ __align__(128) unsigned char dsm[];
-    __shared__ __align__(8) uint64_t bar;
+__device__ __forceinline__ uint4 l2_row(const T* in, int64_t i0, int64_t n, bool full, uint64_t pol) {
+    if (full) return ld_policy_u4(in + i0, pol);
+    constexpr int E = 16 / int(sizeof(T));
+    T x[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) x[k] = i0 + k < n ? __ldg(in + i0 + k) : T(0);
+    uint4 v;
+    memcpy(&v, x, 16);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kL2Threads, 12) k_scan_l2(ScanK<T> g) {
+    constexpr int E = L2Tile<T>::kVec;
+    constexpr int TILE = L2Tile<T>::kItems;
+    constexpr int B = kL2Flight;
     __shared__ T s_wsum[4];
     __shared__ T s_prefix;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    if (t == 0) {
-        mbar_init(&bar, 1);
-        fence_mbar_init();
-    }
-    const uint32_t tile = grab_work(g.ctrl, kWork0);  // barriers on both sides: the barrier's init is seen
+    const uint32_t tile = grab_work(g.ctrl, kWork0);
     if (tile >= g.tiles) return;
     const int64_t base = int64_t(tile) * TILE;
-    const int64_t cnt = g.n - base < TILE ? g.n - base : TILE;
+    const bool full = g.n - base >= TILE;
     const T* in = static_cast<const T*>(g.src.in);
-    T* tbuf = reinterpret_cast<T*>(dsm);
-    if (cnt == TILE) {
-        if (t == 0) {
-            mbar_arrive_tx(&bar, BulkTile<T>::kBytes);
-            bulk_load_1d(dsm, in + base, BulkTile<T>::kBytes, &bar);
-        }
-        // every thread waits for the copy itself: a CTA leaves only after its copy has landed
-        if (!mbar_wait_own_copy(&bar, 0)) {
-            set_status(g.ctrl, CSPB_DEV_TIMEOUT);
-            return;
-        }
-    } else {
-        for (int i = t; i < TILE; i += kBulkThreads) tbuf[i] = i < cnt ? __ldg(in + base + i) : T(0);
-        __syncthreads();
-    }
-    const uint4* buf = reinterpret_cast<const uint4*>(dsm);
-    // pass 1: each warp's sum
+    const uint64_t keep = evict_last_l2_policy(), drop = evict_first_policy();
+    // pass 1: the warp's sum, its rows kept in L2
     T s = 0;
 #pragma unroll
-    for (int j = 0; j < kBulkRows; ++j) {
-        T x[E];
-        Vec16<T>::unpack(buf[(warp * kBulkRows + j) * 32 + lane], x);
+    for (int j0 = 0; j0 < kL2Rows; j0 += B) {
+        uint4 v[B];
 #pragma unroll
-        for (int k = 0; k < E; ++k) s += x[k];
+        for (int k = 0; k < B; ++k)
+            v[k] = l2_row<T>(in, base + int64_t(warp * kL2Rows + j0 + k) * 32 * E + lane * E, g.n, full, keep);
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            T x[E];
+            Vec16<T>::unpack(v[k], x);
+#pragma unroll
+            for (int q = 0; q < E; ++q) s += x[q];
+        }
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
@@ -437,38 +482,44 @@ __global__ void __launch_bounds__(kBulkThreads, 9) k_scan_bulk(ScanK<T> g) {
     const T agg = (s_wsum[0] + s_wsum[1]) + (s_wsum[2] + s_wsum[3]);
     if (warp == 0) tile_lookback<T>(g, tile, agg, &s_prefix);
     __syncthreads();
-    // pass 2: the warp's rows from the tile's prefix plus the sums of the warps before it
+    // pass 2: the rows again (from L2), scanned from the tile's prefix plus the sums of the warps before
     T carry = s_prefix;
 #pragma unroll
     for (int w = 0; w < 3; ++w)
         if (w < warp) carry += s_wsum[w];
     T* out = g.out;
 #pragma unroll
-    for (int j = 0; j < kBulkRows; ++j) {
-        const int row = warp * kBulkRows + j;
-        T x[E];
-        Vec16<T>::unpack(buf[row * 32 + lane], x);
-        T c[E];
-        c[0] = x[0];
+    for (int j0 = 0; j0 < kL2Rows; j0 += B) {
+        uint4 v[B];
 #pragma unroll
-        for (int k = 1; k < E; ++k) c[k] = c[k - 1] + x[k];
-        const T inc = warp_incl_scan(c[E - 1]);
-        const T e = carry + inc - c[E - 1];
-        carry += __shfl_sync(0xffffffffu, inc, 31);
-        T o[E];
-        o[0] = e;
+        for (int k = 0; k < B; ++k)
+            v[k] = l2_row<T>(in, base + int64_t(warp * kL2Rows + j0 + k) * 32 * E + lane * E, g.n, full, drop);
 #pragma unroll
-        for (int k = 1; k < E; ++k) o[k] = e + c[k - 1];
-        const int64_t i0 = base + int64_t(row) * 32 * E + lane * E;
-        if (cnt == TILE) {
-            Vec16<T>::store(out + i0, o);
-        } else {
+        for (int k = 0; k < B; ++k) {
+            T x[E];
+            Vec16<T>::unpack(v[k], x);
+            T c[E];
+            c[0] = x[0];
 #pragma unroll
-            for (int k = 0; k < E; ++k)
-                if (i0 + k < g.n) __stcg(out + i0 + k, o[k]);
+            for (int q = 1; q < E; ++q) c[q] = c[q - 1] + x[q];
+            const T inc = warp_incl_scan(c[E - 1]);
+            const T e = carry + inc - c[E - 1];
+            carry += __shfl_sync(0xffffffffu, inc, 31);
+            T o[E];
+            o[0] = e;
+#pragma unroll
+            for (int q = 1; q < E; ++q) o[q] = e + c[q - 1];
+            const int64_t i0 = base + int64_t(warp * kL2Rows + j0 + k) * 32 * E + lane * E;
+            if (full) {
+                VecCs<T>::store(out + i0, o);
+            } else {
+#pragma unroll
+                for (int q = 0; q < E; ++q)
+                    if (i0 + q < g.n) __stcg(out + i0 + q, o[q]);
+            }
         }
     }
-    if (tile == g.tiles - 1 && t == kBulkThreads - 1) out[g.n] = carry;  // the total
+    if (tile == g.tiles - 1 && t == kL2Threads - 1) out[g.n] = carry;  // the total
 }
 
 // Counts mode of build_column on bulk tiles: a 32-bit count source with stride 1. Pass 1 narrows the counts (a
@@ -731,9 +782,9 @@ int run_scan(const ScanSrc& src, T* out, uint32_t* out32, int64_t n, void* ws, s
     g.total_flag = total_flag;
     g.total64 = total64;
     if (!src.column && aligned(src.in, 16) && aligned(out, 16)) {
-        // bulk tiles (fewer, larger tiles than the layout's: the layout's status words cover them)
-        g.tiles = (n + BulkTile<T>::kItems - 1) / BulkTile<T>::kItems;
-        k_scan_bulk<T><<<unsigned(g.tiles), kBulkThreads, BulkTile<T>::kBytes, st>>>(g);
+        // L2 re-read tiles (fewer, larger tiles than the layout's: the layout's status words cover them)
+        g.tiles = (n + L2Tile<T>::kItems - 1) / L2Tile<T>::kItems;
+        k_scan_l2<T><<<unsigned(g.tiles), kL2Threads, 0, st>>>(g);
     } else if (!src.column) k_scan<T, kPlain><<<unsigned(L.tiles), kScanThreads, 0, st>>>(g);
     else if constexpr (std::is_same_v<T, uint64_t>) {
         if ((src.dtype == CSPB_I32 || src.dtype == CSPB_U32) && src.k == 1 && aligned(src.in, 16) &&

@@ -44,12 +44,13 @@ def test_scan_u64(cuda, n):
     assert np.array_equal(out.cpu().numpy().view(np.uint64), oracle.exclusive_scan(v))
 
 
-@pytest.mark.parametrize("misaligned", [False, True], ids=["bulk-tiles", "register-tiles"])
+@pytest.mark.parametrize("misaligned", [False, True], ids=["l2-tiles", "register-tiles"])
 @pytest.mark.parametrize("wide", [False, True], ids=["u32", "u64"])
-@pytest.mark.parametrize("n", [1, 5, 3071, 3072, 3073, 6143, 6144, 6145, 12289, (1 << 22) + 3])
-def test_scan_bulk_and_register_tiles(cuda, n, wide, misaligned):
-    """16-byte aligned input and output take the bulk-copy tiles (6144 u32 / 3072 u64 items); an array that starts one
-    element off a 16-byte boundary takes the register-loaded tiles. Both are bit-exact, at and around the tile sizes."""
+@pytest.mark.parametrize("n", [1, 5, 2047, 2048, 2049, 4095, 4096, 4097, 8191, 8192, 8193, 16385, (1 << 22) + 3])
+def test_scan_l2_and_register_tiles(cuda, n, wide, misaligned):
+    """16-byte aligned input and output take the L2 re-read tiles (8192 u32 / 4096 u64 items); an array that starts
+    one element off a 16-byte boundary takes the register-loaded tiles (4096 u32 / 2048 u64). Both are bit-exact, at
+    and around the tile sizes."""
     import torch
     import cospanmdao_b200 as cb
     rng = np.random.default_rng(n * 2 + wide)
