@@ -326,19 +326,17 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
     const int tx0 = (tile % g.tiles_x) * TX, ty0 = (tile / g.tiles_x) * TY;
     const int64_t plane = int64_t(g.nx) * g.ny;
 
-    // 1. the tile and its halo, boundary rule on the fly, as primitives (tile_load + tile_boundary + to_prim). A thread
-    // takes up to NL cells; the fast form issues all their loads before it converts any of them (one DRAM latency per
-    // tile, not NL: 0.505 -> 0.493 ms at 4096²), the reference-rounding form one cell at a time (its IEEE divisions
-    // need the registers: 0.717 ms the other way against 0.694).
-    constexpr int NL = (LC + kThreads - 1) / kThreads;
-    constexpr int NB = X ? 1 : NL;  // cells whose loads are in flight together
-#pragma unroll
-    for (int q0 = 0; q0 < NL; q0 += NB) {
-        float ld_r[NB], ld_mu[NB], ld_mv[NB], ld_E[NB];
+    // 1. the tile and its halo, boundary rule on the fly, as primitives (tile_load + tile_boundary + to_prim). The fast
+    // form has a thread issue the loads of all its cells (up to NL) before it converts any of them: one DRAM latency
+    // per tile, not NL (0.505 -> 0.493 ms at 4096²). The reference-rounding form converts one cell at a time: its IEEE
+    // divisions need the registers (0.72 ms the other way, against 0.69).
+    if constexpr (!X) {
+        constexpr int NL = (LC + kThreads - 1) / kThreads;
+        float ld_r[NL], ld_mu[NL], ld_mv[NL], ld_E[NL];
         uint32_t flip = 0;  // bit q: cell q's momenta change sign (a wall's mirror image)
 #pragma unroll
-        for (int q = 0; q < NB; ++q) {
-            const int idx = tid + (q0 + q) * kThreads;
+        for (int q = 0; q < NL; ++q) {
+            const int idx = tid + q * kThreads;
             ld_r[q] = ld_mu[q] = ld_mv[q] = ld_E[q] = 0.0f;
             if (idx < LC) {
                 const int lb = idx / LX, la = idx - lb * LX;
@@ -368,33 +366,58 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
             }
         }
 #pragma unroll
-        for (int q = 0; q < NB; ++q) {
-            const int idx = tid + (q0 + q) * kThreads;
+        for (int q = 0; q < NL; ++q) {
+            const int idx = tid + q * kThreads;
             if (idx >= LC) continue;
             const float r = ld_r[q];
             const bool neg = (flip >> q) & 1u;  // a sign flip: exact
             const float mu = neg ? -ld_mu[q] : ld_mu[q];
             const float mv = neg ? -ld_mv[q] : ld_mv[q];
             const float E = ld_E[q];
-            float u, v, p, T;
-            if constexpr (X) {
-                u = __fdiv_rn(mu, r);
-                v = __fdiv_rn(mv, r);
-                p = __fmul_rn(kGm1,
-                              __fsub_rn(E, __fmul_rn(__fmul_rn(0.5f, r), __fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)))));
-                T = __fdiv_rn(p, r);
-            } else {
-                const float ir = __frcp_rn(r);
-                u = mu * ir;
-                v = mv * ir;
-                p = kGm1 * (E - 0.5f * r * (u * u + v * v));
-                T = p * ir;
-            }
+            const float ir = __frcp_rn(r);
+            const float u = mu * ir, v = mv * ir;
+            const float p = kGm1 * (E - 0.5f * r * (u * u + v * v));
             s.W[0][idx] = r;
             s.W[1][idx] = u;
             s.W[2][idx] = v;
             s.W[3][idx] = p;
-            s.T[idx] = T;
+            s.T[idx] = p * ir;
+        }
+    } else {
+        for (int idx = tid; idx < LC; idx += kThreads) {
+            const int lb = idx / LX, la = idx - lb * LX;
+            const int j = ty0 - 2 + lb, i = tx0 - 2 + la;
+            const int is = unsigned(i) < unsigned(g.nx) ? i : wrapi(i, g.nx);  // only halo columns wrap
+            int js = j;
+            float sg = 1.0f;
+            const float* src = g.U;
+            int64_t fs = plane;  // between the fields of src
+            if (j < 0 || j >= g.ny) {
+                const bool lo = j < 0;
+                if (g.edges & (lo ? 1 : 2)) {  // a slab's interior edge: the neighbour's rows
+                    src = lo ? g.halo_lo : g.halo_hi;
+                    fs = 2 * int64_t(g.nx);
+                    js = lo ? j + 2 : j - g.ny;
+                } else if (g.walls) {
+                    js = lo ? -1 - j : 2 * g.ny - 1 - j;
+                    sg = -1.0f;
+                } else {
+                    js = wrapi(j, g.ny);
+                }
+            }
+            const int64_t c = int64_t(js) * g.nx + is;
+            const float r = __ldg(src + c);
+            const float mu = __ldg(src + fs + c) * sg;  // a sign flip: exact
+            const float mv = __ldg(src + 2 * fs + c) * sg;
+            const float E = __ldg(src + 3 * fs + c);
+            const float u = __fdiv_rn(mu, r), v = __fdiv_rn(mv, r);
+            const float p =
+                __fmul_rn(kGm1, __fsub_rn(E, __fmul_rn(__fmul_rn(0.5f, r), __fadd_rn(__fmul_rn(u, u), __fmul_rn(v, v)))));
+            s.W[0][idx] = r;
+            s.W[1][idx] = u;
+            s.W[2][idx] = v;
+            s.W[3][idx] = p;
+            s.T[idx] = __fdiv_rn(p, r);
         }
     }
     __syncthreads();
