@@ -138,6 +138,186 @@ __global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_
     rowsum_finish_lr(g.p2, g.u1, g.u2, __ldcg(dots + 2), __ldcg(dots + 3));
 }
 
+// ---- the bf16 low-rank passes with the unit's cross-warp sums deferred ------------------------------------------------
+// pass_unit ends each unit with two block barriers: the warps of a unit store their column sums (pass 1) or row dots
+// (pass 2) to shared memory, wait for one another, and sum across warps. Here each warp stores its share into one of
+// two buffers and goes on; the next unit's threads form those sums right after issuing their first loads (the
+// barrier of the work hand-off between the units orders the stores before them), so the sums overlap the loads in
+// flight and the unit has no barrier of its own. The arithmetic and its order are pass_unit's
+// (<bf16, kWX, NC, !RANK2, !CSA, CSB | RDOT, RB, DEFER>), so the results are the same bits, as the task runner's.
+namespace lrd {
+
+using Bf = __nv_bfloat16;
+using G = PassGeo<Bf, kWX>;
+constexpr int VEC = G::VEC, WY = G::WY, S = G::S, CW = G::CW;
+
+// The two passes run apart (grid barriers between them), so their buffers share the block's shared memory.
+union Bufs {
+    double cs[2][WY * CW];  // pass 1: each warp's column sums, two units' worth
+    struct {
+        float rd[2][kWX * S];                    // each warp's row dots, two units' worth
+        float rdot[kPassThreads / 32][32 * 32];  // a warp's dots of its 32 rows, [row][lane]
+    } p2;
+};
+
+// pass 1's sums of unit `unit` from buffer `slot`: P[strip][col] = ((w0 + w1) + w2) + w3 over the row warps
+__device__ __forceinline__ void cs_sum(const PassArgs& a, int64_t unit, const double* red) {
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    for (int t = threadIdx.x; t < CW; t += kPassThreads) {
+        const int64_t col = chunk * CW + t;
+        if (col < a.n) {
+            double s = red[t];
+#pragma unroll
+            for (int y = 1; y < WY; ++y) s += red[y * CW + t];
+            a.PB[strip * a.n + col] = s;
+        }
+    }
+}
+// pass 2's row dots of unit `unit`: Wp[chunk][row] = w0 + w1 over the column warps
+__device__ __forceinline__ void rd_sum(const PassArgs& a, int64_t unit, const float* red2) {
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    for (int t = threadIdx.x; t < S; t += kPassThreads) {
+        const int64_t row = strip * S + t;
+        if (row < a.rows) {
+            float s = red2[t];
+#pragma unroll
+            for (int x = 1; x < kWX; ++x) s += red2[x * S + t];
+            a.Wp[chunk * a.n + row] = s;
+        }
+    }
+}
+
+// One unit; `pending` runs once, after the first batch's loads are issued (the previous unit's sums).
+template <bool CS, int RB, class Pending>
+__device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_ok, Bufs& B, int slot,
+                                     Pending&& pending) {
+    static_assert(32 % RB == 0, "batches of rows that divide the warp's 32");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wx = warp % kWX, wy = warp / kWX;
+    const int64_t n = a.n;
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    const int64_t r0 = strip * S + wy * 32;
+    const int64_t c0 = chunk * CW + int64_t(wx * 32 + lane) * VEC;
+    const int64_t rem_r = a.rows - r0, rem_c = n - c0;
+    const int nrows = rem_r <= 0 ? 0 : (rem_r >= 32 ? 32 : int(rem_r));
+    const int ncols = rem_c <= 0 ? 0 : (rem_c >= VEC ? VEC : int(rem_c));
+    float cybr = 0.f;
+    if (CS && lane < nrows) cybr = __ldcg(a.cyB + r0 + lane);
+    float xc[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) xc[e] = (!CS && e < ncols) ? __ldcg(a.xv + c0 + e) : 0.f;
+    double accB[VEC];
+    float pB[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) { accB[e] = 0.0; pB[e] = 0.f; }
+    const Bf* src = static_cast<const Bf*>(a.src);
+    const int64_t lds = a.lds;
+    float* rdot = B.p2.rdot[warp];
+#pragma unroll 1
+    for (int kb = 0; kb < 32; kb += RB) {
+        uint4 raw[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k)
+            raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<Bf, true>(src + (r0 + kb + k) * lds, c0, ncols, vec_ok)
+                                                   : make_uint4(0u, 0u, 0u, 0u);
+        if (kb == 0) pending();
+        if (kb < nrows) {
+#pragma unroll
+            for (int k = 0; k < RB; ++k) {
+                const int kk = kb + k;
+                const float cybk = __shfl_sync(kFull, cybr, kk);
+                if (kk < nrows) {
+                    float b[VEC];
+                    unpack<Bf>(raw[k], b);
+                    if constexpr (CS) {
+                        const bool flush = (kk & 7) == 7 || kk == nrows - 1;
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) pB[e] = fmaf(b[e], cybk, pB[e]);
+                        if (flush) {
+#pragma unroll
+                            for (int e = 0; e < VEC; ++e) { accB[e] += double(pB[e]); pB[e] = 0.f; }
+                        }
+                    } else {
+                        float d = 0.f;
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) d = fmaf(b[e], xc[e], d);
+                        rdot[kk * 32 + lane] = d;
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (CS) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) B.cs[slot][wy * CW + (wx * 32 + lane) * VEC + e] = accB[e];
+    } else {
+        float racc[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) racc[k] = k < nrows ? rdot[k * 32 + lane] : 0.f;  // this lane's own values
+        B.p2.rd[slot][wx * S + wy * 32 + lane] = transpose_reduce32(racc);
+    }
+}
+
+}  // namespace lrd
+
+
+// k_gemver_lr<bf16, false> with the deferred cross-warp sums (lrd::unit): the same bits, no barrier inside a unit.
+__global__ void __launch_bounds__(kPassThreads, (kLrBlocks<__nv_bfloat16, false>)) k_gemver_lr_bf16(LowRankK g,
+                                                                                                    int vec_ok) {
+    constexpr int RB = kLrRB<__nv_bfloat16, false>;
+    __shared__ lrd::Bufs B;
+    double* dots = reinterpret_cast<double*>(g.ctrl + kDots0);
+    if (blockIdx.x == 0) {  // u1·y, u2·y: inputs only
+        double s1, s2;
+        block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
+        if (threadIdx.x == 0) {
+            dots[0] = s1;
+            dots[1] = s2;
+        }
+    }
+    {
+        int64_t pend = -1;
+        int slot = 0;
+        for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0);
+            lrd::unit<true, RB>(g.p1, u, vec_ok != 0, B, slot, [&] {
+                if (pend >= 0) lrd::cs_sum(g.p1, pend, B.cs[slot ^ 1]);
+            });
+            pend = u;
+            slot ^= 1;
+            u = share_work(next);  // its barrier orders this unit's buffer stores before their sums
+        }
+        if (pend >= 0) lrd::cs_sum(g.p1, pend, B.cs[slot ^ 1]);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, __ldcg(dots), __ldcg(dots + 1), g.x);
+    if (!grid_barrier(g.ctrl)) return;
+    if (blockIdx.x == 0) {  // v1·x, v2·x: x is complete after the barrier
+        double t1, t2;
+        block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
+        if (threadIdx.x == 0) {
+            dots[2] = t1;
+            dots[3] = t2;
+        }
+    }
+    {
+        int64_t pend = -1;
+        int slot = 0;
+        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+            lrd::unit<false, RB>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, B, slot, [&] {
+                if (pend >= 0) lrd::rd_sum(g.p2, pend, B.p2.rd[slot ^ 1]);
+            });
+            pend = g.units - 1 - int64_t(u);
+            slot ^= 1;
+            u = share_work(next);
+        }
+        if (pend >= 0) lrd::rd_sum(g.p2, pend, B.p2.rd[slot ^ 1]);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish_lr(g.p2, g.u1, g.u2, __ldcg(dots + 2), __ldcg(dots + 3));
+}
+
 // The same three passes with the matrix streamed through a shared-memory ring by bulk copies (bulkpass.cuh): one
 // CTA per SM, 8 consumer warps and a producer warp; the results are bit-identical to k_gemver's.
 template <typename T, bool P2_FROM_B, int NST>
@@ -571,7 +751,7 @@ int cspb_gemver_fused(const cspb_gemver_desc* d, void* stream) {
         g.x = d->x;
         void* args[] = {&g, const_cast<int*>(&vec_ok)};
         if (bf16 && store) return launch_coop(k_gemver_lr<__nv_bfloat16, true>, args, L.units, zero, ws, st);
-        if (bf16) return launch_coop(k_gemver_lr<__nv_bfloat16, false>, args, L.units, zero, ws, st);
+        if (bf16) return launch_coop(k_gemver_lr_bf16, args, L.units, zero, ws, st);
         return launch_coop(k_gemver_lr<float, false>, args, L.units, zero, ws, st);
     }
     // the bulk-copy ring: every row segment and vector piece must start on 16 bytes and be a multiple of 16 bytes long
