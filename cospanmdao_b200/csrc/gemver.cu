@@ -44,6 +44,72 @@ struct GemverK {
     float* x;
 };
 
+// The f32 headline's pass 2 (row dots of the stored Â, read back coherently) with the unit's cross-warp sums deferred
+// as in lrd: each warp's 32 row dots go to one of two buffers, and the next unit forms Wp after its first loads. The
+// arithmetic and its order are pass_unit<float, kWX, false, false, false, false, true, 16, true>'s.
+namespace p2f {
+
+using G = PassGeo<float, kWX>;
+constexpr int VEC = G::VEC, S = G::S, CW = G::CW, RB = 16;
+
+__device__ __forceinline__ void rd_sum(const PassArgs& a, int64_t unit, const float* red2) {
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    for (int t = threadIdx.x; t < S; t += kPassThreads) {
+        const int64_t row = strip * S + t;
+        if (row < a.rows) {
+            float s = red2[t];
+#pragma unroll
+            for (int x = 1; x < kWX; ++x) s += red2[x * S + t];
+            a.Wp[chunk * a.n + row] = s;
+        }
+    }
+}
+
+template <class Pending>
+__device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_ok, float* red_out, Pending&& pending) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wx = warp % kWX, wy = warp / kWX;
+    const int64_t n = a.n;
+    const int64_t strip = unit / a.chunks, chunk = unit % a.chunks;
+    const int64_t r0 = strip * S + wy * 32;
+    const int64_t c0 = chunk * CW + int64_t(wx * 32 + lane) * VEC;
+    const int64_t rem_r = a.rows - r0, rem_c = n - c0;
+    const int nrows = rem_r <= 0 ? 0 : (rem_r >= 32 ? 32 : int(rem_r));
+    const int ncols = rem_c <= 0 ? 0 : (rem_c >= VEC ? VEC : int(rem_c));
+    float xc[VEC];
+#pragma unroll
+    for (int e = 0; e < VEC; ++e) xc[e] = e < ncols ? __ldcg(a.xv + c0 + e) : 0.f;
+    float racc[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) racc[k] = 0.f;
+    const float* src = static_cast<const float*>(a.src);
+    const int64_t lds = a.lds;
+#pragma unroll
+    for (int kb = 0; kb < 32; kb += RB) {
+        uint4 raw[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k)
+            raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<float, false>(src + (r0 + kb + k) * lds, c0, ncols, vec_ok)
+                                                   : make_uint4(0u, 0u, 0u, 0u);
+        if (kb == 0) pending();
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int kk = kb + k;
+            if (kk < nrows) {
+                float b[VEC];
+                unpack<float>(raw[k], b);
+                float d = 0.f;
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) d = fmaf(b[e], xc[e], d);
+                racc[kk] = d;
+            }
+        }
+    }
+    red_out[wx * S + wy * 32 + lane] = transpose_reduce32(racc);
+}
+
+}  // namespace p2f
+
 template <typename T, bool P2_FROM_B>
 __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_ok) {
     __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
@@ -55,14 +121,28 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
     if (!grid_barrier(g.ctrl)) return;
-    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-        const int64_t unit = g.units - 1 - int64_t(u);
-        if constexpr (P2_FROM_B)
-            pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, unit, vec_ok != 0, smem);
-        else
-            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p2, unit, vec_ok != 0, smem);
-        u = share_work(next);
+    if constexpr (P2_FROM_B) {
+        __shared__ float rd[2][kWX * p2f::S];
+        int64_t pend = -1;
+        int slot = 0;
+        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+            const int64_t unit = g.units - 1 - int64_t(u);
+            p2f::unit(g.p2, unit, vec_ok != 0, rd[slot], [&] {
+                if (pend >= 0) p2f::rd_sum(g.p2, pend, rd[slot ^ 1]);
+            });
+            pend = unit;
+            slot ^= 1;
+            u = share_work(next);  // its barrier orders this unit's buffer stores before their sums
+        }
+        if (pend >= 0) p2f::rd_sum(g.p2, pend, rd[slot ^ 1]);
+    } else {
+        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0,
+                                                                       smem);
+            u = share_work(next);
+        }
     }
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p2);
