@@ -44,9 +44,9 @@ struct GemverK {
     float* x;
 };
 
-// The f32 headline's pass 2 (row dots of the stored Â, read back coherently) with the unit's cross-warp sums deferred
-// as in lrd: each warp's 32 row dots go to one of two buffers, and the next unit forms Wp after its first loads. The
-// arithmetic and its order are pass_unit<float, kWX, false, false, false, false, true, 16, true>'s.
+// The f32 row-dot passes over a stored Â (GEMVER's pass 2, the chain's passes 2 and 4, a row shard's finish) with the
+// unit's cross-warp sums deferred as in lrd: each warp's 32 row dots go to one of two buffers, and the next unit forms Wp after its first loads. The
+// arithmetic and its order are pass_unit<float, kWX, NC, false, false, false, true, 16, true>'s.
 namespace p2f {
 
 using G = PassGeo<float, kWX>;
@@ -65,7 +65,7 @@ __device__ __forceinline__ void rd_sum(const PassArgs& a, int64_t unit, const fl
     }
 }
 
-template <class Pending>
+template <bool NC, class Pending>
 __device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_ok, float* red_out, Pending&& pending) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wx = warp % kWX, wy = warp / kWX;
@@ -89,7 +89,7 @@ __device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_o
         uint4 raw[RB];
 #pragma unroll
         for (int k = 0; k < RB; ++k)
-            raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<float, false>(src + (r0 + kb + k) * lds, c0, ncols, vec_ok)
+            raw[k] = (kb + k < nrows && ncols > 0) ? load_raw<float, NC>(src + (r0 + kb + k) * lds, c0, ncols, vec_ok)
                                                    : make_uint4(0u, 0u, 0u, 0u);
         if (kb == 0) pending();
 #pragma unroll
@@ -108,6 +108,25 @@ __device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_o
     red_out[wx * S + wy * 32 + lane] = transpose_reduce32(racc);
 }
 
+// The pass over the units of counter `word`, from the last unit back (the rows written last are still in L2).
+template <bool NC>
+__device__ __forceinline__ void pass(const PassArgs& a, uint32_t* ctrl, int word, int64_t units, bool vec_ok) {
+    __shared__ float rd[2][kWX * S];
+    int64_t pend = -1;
+    int slot = 0;
+    for (uint32_t u = grab_work(ctrl, word); int64_t(u) < units;) {
+        const uint32_t next = prefetch_work(ctrl, word);
+        const int64_t cur = units - 1 - int64_t(u);
+        unit<NC>(a, cur, vec_ok, rd[slot], [&] {
+            if (pend >= 0) rd_sum(a, pend, rd[slot ^ 1]);
+        });
+        pend = cur;
+        slot ^= 1;
+        u = share_work(next);  // its barrier orders this unit's buffer stores before their sums
+    }
+    if (pend >= 0) rd_sum(a, pend, rd[slot ^ 1]);
+}
+
 }  // namespace p2f
 
 template <typename T, bool P2_FROM_B>
@@ -122,20 +141,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_gemver(GemverK g, int vec_o
     colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
     if (!grid_barrier(g.ctrl)) return;
     if constexpr (P2_FROM_B) {
-        __shared__ float rd[2][kWX * p2f::S];
-        int64_t pend = -1;
-        int slot = 0;
-        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
-            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-            const int64_t unit = g.units - 1 - int64_t(u);
-            p2f::unit(g.p2, unit, vec_ok != 0, rd[slot], [&] {
-                if (pend >= 0) p2f::rd_sum(g.p2, pend, rd[slot ^ 1]);
-            });
-            pend = unit;
-            slot ^= 1;
-            u = share_work(next);  // its barrier orders this unit's buffer stores before their sums
-        }
-        if (pend >= 0) p2f::rd_sum(g.p2, pend, rd[slot ^ 1]);
+        p2f::pass<false>(g.p2, g.ctrl, kWork0 + 1, g.units, vec_ok != 0);
     } else {
         for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
             const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
@@ -555,11 +561,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain_g1(ChainK g, int vec_
     if (!grid_barrier(g.ctrl)) return;
     colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.za, g.beta, g.x1);
     if (!grid_barrier(g.ctrl)) return;
-    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-        pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p2, g.units - 1 - int64_t(u), vo, smem);
-        u = share_work(next);
-    }
+    p2f::pass<false>(g.p2, g.ctrl, kWork0 + 1, g.units, vo);
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p2);
 }
@@ -581,11 +583,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_chain_g2(ChainK g, int vec_
     colsum_finish(g.p3.PA, g.p3.strips, g.p3.n, nullptr, 1.0f, g.s);    // s = B1ᵀ·w1
     colsum_finish(g.p3.PB, g.p3.strips, g.p3.n, g.s, g.beta, g.x2);     // x2 = s + β·B2ᵀ·q (same thread owns s[j])
     if (!grid_barrier(g.ctrl)) return;
-    for (uint32_t u = grab_work(g.ctrl, kWork0 + 3); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 3);
-        pass_unit<float, kWX, false, false, false, false, true, 16, true>(g.p4, g.units - 1 - int64_t(u), vo, smem);
-        u = share_work(next);
-    }
+    p2f::pass<false>(g.p4, g.ctrl, kWork0 + 3, g.units, vo);
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p4);
 }
@@ -630,14 +628,15 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_rows_finish(RowsK g, int ve
         g.x[j] = float(zz + double(g.beta) * __ldcg(g.total + j));
     }
     if (!grid_barrier(g.ctrl)) return;
-    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-        const int64_t unit = g.units - 1 - int64_t(u);
-        if constexpr (FROM_B)
-            pass_unit<float, kWX, true, false, false, false, true, 16, true>(g.p, unit, vec_ok != 0, smem);
-        else
-            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p, unit, vec_ok != 0, smem);
-        u = share_work(next);
+    if constexpr (FROM_B) {
+        p2f::pass<true>(g.p, g.ctrl, kWork0 + 1, g.units, vec_ok != 0);
+    } else {
+        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+            pass_unit<T, kWX, true, true, false, false, true, 0, true>(g.p, g.units - 1 - int64_t(u), vec_ok != 0,
+                                                                       smem);
+            u = share_work(next);
+        }
     }
     if (!grid_barrier(g.ctrl)) return;
     rowsum_finish(g.p);
