@@ -176,54 +176,6 @@ struct LowRankK {
 template <typename T, bool STORE> inline constexpr int kLrRB = (sizeof(T) == 2 && !STORE) ? 8 : 16;
 template <typename T, bool STORE> inline constexpr int kLrBlocks = (sizeof(T) == 2 && !STORE) ? 3 : 2;
 
-template <typename T, bool STORE>
-__global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_lr(LowRankK g, int vec_ok) {
-    constexpr int RB = kLrRB<T, STORE>;
-    __shared__ __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
-    // The dot products of the finishes are formed by block 0 alone (block_dot2: one order, whatever the grid) and read
-    // by every block after the next grid barrier; every block forming them read 3 vectors each time (85 MB of L2 reads
-    // per finish at n = 16384 and 444 blocks).
-    double* dots = reinterpret_cast<double*>(g.ctrl + kDots0);
-    if constexpr (!STORE) {
-        if (blockIdx.x == 0) {  // u1·y, u2·y: inputs only
-            double s1, s2;
-            block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
-            if (threadIdx.x == 0) {
-                dots[0] = s1;
-                dots[1] = s2;
-            }
-        }
-    }
-    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0);
-        if constexpr (STORE) pass_unit<T, kWX, true, true, false, true, false, 0>(g.p1, u, vec_ok != 0, smem);
-        else pass_unit<T, kWX, true, false, false, true, false, RB>(g.p1, u, vec_ok != 0, smem);
-        u = share_work(next);
-    }
-    if (!grid_barrier(g.ctrl)) return;
-    if constexpr (STORE) {
-        colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
-    } else {
-        colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, __ldcg(dots), __ldcg(dots + 1), g.x);
-    }
-    if (!grid_barrier(g.ctrl)) return;
-    if (blockIdx.x == 0) {  // v1·x, v2·x: x is complete after the barrier
-        double t1, t2;
-        block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
-        if (threadIdx.x == 0) {
-            dots[2] = t1;
-            dots[3] = t2;
-        }
-    }
-    for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
-        const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
-        pass_unit<T, kWX, true, false, false, false, true, RB, true>(g.p2, g.units - 1 - int64_t(u), vec_ok != 0, smem);
-        u = share_work(next);
-    }
-    if (!grid_barrier(g.ctrl)) return;
-    rowsum_finish_lr(g.p2, g.u1, g.u2, __ldcg(dots + 2), __ldcg(dots + 3));
-}
-
 // ---- the bf16 low-rank passes with the unit's cross-warp sums deferred ------------------------------------------------
 // pass_unit ends each unit with two block barriers: the warps of a unit store their column sums (pass 1) or row dots
 // (pass 2) to shared memory, wait for one another, and sum across warps. Here each warp stores its share into one of
@@ -345,6 +297,73 @@ __device__ __forceinline__ void unit(const PassArgs& a, int64_t unit, bool vec_o
 }
 
 }  // namespace lrd
+
+template <typename T, bool STORE>
+__global__ void __launch_bounds__(kPassThreads, (kLrBlocks<T, STORE>)) k_gemver_lr(LowRankK g, int vec_ok) {
+    constexpr int RB = kLrRB<T, STORE>;
+    // pass 1's pass_unit and pass 2's deferred sums run apart (grid barriers between them): one block of shared memory
+    __shared__ union {
+        __align__(16) unsigned char smem[pass_smem_bytes<T, kWX>()];
+        lrd::Bufs B;
+    } sh;
+    unsigned char* smem = sh.smem;
+    // The dot products of the finishes are formed by block 0 alone (block_dot2: one order, whatever the grid) and read
+    // by every block after the next grid barrier; every block forming them read 3 vectors each time (85 MB of L2 reads
+    // per finish at n = 16384 and 444 blocks).
+    double* dots = reinterpret_cast<double*>(g.ctrl + kDots0);
+    if constexpr (!STORE) {
+        if (blockIdx.x == 0) {  // u1·y, u2·y: inputs only
+            double s1, s2;
+            block_dot2(g.u1, g.u2, g.y, g.p1.n, s1, s2);
+            if (threadIdx.x == 0) {
+                dots[0] = s1;
+                dots[1] = s2;
+            }
+        }
+    }
+    for (uint32_t u = grab_work(g.ctrl, kWork0); u < g.units;) {
+        const uint32_t next = prefetch_work(g.ctrl, kWork0);
+        if constexpr (STORE) pass_unit<T, kWX, true, true, false, true, false, 0>(g.p1, u, vec_ok != 0, smem);
+        else pass_unit<T, kWX, true, false, false, true, false, RB>(g.p1, u, vec_ok != 0, smem);
+        u = share_work(next);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    if constexpr (STORE) {
+        colsum_finish(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.x);
+    } else {
+        colsum_finish_lr(g.p1.PB, g.p1.strips, g.p1.n, g.z, g.beta, g.v1, g.v2, __ldcg(dots), __ldcg(dots + 1), g.x);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    if (blockIdx.x == 0) {  // v1·x, v2·x: x is complete after the barrier
+        double t1, t2;
+        block_dot2(g.v1, g.v2, g.x, g.p2.n, t1, t2);
+        if (threadIdx.x == 0) {
+            dots[2] = t1;
+            dots[3] = t2;
+        }
+    }
+    // pass 2 with the cross-warp sums of each unit deferred to the next unit (the same bits as pass_unit's)
+    if constexpr (sizeof(T) == 4) {
+        p2f::pass<true>(g.p2, g.ctrl, kWork0 + 1, g.units, vec_ok != 0);
+    } else {
+        int64_t pend = -1;
+        int slot = 0;
+        for (uint32_t u = grab_work(g.ctrl, kWork0 + 1); u < g.units;) {
+            const uint32_t next = prefetch_work(g.ctrl, kWork0 + 1);
+            const int64_t cur = g.units - 1 - int64_t(u);
+            lrd::unit<false, RB>(g.p2, cur, vec_ok != 0, sh.B, slot, [&] {
+                if (pend >= 0) lrd::rd_sum(g.p2, pend, sh.B.p2.rd[slot ^ 1]);
+            });
+            pend = cur;
+            slot ^= 1;
+            u = share_work(next);
+        }
+        if (pend >= 0) lrd::rd_sum(g.p2, pend, sh.B.p2.rd[slot ^ 1]);
+    }
+    if (!grid_barrier(g.ctrl)) return;
+    rowsum_finish_lr(g.p2, g.u1, g.u2, __ldcg(dots + 2), __ldcg(dots + 3));
+}
+
 
 
 // k_gemver_lr<bf16, false> with the deferred cross-warp sums (lrd::unit): the same bits, no barrier inside a unit.
