@@ -297,9 +297,6 @@ __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, in
 }
 
 // The norm partial of block (or tile) b: a warp xor tree, the block in warp order, into part[b].
-// FENCE: the partial is made visible to the last block of the same launch (a completion count follows); without it the
-// partials are read by a later launch (k_nsi_final), after the kernel boundary.
-template <bool FENCE = true>
 __device__ __forceinline__ void nsi_partial(const NsiK& g, int64_t b, double su, double sv, double sc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -315,7 +312,7 @@ __device__ __forceinline__ void nsi_partial(const NsiK& g, int64_t b, double su,
         double t = s_part[0][threadIdx.x];
         for (int w = 1; w < kNsiWarps; ++w) t += s_part[w][threadIdx.x];
         g.part[b * 3 + threadIdx.x] = t;
-        if (FENCE) __threadfence();  // visible before any completion count taken after the barrier
+        __threadfence();  // visible before any completion count taken after the barrier
     }
     __syncthreads();
 }
@@ -643,23 +640,12 @@ template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
     nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
 }
-// The tile path: one block per tile, 4 blocks per SM (64 registers a thread at most). SPLIT: a tile writes its norm
-// partial and leaves; k_nsi_final, launched next on the stream, sums the partials in the same order as the last block
-// would. A tile then ends without the fence that made its partial visible within the launch, which held the block until
-// its own residual stores had drained (4096² f32: 0.0824 ms with the fence and count in the tile).
-template <typename T, bool SPLIT = false>
+// The tile path: one block per tile, 4 blocks per SM (64 registers a thread at most).
+template <typename T>
 __global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_tile(NsiK g) {
     extern __shared__ __align__(16) unsigned char nsi_raw[];
-    if constexpr (SPLIT) {
-        double su = 0.0, sv = 0.0, sc = 0.0;
-        nsi_tile<T>(g, blockIdx.x, reinterpret_cast<T*>(nsi_raw), su, sv, sc);
-        nsi_partial<false>(g, blockIdx.x, su, sv, sc);
-    } else {
-        nsi_tile_block<T>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, reinterpret_cast<T*>(nsi_raw));
-    }
+    nsi_tile_block<T>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, reinterpret_cast<T*>(nsi_raw));
 }
-// The norms of a split tile launch: one block, nsi_final's order.
-__global__ void __launch_bounds__(kNsiThreads) k_nsi_final(NsiK g, int64_t nblocks) { nsi_final(g, nblocks); }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
 // The row-strip height H of a grid: the one whose block count best fills whole waves of kNsiWave blocks (4 per SM on
@@ -922,9 +908,8 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
     } else if (tile) {
         const size_t bytes = kNsiTileBytes<float>;
-        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float, true>), bytes)) return CSPB_ERR_LAUNCH;
-        k_ns_incomp_tile<float, true><<<grid, block, bytes, st>>>(g);
-        k_nsi_final<<<1, kNsiThreads, 0, st>>>(g, int64_t(grid.x));
+        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), bytes)) return CSPB_ERR_LAUNCH;
+        k_ns_incomp_tile<float><<<grid, block, bytes, st>>>(g);
     } else {
         k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
@@ -1017,11 +1002,8 @@ int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
         g.dn[f] = d->dn[f];
     }
     g.slab = 1;
-    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float, true>), kNsiTileBytes<float>))
-        return CSPB_ERR_LAUNCH;
-    const int64_t tiles = nsi_tiles(d->nx, d->rows);
-    k_ns_incomp_tile<float, true><<<dim3(unsigned(tiles)), dim3(kNsiThreads), kNsiTileBytes<float>, st>>>(g);
-    k_nsi_final<<<1, kNsiThreads, 0, st>>>(g, tiles);
+    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), kNsiTileBytes<float>)) return CSPB_ERR_LAUNCH;
+    k_ns_incomp_tile<float><<<dim3(unsigned(nsi_tiles(d->nx, d->rows))), dim3(kNsiThreads), kNsiTileBytes<float>, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
