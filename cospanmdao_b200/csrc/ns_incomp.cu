@@ -52,6 +52,78 @@ struct NsiRow {
     float l, r;    // the wrapped neighbours outside the lane's cells when this lane needs them from memory
 };
 
+// ---- the residual of a cell, every rounding written out ------------------------------------------------------------
+//   dfdx = (fE − fW)·inv2h, dfdy = (fN − fS)·inv2h, lap f = (((fE − fc) + (fW − fc)) + ((fN − fc) + (fS − fc)))·invh2
+//   r_u = fma(−ν, lap u, fma(u, dudx, v·dudy) + dpdx), r_v = fma(−ν, lap v, fma(u, dvdx, v·dvdy) + dpdy),
+//   r_c = dudx + dvdy
+// Each operation is rounded to nearest on its own (the fused multiply-adds are the two written), so the compiler has
+// no contraction left to choose. NsiOne evaluates one cell with the scalar instructions; NsiTwo two cells at once with
+// Blackwell's packed f32x2 instructions (.rn, no flush to zero), which round each lane exactly as the scalar
+// instruction would: both give the same bits for a cell, and the tile paths (pairs) and the register path (single
+// cells) agree.
+struct NsiOne {
+    using V = float;
+    static __device__ __forceinline__ V sp(float a) { return a; }
+    static __device__ __forceinline__ V add(V a, V b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ V sub(V a, V b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ V mul(V a, V b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ V fma(V a, V b, V c) { return __fmaf_rn(a, b, c); }
+};
+struct NsiTwo {
+    using V = float2;
+    static __device__ __forceinline__ V sp(float a) { return make_float2(a, a); }
+    static __device__ __forceinline__ V add(V a, V b) {
+        V d;
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+            "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+    }
+    static __device__ __forceinline__ V sub(V a, V b) {
+        V d;
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+            "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+    }
+    static __device__ __forceinline__ V mul(V a, V b) {
+        V d;
+        asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+            "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+        return d;
+    }
+    static __device__ __forceinline__ V fma(V a, V b, V c) {
+        V d;
+        asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+            "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+            : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+        return d;
+    }
+};
+// The 5-point values of one field around a cell (or a pair of cells): centre, west, east, south, north.
+template <class A>
+struct NsiStar {
+    typename A::V c, w, e, s, n;
+};
+template <class A>
+__device__ __forceinline__ void nsi_cell(const NsiStar<A>& u, const NsiStar<A>& v, const NsiStar<A>& p, float inv2h,
+                                         float invh2, float nu, typename A::V& ru, typename A::V& rv,
+                                         typename A::V& rc) {
+    using V = typename A::V;
+    const V i2h = A::sp(inv2h), ih2 = A::sp(invh2), mnu = A::sp(-nu);
+    const V dudx = A::mul(A::sub(u.e, u.w), i2h), dudy = A::mul(A::sub(u.n, u.s), i2h);
+    const V dvdx = A::mul(A::sub(v.e, v.w), i2h), dvdy = A::mul(A::sub(v.n, v.s), i2h);
+    const V dpdx = A::mul(A::sub(p.e, p.w), i2h), dpdy = A::mul(A::sub(p.n, p.s), i2h);
+    const V lapu = A::mul(A::add(A::add(A::sub(u.e, u.c), A::sub(u.w, u.c)), A::add(A::sub(u.n, u.c), A::sub(u.s, u.c))),
+                          ih2);
+    const V lapv = A::mul(A::add(A::add(A::sub(v.e, v.c), A::sub(v.w, v.c)), A::add(A::sub(v.n, v.c), A::sub(v.s, v.c))),
+                          ih2);
+    ru = A::fma(mnu, lapu, A::add(A::fma(u.c, dudx, A::mul(v.c, dudy)), dpdx));
+    rv = A::fma(mnu, lapv, A::add(A::fma(u.c, dvdx, A::mul(v.c, dvdy)), dpdy));
+    rc = A::add(dudx, dvdy);
+}
+
 template <typename T>
 __device__ __forceinline__ float ld1(const T* p, int64_t i) {
     if constexpr (sizeof(T) == 4) return __ldg(reinterpret_cast<const float*>(p) + i);
@@ -146,8 +218,8 @@ template <typename T, int FIELD>
 __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, int x0, int y0, int scols, int th,
                                                  double& su, double& sv, double& sc);
 
-// Tile b of a residual whose rows satisfy nsi_tile_rows. The residuals are the register path's, operation for
-// operation; each lane's 4 squares are summed in f32 before one f64 addition per norm.
+// Tile b of a residual whose rows satisfy nsi_tile_rows. The residuals are the register path's (nsi_cell); each lane's
+// 4 squares are summed in f32 (cells 0 and 2, cells 1 and 3, then the two sums) before one f64 addition per norm.
 template <typename T>
 __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, double& su, double& sv, double& sc) {
     constexpr int C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>;
@@ -227,8 +299,8 @@ __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, doubl
 
 // The residuals of one tile staged in shared memory (row r of field f at buf + f·FIELD + r·PITCH, cell x0 + c at
 // column C0 + c, the halo cells at C0 - 1 and C0 + scols, tile row r = grid row y0 - 1 + r): the register path's
-// arithmetic, operation for operation; each lane's 4 squares are summed in f32 before one f64 addition per norm. Warp
-// w computes the tile rows w, w + 8, ...
+// arithmetic (nsi_cell, two cells per packed instruction); each lane's 4 squares are summed in f32 (cells 0 and 2,
+// cells 1 and 3, then the two sums) before one f64 addition per norm. Warp w computes the tile rows w, w + 8, ...
 template <typename T, int FIELD>
 __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, int x0, int y0, int scols, int th,
                                                  double& su, double& sv, double& sc) {
@@ -264,34 +336,33 @@ __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, in
                 nsi_ld4(mS + 2 * kField, pS);
                 nsi_ld4(mN + 2 * kField, pN);
             }
-            float oru[4], orv[4], orc[4];
-            float qu = 0.f, qv = 0.f, qc = 0.f;
+            // cells (0, 1) and (2, 3) as pairs
+            float2 ru[2], rv[2], rc[2];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const float uc = cu[e + 1], vc = cv[e + 1];
-                const float uW = cu[e], uE = cu[e + 2];
-                const float vW = cv[e], vE = cv[e + 2];
-                const float pW = cp[e], pE = cp[e + 2];
-                const float dudx = (uE - uW) * inv2h, dudy = (uN[e] - uS[e]) * inv2h;
-                const float dvdx = (vE - vW) * inv2h, dvdy = (vN[e] - vS[e]) * inv2h;
-                const float dpdx = (pE - pW) * inv2h, dpdy = (pN[e] - pS[e]) * inv2h;
-                const float lapu = (((uE - uc) + (uW - uc)) + ((uN[e] - uc) + (uS[e] - uc))) * invh2;
-                const float lapv = (((vE - vc) + (vW - vc)) + ((vN[e] - vc) + (vS[e] - vc))) * invh2;
-                const float ru = ((uc * dudx + vc * dudy) + dpdx) - nu * lapu;
-                const float rv = ((uc * dvdx + vc * dvdy) + dpdy) - nu * lapv;
-                const float rc = dudx + dvdy;
-                oru[e] = ru; orv[e] = rv; orc[e] = rc;
-                qu = fmaf(ru, ru, qu);
-                qv = fmaf(rv, rv, qv);
-                qc = fmaf(rc, rc, qc);
+            for (int h = 0; h < 2; ++h) {
+                const int e = 2 * h;
+                const NsiStar<NsiTwo> su2{make_float2(cu[e + 1], cu[e + 2]), make_float2(cu[e], cu[e + 1]),
+                                          make_float2(cu[e + 2], cu[e + 3]), make_float2(uS[e], uS[e + 1]),
+                                          make_float2(uN[e], uN[e + 1])};
+                const NsiStar<NsiTwo> sv2{make_float2(cv[e + 1], cv[e + 2]), make_float2(cv[e], cv[e + 1]),
+                                          make_float2(cv[e + 2], cv[e + 3]), make_float2(vS[e], vS[e + 1]),
+                                          make_float2(vN[e], vN[e + 1])};
+                const NsiStar<NsiTwo> sp2{make_float2(cp[e + 1], cp[e + 2]), make_float2(cp[e], cp[e + 1]),
+                                          make_float2(cp[e + 2], cp[e + 3]), make_float2(pS[e], pS[e + 1]),
+                                          make_float2(pN[e], pN[e + 1])};
+                nsi_cell<NsiTwo>(su2, sv2, sp2, inv2h, invh2, nu, ru[h], rv[h], rc[h]);
             }
-            su += double(qu);
-            sv += double(qv);
-            sc += double(qc);
+            // squares: lane x of the pair sums cells 0 and 2, lane y cells 1 and 3, then x + y
+            const float2 qu = NsiTwo::fma(ru[1], ru[1], NsiTwo::mul(ru[0], ru[0]));
+            const float2 qv = NsiTwo::fma(rv[1], rv[1], NsiTwo::mul(rv[0], rv[0]));
+            const float2 qc = NsiTwo::fma(rc[1], rc[1], NsiTwo::mul(rc[0], rc[0]));
+            su += double(__fadd_rn(qu.x, qu.y));
+            sv += double(__fadd_rn(qv.x, qv.y));
+            sc += double(__fadd_rn(qc.x, qc.y));
             const int64_t ro = int64_t(y0 + j) * nx + c0;
-            st_f4(g.ru + ro, make_float4(oru[0], oru[1], oru[2], oru[3]));
-            st_f4(g.rv + ro, make_float4(orv[0], orv[1], orv[2], orv[3]));
-            st_f4(g.rc + ro, make_float4(orc[0], orc[1], orc[2], orc[3]));
+            st_f4(g.ru + ro, make_float4(ru[0].x, ru[0].y, ru[1].x, ru[1].y));
+            st_f4(g.rv + ro, make_float4(rv[0].x, rv[0].y, rv[1].x, rv[1].y));
+            st_f4(g.rc + ro, make_float4(rc[0].x, rc[0].y, rc[1].x, rc[1].y));
         }
     }
 }
@@ -423,15 +494,11 @@ __device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblo
                 const float uW = e == 0 ? ul : u1.c[e - 1], uE = e == VEC - 1 ? ur : u1.c[e + 1];
                 const float vW = e == 0 ? vl : v1.c[e - 1], vE = e == VEC - 1 ? vr : v1.c[e + 1];
                 const float pW = e == 0 ? pl : p1.c[e - 1], pE = e == VEC - 1 ? pr : p1.c[e + 1];
-                const float uS = u0.c[e], uN = u2.c[e], vS = v0.c[e], vN = v2.c[e], pS = p0.c[e], pN = p2.c[e];
-                const float dudx = (uE - uW) * inv2h, dudy = (uN - uS) * inv2h;
-                const float dvdx = (vE - vW) * inv2h, dvdy = (vN - vS) * inv2h;
-                const float dpdx = (pE - pW) * inv2h, dpdy = (pN - pS) * inv2h;
-                const float lapu = (((uE - uc) + (uW - uc)) + ((uN - uc) + (uS - uc))) * invh2;
-                const float lapv = (((vE - vc) + (vW - vc)) + ((vN - vc) + (vS - vc))) * invh2;
-                const float ru = ((uc * dudx + vc * dudy) + dpdx) - nu * lapu;
-                const float rv = ((uc * dvdx + vc * dvdy) + dpdy) - nu * lapv;
-                const float rc = dudx + dvdy;
+                const NsiStar<NsiOne> su1{uc, uW, uE, u0.c[e], u2.c[e]};
+                const NsiStar<NsiOne> sv1{vc, vW, vE, v0.c[e], v2.c[e]};
+                const NsiStar<NsiOne> sp1{p1.c[e], pW, pE, p0.c[e], p2.c[e]};
+                float ru, rv, rc;
+                nsi_cell<NsiOne>(su1, sv1, sp1, inv2h, invh2, nu, ru, rv, rc);
                 oru[e] = ru; orv[e] = rv; orc[e] = rc;
                 if (e < ncols) {
                     su = __fma_rn(double(ru), double(ru), su);
