@@ -27,32 +27,6 @@ DeviceInfo device_info() {
 
 int map_cuda_error(cudaError_t e) { return e == cudaSuccess ? CSPB_OK : CSPB_ERR_CUDA; }
 
-bool encode_tensor_map_2d(CUtensorMap* map, const void* base, bool bf16, uint64_t cols, uint64_t rows,
-                          uint64_t pitch_elems, uint32_t box_cols, uint32_t box_rows) {
-    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-    static std::once_flag once;
-    static Encode encode = nullptr;
-    std::call_once(once, [] {
-        void* fn = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            encode = reinterpret_cast<Encode>(fn);
-    });
-    if (!encode) return false;
-    const uint64_t esz = bf16 ? 2 : 4;
-    const cuuint64_t dims[2] = {cols, rows};
-    const cuuint64_t strides[1] = {pitch_elems * esz};  // bytes between rows
-    const cuuint32_t box[2] = {box_cols, box_rows};
-    const cuuint32_t estr[2] = {1, 1};
-    return encode(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                  const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
 }  // namespace cspb_host
 
 namespace {

@@ -1,8 +1,6 @@
-// mbar.cuh — mbarrier and tensor-map (TMA) helpers shared by the kernels that stage data through shared memory with
+// mbar.cuh — mbarrier and bulk-copy (TMA) helpers shared by the kernels that stage data through shared memory with
 // asynchronous bulk copies. Every wait is bounded (common.cuh).
 #pragma once
-
-#include <cuda.h>
 
 #include "common.cuh"
 
@@ -43,15 +41,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const 
         }
     }
 }
-// One tiled tensor copy (TMA) of a 2D box at element coordinates (x, y) of `map` into this CTA's shared memory,
-// completing on `bar`. x times the element size must be a multiple of 16 bytes; the map covers this GPU's own memory.
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-            "r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
 // One untiled bulk copy (TMA) of `bytes` from this GPU's global memory into this CTA's shared memory, completing on
 // `bar`: both addresses 16-byte aligned, `bytes` a multiple of 16.
 __device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -75,13 +64,3 @@ __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier
 
 }  // namespace cspb
 
-namespace cspb_host {
-
-// A 2D tiled tensor map over a row-major (rows, cols) array of 4-byte (f32) or 2-byte (bf16) elements with row pitch
-// `pitch_elems`, boxes of (box_cols, box_rows) elements, zero fill outside the array. Encoded through the driver's
-// cuTensorMapEncodeTiled, found with cudaGetDriverEntryPoint (the library links no driver library). false when the
-// driver refuses the arguments (base not 16-byte aligned, pitch not a multiple of 16 bytes, box too large).
-bool encode_tensor_map_2d(CUtensorMap* map, const void* base, bool bf16, uint64_t cols, uint64_t rows,
-                          uint64_t pitch_elems, uint32_t box_cols, uint32_t box_rows);
-
-}  // namespace cspb_host

@@ -22,7 +22,6 @@
 // The three squared norms are accumulated per thread in f64, reduced per warp by a fixed xor tree, per block in warp
 // order, and across blocks in block order by the last block to finish: bit-identical on every run.
 #include "common.cuh"
-#include "mbar.cuh"
 
 namespace cspb {
 
@@ -169,21 +168,26 @@ __device__ __forceinline__ void x_neighbours(const NsiRow<T, VEC>& row, bool nee
 // ---- block tiles (cp.async) -------------------------------------------------------------------------------------
 // A block computes one tile of kNsiTileCols × kNsiTileRows cells. It first copies the tile's rows of u, v, p with the
 // rows above and below it and the two wrapped halo columns into shared memory (cp.async: each warp takes every 8th
-// row, each lane a 16-byte chunk of it, then lane 0 and the last active lane the halo cells), waits once, then
-// computes its rows from shared memory and stores the residuals. Four such blocks per SM keep whole tiles in flight
-// while other blocks compute. Measured on B200 at 4096² (f32): 82 µs against 136 µs for a per-warp ring of 4 row
-// slots (one row in flight per warp), with bit-identical residuals; taller tiles (48, 64 rows: 2-3 blocks per SM) ran
-// 91-94 µs. The fields stay in their storage type in shared memory (bf16 is widened as it is read). A tile row is
-// [c0 - 1] the cell left of the tile, [c0 .. c0 + 128) its cells, [c0 + cols] the cell right, c0 = 16 B / sizeof(T).
-constexpr int kNsiTileCols = 128;
-constexpr int kNsiTileRows = 32;
-template <typename T> inline constexpr int kNsiCell0 = 16 / int(sizeof(T));                 // 4 f32, 8 bf16
-template <typename T> inline constexpr int kNsiPitch = kNsiCell0<T> + kNsiTileCols + kNsiCell0<T>;  // 136, 144
-template <typename T>
-inline constexpr size_t kNsiTileBytes = size_t(3) * (kNsiTileRows + 2) * kNsiPitch<T> * sizeof(T);
+// row, its lanes the row's 16-byte chunks, then lane 0 and the last active lane the halo cells), waits once, then
+// computes its rows from shared memory and stores the residuals. Four such tiles per SM are in flight while other
+// tiles compute. The fields stay in their storage type in shared memory (bf16 is widened as it is read).
+// Tile shapes (measured on B200 at 4096², the same per-cell bits whatever the shape): f32 128 × 32 (512-byte row runs;
+// 256 × 16 and 512 × 8 ran alike); bf16 512 × 16, whose 1 KB row runs took 0.059 ms against 0.072 ms for 128 × 32
+// (256-byte runs) with the same shared memory per tile. A tile row is [C0 - 1] the cell left of the tile,
+// [C0 .. C0 + cols) its cells, [C0 + cols] the cell right, C0 = 16 B / sizeof(T).
+template <typename T> inline constexpr int kNsiTileCols = sizeof(T) == 4 ? 128 : 512;
+template <typename T> inline constexpr int kNsiTileRows = sizeof(T) == 4 ? 32 : 16;
+template <typename T> inline constexpr int kNsiCell0 = 16 / int(sizeof(T));                             // 4 f32, 8 bf16
+template <typename T> inline constexpr int kNsiPitch = kNsiCell0<T> + kNsiTileCols<T> + kNsiCell0<T>;  // 136, 528
+template <typename T>  // 55,488 B (f32), 57,024 B (bf16)
+inline constexpr size_t kNsiTileBytes = size_t(3) * (kNsiTileRows<T> + 2) * kNsiPitch<T> * sizeof(T);
 
+template <typename T>
 __host__ __device__ inline int64_t nsi_tiles(int nx, int ny) {
-    return int64_t((nx + kNsiTileCols - 1) / kNsiTileCols) * ((ny + kNsiTileRows - 1) / kNsiTileRows);
+    return int64_t((nx + kNsiTileCols<T> - 1) / kNsiTileCols<T>) * ((ny + kNsiTileRows<T> - 1) / kNsiTileRows<T>);
+}
+__host__ __device__ inline int64_t nsi_tiles(bool bf16, int nx, int ny) {
+    return bf16 ? nsi_tiles<__nv_bfloat16>(nx, ny) : nsi_tiles<float>(nx, ny);
 }
 // The tile path takes 16-byte aligned fields (checked by the caller) whose rows are whole 16-byte chunks: nx % 4 == 0
 // in f32, nx % 8 == 0 in bf16. Single calls and task tables use this same rule, so a grid's decomposition (and hence
@@ -222,13 +226,13 @@ __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, in
 // 4 squares are summed in f32 (cells 0 and 2, cells 1 and 3, then the two sums) before one f64 addition per norm.
 template <typename T>
 __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, double& su, double& sv, double& sc) {
-    constexpr int C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>;
-    constexpr int VC = 16 / int(sizeof(T));                  // cells per 16-byte copy
-    constexpr int kField = (kNsiTileRows + 2) * PITCH;       // elements between the fields
-    const int tilesx = (g.nx + kNsiTileCols - 1) / kNsiTileCols;
-    const int x0 = int(b % tilesx) * kNsiTileCols, y0 = int(b / tilesx) * kNsiTileRows;
-    const int scols = g.nx - x0 >= kNsiTileCols ? kNsiTileCols : g.nx - x0;  // a multiple of VC
-    const int th = g.ny - y0 >= kNsiTileRows ? kNsiTileRows : g.ny - y0;
+    constexpr int C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>, COLS = kNsiTileCols<T>, ROWS = kNsiTileRows<T>;
+    constexpr int VC = 16 / int(sizeof(T));            // cells per 16-byte copy
+    constexpr int kField = (ROWS + 2) * PITCH;         // elements between the fields
+    const int tilesx = (g.nx + COLS - 1) / COLS;
+    const int x0 = int(b % tilesx) * COLS, y0 = int(b / tilesx) * ROWS;
+    const int scols = g.nx - x0 >= COLS ? COLS : g.nx - x0;  // a multiple of VC
+    const int th = g.ny - y0 >= ROWS ? ROWS : g.ny - y0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int lcol = x0 == 0 ? g.nx - 1 : x0 - 1;
     const int rcol = (x0 + scols) % g.nx;
@@ -253,45 +257,37 @@ __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, doubl
         const int64_t ro = int64_t(gy) * nx;
         ru_ = U + ro; rv_ = V + ro; rp_ = P + ro;
     };
-    const int cc = lane * VC;  // this lane's chunk of the row (f32: 32 lanes × 4 cells; bf16: 16 lanes × 8)
+    // The halo cells, by 4-byte copies. In bf16 a copy moves the aligned pair of cells that holds the halo cell: the
+    // left halo column is odd (x0 - 1 with x0 a multiple of 512, or nx - 1 with nx even), so its pair starts one cell
+    // before it, at C0 - 2; the right one is even (a multiple of 8, or 0) and its pair starts at it, at C0 + scols (the
+    // pair's second cell, inside the grid, lands in the pitch's padding).
+    constexpr int kHaloL = sizeof(T) == 4 ? 0 : 1;  // cells the left copy starts before the halo cell
+    const int last = (scols - 1) / VC % 32;         // the lane holding the row's last chunk
     for (int r = warp; r < th + 2; r += kNsiWarps) {
         const T *ru_, *rv_, *rp_;
         row_src(r, ru_, rv_, rp_);
         T* row = buf + r * PITCH;
-        if (cc < scols) {
-            nsi_cp16(row + C0 + cc, ru_ + x0 + cc);
-            nsi_cp16(row + kField + C0 + cc, rv_ + x0 + cc);
-            nsi_cp16(row + 2 * kField + C0 + cc, rp_ + x0 + cc);
+#pragma unroll
+        for (int k = 0; k < (COLS / VC + 31) / 32; ++k) {
+            const int cc = (k * 32 + lane) * VC;  // this lane's chunks of the row
+            if (cc < scols) {
+                nsi_cp16(row + C0 + cc, ru_ + x0 + cc);
+                nsi_cp16(row + kField + C0 + cc, rv_ + x0 + cc);
+                nsi_cp16(row + 2 * kField + C0 + cc, rp_ + x0 + cc);
+            }
         }
-        if constexpr (sizeof(T) == 4) {
-            if (lane == 0) {
-                nsi_cp4(row + C0 - 1, ru_ + lcol);
-                nsi_cp4(row + kField + C0 - 1, rv_ + lcol);
-                nsi_cp4(row + 2 * kField + C0 - 1, rp_ + lcol);
-            }
-            if (cc < scols && cc + VC >= scols) {
-                nsi_cp4(row + C0 + scols, ru_ + rcol);
-                nsi_cp4(row + kField + C0 + scols, rv_ + rcol);
-                nsi_cp4(row + 2 * kField + C0 + scols, rp_ + rcol);
-            }
+        if (lane == 0) {
+            nsi_cp4(row + C0 - 1 - kHaloL, ru_ + lcol - kHaloL);
+            nsi_cp4(row + kField + C0 - 1 - kHaloL, rv_ + lcol - kHaloL);
+            nsi_cp4(row + 2 * kField + C0 - 1 - kHaloL, rp_ + lcol - kHaloL);
+        }
+        if (lane == last) {
+            nsi_cp4(row + C0 + scols, ru_ + rcol);
+            nsi_cp4(row + kField + C0 + scols, rv_ + rcol);
+            nsi_cp4(row + 2 * kField + C0 + scols, rp_ + rcol);
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
-    if constexpr (sizeof(T) == 2) {
-        // 2-byte halo cells are below cp.async's 4-byte minimum: plain loads, issued after all the row copies, by
-        // lanes 0-5 of each warp (lane = 2·field + side) for the warp's rows
-        if (lane < 6) {
-            const int f = lane >> 1, side = lane & 1;
-            const int64_t col = side ? rcol : lcol;
-            const int at = f * kField + (side ? C0 + scols : C0 - 1);
-            for (int r = warp; r < th + 2; r += kNsiWarps) {
-                const T *ru_, *rv_, *rp_;
-                row_src(r, ru_, rv_, rp_);
-                const T* src = f == 0 ? ru_ : (f == 1 ? rv_ : rp_);
-                buf[r * PITCH + at] = src[col];
-            }
-        }
-    }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
     nsi_tile_compute<T, kField>(g, buf, x0, y0, scols, th, su, sv, sc);
@@ -300,74 +296,86 @@ __device__ __forceinline__ void nsi_tile(const NsiK& g, int64_t b, T* buf, doubl
 // The residuals of one tile staged in shared memory (row r of field f at buf + f·FIELD + r·PITCH, cell x0 + c at
 // column C0 + c, the halo cells at C0 - 1 and C0 + scols, tile row r = grid row y0 - 1 + r): the register path's
 // arithmetic (nsi_cell, two cells per packed instruction); each lane's 4 squares are summed in f32 (cells 0 and 2,
-// cells 1 and 3, then the two sums) before one f64 addition per norm. Warp w computes the tile rows w, w + 8, ...
+// cells 1 and 3, then the two sums) before one f64 addition per norm. Warp w computes the items w, w + 8, ... of the
+// tile (item = row × segments + segment).
 template <typename T, int FIELD>
 __device__ __forceinline__ void nsi_tile_compute(const NsiK& g, const T* buf, int x0, int y0, int scols, int th,
                                                  double& su, double& sv, double& sc) {
     constexpr int C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>;
     constexpr int kField = FIELD;
+    constexpr int SEGS = kNsiTileCols<T> / 128;  // segments of a tile row: 32 lanes × 4 cells each
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t nx = g.nx;
-    const bool active = lane * 4 < scols;
-    if (active) {
-        const int c0 = x0 + lane * 4;
-        const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
-        const T* const mine = buf + C0 + lane * 4;
-        for (int j = warp; j < th; j += kNsiWarps) {
-            const T* a = mine + (j + 1) * PITCH;
-            const T* mS = mine + j * PITCH;
-            const T* mN = mine + (j + 2) * PITCH;
-            float cu[6], cv[6], cp[6];  // W, 4 cells, E of the row
-            float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
-            {
-                float ua[4], va[4], pa[4];
-                nsi_ld4(a, ua);
-                nsi_ld4(a + kField, va);
-                nsi_ld4(a + 2 * kField, pa);
-                cu[0] = nsi_ld1(a - 1); cu[5] = nsi_ld1(a + 4);
-                cv[0] = nsi_ld1(a + kField - 1); cv[5] = nsi_ld1(a + kField + 4);
-                cp[0] = nsi_ld1(a + 2 * kField - 1); cp[5] = nsi_ld1(a + 2 * kField + 4);
+    const float inv2h = g.inv2h, invh2 = g.invh2, nu = g.nu;
+    // item = tile row j × SEGS + segment; warp w takes items w, w + 8, ... (in f32 a tile row is one segment)
+    for (int it = warp; it < th * SEGS; it += kNsiWarps) {
+        const int j = it / SEGS, xs = (it % SEGS) * 128 + lane * 4;  // the lane's first cell within the tile
+        if (xs >= scols) continue;                                     // past the tile's last cell
+        const int c0 = x0 + xs;
+        const T* const mine = buf + C0 + xs;
+        const T* a = mine + (j + 1) * PITCH;
+        const T* mS = mine + j * PITCH;
+        const T* mN = mine + (j + 2) * PITCH;
+        float cu[6], cv[6], cp[6];  // W, 4 cells, E of the row
+        float uS[4], uN[4], vS[4], vN[4], pS[4], pN[4];
+        {
+            float ua[4], va[4], pa[4];
+            nsi_ld4(a, ua);
+            nsi_ld4(a + kField, va);
+            nsi_ld4(a + 2 * kField, pa);
+            cu[0] = nsi_ld1(a - 1); cu[5] = nsi_ld1(a + 4);
+            cv[0] = nsi_ld1(a + kField - 1); cv[5] = nsi_ld1(a + kField + 4);
+            cp[0] = nsi_ld1(a + 2 * kField - 1); cp[5] = nsi_ld1(a + 2 * kField + 4);
 #pragma unroll
-                for (int e = 0; e < 4; ++e) { cu[e + 1] = ua[e]; cv[e + 1] = va[e]; cp[e + 1] = pa[e]; }
-                nsi_ld4(mS, uS);
-                nsi_ld4(mN, uN);
-                nsi_ld4(mS + kField, vS);
-                nsi_ld4(mN + kField, vN);
-                nsi_ld4(mS + 2 * kField, pS);
-                nsi_ld4(mN + 2 * kField, pN);
-            }
-            // cells (0, 1) and (2, 3) as pairs
-            float2 ru[2], rv[2], rc[2];
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int e = 2 * h;
-                const NsiStar<NsiTwo> su2{make_float2(cu[e + 1], cu[e + 2]), make_float2(cu[e], cu[e + 1]),
-                                          make_float2(cu[e + 2], cu[e + 3]), make_float2(uS[e], uS[e + 1]),
-                                          make_float2(uN[e], uN[e + 1])};
-                const NsiStar<NsiTwo> sv2{make_float2(cv[e + 1], cv[e + 2]), make_float2(cv[e], cv[e + 1]),
-                                          make_float2(cv[e + 2], cv[e + 3]), make_float2(vS[e], vS[e + 1]),
-                                          make_float2(vN[e], vN[e + 1])};
-                const NsiStar<NsiTwo> sp2{make_float2(cp[e + 1], cp[e + 2]), make_float2(cp[e], cp[e + 1]),
-                                          make_float2(cp[e + 2], cp[e + 3]), make_float2(pS[e], pS[e + 1]),
-                                          make_float2(pN[e], pN[e + 1])};
-                nsi_cell<NsiTwo>(su2, sv2, sp2, inv2h, invh2, nu, ru[h], rv[h], rc[h]);
-            }
-            // squares: lane x of the pair sums cells 0 and 2, lane y cells 1 and 3, then x + y
-            const float2 qu = NsiTwo::fma(ru[1], ru[1], NsiTwo::mul(ru[0], ru[0]));
-            const float2 qv = NsiTwo::fma(rv[1], rv[1], NsiTwo::mul(rv[0], rv[0]));
-            const float2 qc = NsiTwo::fma(rc[1], rc[1], NsiTwo::mul(rc[0], rc[0]));
-            su += double(__fadd_rn(qu.x, qu.y));
-            sv += double(__fadd_rn(qv.x, qv.y));
-            sc += double(__fadd_rn(qc.x, qc.y));
-            const int64_t ro = int64_t(y0 + j) * nx + c0;
-            st_f4(g.ru + ro, make_float4(ru[0].x, ru[0].y, ru[1].x, ru[1].y));
-            st_f4(g.rv + ro, make_float4(rv[0].x, rv[0].y, rv[1].x, rv[1].y));
-            st_f4(g.rc + ro, make_float4(rc[0].x, rc[0].y, rc[1].x, rc[1].y));
+            for (int e = 0; e < 4; ++e) { cu[e + 1] = ua[e]; cv[e + 1] = va[e]; cp[e + 1] = pa[e]; }
+            nsi_ld4(mS, uS);
+            nsi_ld4(mN, uN);
+            nsi_ld4(mS + kField, vS);
+            nsi_ld4(mN + kField, vN);
+            nsi_ld4(mS + 2 * kField, pS);
+            nsi_ld4(mN + 2 * kField, pN);
         }
+        // cells (0, 1) and (2, 3) as pairs
+        float2 ru[2], rv[2], rc[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = 2 * h;
+            const NsiStar<NsiTwo> su2{make_float2(cu[e + 1], cu[e + 2]), make_float2(cu[e], cu[e + 1]),
+                                      make_float2(cu[e + 2], cu[e + 3]), make_float2(uS[e], uS[e + 1]),
+                                      make_float2(uN[e], uN[e + 1])};
+            const NsiStar<NsiTwo> sv2{make_float2(cv[e + 1], cv[e + 2]), make_float2(cv[e], cv[e + 1]),
+                                      make_float2(cv[e + 2], cv[e + 3]), make_float2(vS[e], vS[e + 1]),
+                                      make_float2(vN[e], vN[e + 1])};
+            const NsiStar<NsiTwo> sp2{make_float2(cp[e + 1], cp[e + 2]), make_float2(cp[e], cp[e + 1]),
+                                      make_float2(cp[e + 2], cp[e + 3]), make_float2(pS[e], pS[e + 1]),
+                                      make_float2(pN[e], pN[e + 1])};
+            nsi_cell<NsiTwo>(su2, sv2, sp2, inv2h, invh2, nu, ru[h], rv[h], rc[h]);
+        }
+        // squares: lane x of the pair sums cells 0 and 2, lane y cells 1 and 3, then x + y
+        const float2 qu = NsiTwo::fma(ru[1], ru[1], NsiTwo::mul(ru[0], ru[0]));
+        const float2 qv = NsiTwo::fma(rv[1], rv[1], NsiTwo::mul(rv[0], rv[0]));
+        const float2 qc = NsiTwo::fma(rc[1], rc[1], NsiTwo::mul(rc[0], rc[0]));
+        su += double(__fadd_rn(qu.x, qu.y));
+        sv += double(__fadd_rn(qv.x, qv.y));
+        sc += double(__fadd_rn(qc.x, qc.y));
+        const int64_t ro = int64_t(y0 + j) * nx + c0;
+        st_f4(g.ru + ro, make_float4(ru[0].x, ru[0].y, ru[1].x, ru[1].y));
+        st_f4(g.rv + ro, make_float4(rv[0].x, rv[0].y, rv[1].x, rv[1].y));
+        st_f4(g.rc + ro, make_float4(rc[0].x, rc[0].y, rc[1].x, rc[1].y));
     }
 }
 
-// The norm partial of block (or tile) b: a warp xor tree, the block in warp order, into part[b].
+// The per-warp sums of nsi_partial and nsi_final, one array for both (they never overlap in time): four bf16 tiles
+// per SM leave room for 200 bytes of static shared memory per block, not for two such arrays.
+__device__ __forceinline__ double (*nsi_red())[3] {
+    __shared__ double s_red[kNsiWarps][3];
+    return s_red;
+}
+
+// The norm partial of block (or tile) b: a warp xor tree, the block in warp order, into part[b]. FENCE: make the
+// partial visible and close with a barrier; without, the caller fences after its last partial, and the next s_part
+// stores wait for the caller's next barrier.
+template <bool FENCE = true>
 __device__ __forceinline__ void nsi_partial(const NsiK& g, int64_t b, double su, double sv, double sc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -376,16 +384,16 @@ __device__ __forceinline__ void nsi_partial(const NsiK& g, int64_t b, double su,
         sv += __shfl_xor_sync(0xffffffffu, sv, off);
         sc += __shfl_xor_sync(0xffffffffu, sc, off);
     }
-    __shared__ double s_part[kNsiWarps][3];
+    double (*const s_part)[3] = nsi_red();
     if (lane == 0) { s_part[warp][0] = su; s_part[warp][1] = sv; s_part[warp][2] = sc; }
     __syncthreads();
     if (threadIdx.x < 3) {
         double t = s_part[0][threadIdx.x];
         for (int w = 1; w < kNsiWarps; ++w) t += s_part[w][threadIdx.x];
         g.part[b * 3 + threadIdx.x] = t;
-        __threadfence();  // visible before any completion count taken after the barrier
+        if (FENCE) __threadfence();  // visible before any completion count taken after the barrier
     }
-    __syncthreads();
+    if (FENCE) __syncthreads();
 }
 
 // The norms from the partials of blocks 0 .. nblocks-1, by the whole calling block in a fixed assignment and order
@@ -393,7 +401,7 @@ __device__ __forceinline__ void nsi_partial(const NsiK& g, int64_t b, double su,
 // every run. Every thread of the block calls it (it holds a barrier); threads past 256 add nothing.
 __device__ __forceinline__ void nsi_final(const NsiK& g, int64_t nblocks) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __shared__ double s_red[kNsiWarps][3];
+    double (*const s_red)[3] = nsi_red();
     __threadfence();
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     const int64_t start = threadIdx.x < kNsiThreads ? int64_t(threadIdx.x) : nblocks;
@@ -527,191 +535,36 @@ __device__ __forceinline__ void nsi_block(const NsiK& g, int64_t b, int64_t nblo
     nsi_norms(g, b, nblocks, done, su, sv, sc);
 }
 
-// ---- block tiles fed by TMA, persistent, warp-specialized --------------------------------------------------------
-// The tile path without a block-wide wait per tile. A CTA (2 per SM) owns tiles blockIdx.x, + gridDim.x, ... and a
-// ring of S stages in shared memory; each stage holds one tile's box of u, v, p — (128 + 2·C0) columns from x0 - C0
-// (an x coordinate that is a multiple of 16 bytes) by 34 rows from y0 - 1 — loaded by three 2D tensor-map copies
-// (cp.async.bulk.tensor) that complete on the stage's FULL mbarrier. A producer warp refills a stage as soon as the 8
-// consumer warps have released it on its EMPTY mbarrier, so the consumers never wait for one another: a warp computes
-// its rows of a tile, writes its norm partial, releases the stage and moves on to the next tile. The copies read this
-// GPU's own memory only (no cluster multicast). Outside the grid a copy fills zeros; on the grid's edges each warp
-// overwrites the wrapped halo cells its own rows read with plain loads. The compute is the tile path's function, and
-// the last warp to finish a tile adds the 8 warp partials in warp order, as the tile path does: residuals and norms
-// are bit-identical to it (and so to the task tables).
-template <typename T> inline constexpr int kNsiTmaStages = sizeof(T) == 4 ? 2 : 3;
-template <typename T> inline constexpr int kNsiTmaBox = (kNsiTileRows + 2) * kNsiPitch<T>;  // elements per field
-// elements between the fields of a stage: the box rounded up to 128 bytes
-template <typename T>
-inline constexpr int kNsiTmaField = (kNsiTmaBox<T> * int(sizeof(T)) + 127) / 128 * 128 / int(sizeof(T));
-template <typename T> inline constexpr size_t kNsiTmaStageBytes = size_t(3) * kNsiTmaField<T> * sizeof(T);
-// per stage: the ring data, then [FULL, EMPTY] mbarriers, the 8 warp partials (3 doubles each) and a finish counter
-template <typename T>
-inline constexpr size_t kNsiTmaSmem = kNsiTmaStages<T> * (kNsiTmaStageBytes<T> + 16 + kNsiWarps * 24 + 8);
-constexpr int kNsiTmaCtasPerSm = 2;
-constexpr int kNsiTmaThreads = kNsiThreads + 32;  // 8 consumer warps + 1 producer warp
-
-// Bounded wait on an mbarrier phase: false after budget_ns.
-__device__ __forceinline__ bool nsi_mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long budget_ns) {
-    if (mbar_test(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    while (!mbar_test(bar, parity)) {
-        if (globaltimer_ns() - t0 > budget_ns) return false;
-        __nanosleep(20);
-    }
-    return true;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kNsiTmaThreads, kNsiTmaCtasPerSm)
-    k_ns_incomp_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
-                    const __grid_constant__ CUtensorMap mp, NsiK g, int64_t tiles) {
-    constexpr int S = kNsiTmaStages<T>, FIELD = kNsiTmaField<T>, C0 = kNsiCell0<T>, PITCH = kNsiPitch<T>;
-    constexpr uint32_t kStageTx = uint32_t(3 * kNsiTmaBox<T> * sizeof(T));
-    extern __shared__ __align__(128) unsigned char nsi_tma_raw[];
-    T* const ring = reinterpret_cast<T*>(nsi_tma_raw);
-    uint64_t* const full = reinterpret_cast<uint64_t*>(nsi_tma_raw + S * kNsiTmaStageBytes<T>);
-    uint64_t* const empty = full + S;
-    double* const wpart = reinterpret_cast<double*>(empty + S);                       // [S][8][3]
-    uint32_t* const finished = reinterpret_cast<uint32_t*>(wpart + S * kNsiWarps * 3);  // [S]
-    __shared__ int s_abort, s_last;
-    __shared__ int64_t s_issued, s_consumed;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tilesx = (g.nx + kNsiTileCols - 1) / kNsiTileCols;
-    const int64_t nx = g.nx;
-    const int64_t mine = tiles > int64_t(blockIdx.x) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // this CTA's
-
-    if (tid == 0) {
-        for (int st = 0; st < S; ++st) {
-            mbar_init(full + st, 1);
-            mbar_init(empty + st, kNsiWarps);
-            finished[st] = 0;
-        }
-        fence_mbar_init();
-        s_abort = 0;
-        s_issued = 0;
-        s_consumed = mine;
-    }
-    __syncthreads();
-
-    if (warp == kNsiWarps) {
-        // producer: tile k into stage k % S once the consumers released the stage's previous tile (k - S)
-        if (lane == 0) {
-            int64_t k = 0;
-            for (; k < mine; ++k) {
-                const int st = int(k % S);
-                if (k >= S && !nsi_mbar_wait(empty + st, uint32_t((k / S) - 1) & 1u, kWaitBudgetNs)) {
-                    set_status(g.ctrl, CSPB_DEV_TIMEOUT);
-                    *reinterpret_cast<volatile int*>(&s_abort) = 1;
-                    break;
-                }
-                if (*reinterpret_cast<volatile int*>(&s_abort)) break;
-                const int64_t b = int64_t(blockIdx.x) + k * gridDim.x;
-                T* buf = ring + size_t(st) * 3 * FIELD;
-                const int x = int(b % tilesx) * kNsiTileCols - C0, y = int(b / tilesx) * kNsiTileRows - 1;
-                mbar_arrive_tx(full + st, kStageTx);
-                tma_load_2d(buf, &mu, x, y, full + st);
-                tma_load_2d(buf + FIELD, &mv, x, y, full + st);
-                tma_load_2d(buf + 2 * FIELD, &mp, x, y, full + st);
-            }
-            s_issued = k;
-        }
-    } else {
-        int64_t k = 0;
-        for (; k < mine; ++k) {
-            const int st = int(k % S);
-            const int64_t b = int64_t(blockIdx.x) + k * gridDim.x;
-            const bool ok = nsi_mbar_wait(full + st, uint32_t(k / S) & 1u, kWaitBudgetNs);
-            if (!__all_sync(0xffffffffu, ok) || *reinterpret_cast<volatile int*>(&s_abort)) {
-                if (lane == 0) {
-                    set_status(g.ctrl, CSPB_DEV_TIMEOUT);
-                    *reinterpret_cast<volatile int*>(&s_abort) = 1;
-                }
-                break;
-            }
-            T* const buf = ring + size_t(st) * 3 * FIELD;
-            const int x0 = int(b % tilesx) * kNsiTileCols, y0 = int(b / tilesx) * kNsiTileRows;
-            const int scols = g.nx - x0 >= kNsiTileCols ? kNsiTileCols : g.nx - x0;
-            const int th = g.ny - y0 >= kNsiTileRows ? kNsiTileRows : g.ny - y0;
-            const bool fixL = x0 == 0, fixR = x0 + scols >= g.nx, fixT = y0 == 0, fixB = y0 + th >= g.ny;
-            if (fixL || fixR || fixT || fixB) {
-                // a tile on the grid's edge: each warp wraps the halo cells its own rows read (the centre row's left
-                // and right cells; the row above its first tile row, the row below the last), so no warp waits for
-                // another; cells that two warps both need get the same value from both
-                const T* F[3] = {static_cast<const T*>(g.u), static_cast<const T*>(g.v), static_cast<const T*>(g.p)};
-                auto put = [&](int f, int r, int c) {  // box row r, column C0 - 1 + c
-                    int gy = y0 - 1 + r, gx = x0 - 1 + c;
-                    gy = gy < 0 ? gy + g.ny : (gy >= g.ny ? gy - g.ny : gy);
-                    gx = gx < 0 ? gx + g.nx : (gx >= g.nx ? gx - g.nx : gx);
-                    buf[f * FIELD + r * PITCH + (C0 - 1) + c] = F[f][int64_t(gy) * nx + gx];
-                };
-                for (int j = warp; j < th; j += kNsiWarps) {
-                    if ((fixL || fixR) && lane < 6) {
-                        const int f = lane >> 1, side = lane & 1;
-                        if (side ? fixR : fixL) put(f, j + 1, side ? scols + 1 : 0);
-                    }
-                    if (fixT && j == 0)
-                        for (int q = lane; q < 3 * scols; q += 32) put(q / scols, 0, 1 + q % scols);
-                    if (fixB && j == th - 1)
-                        for (int q = lane; q < 3 * scols; q += 32) put(q / scols, th + 1, 1 + q % scols);
-                }
-                __syncwarp();
-            }
-            double su = 0.0, sv = 0.0, sc = 0.0;
-            nsi_tile_compute<T, FIELD>(g, buf, x0, y0, scols, th, su, sv, sc);
-#pragma unroll
-            for (int off = 16; off >= 1; off >>= 1) {
-                su += __shfl_xor_sync(0xffffffffu, su, off);
-                sv += __shfl_xor_sync(0xffffffffu, sv, off);
-                sc += __shfl_xor_sync(0xffffffffu, sc, off);
-            }
-            fence_proxy_async_shared();  // this thread's accesses of the stage, before the copies that refill it
-            __syncwarp();
-            if (lane == 0) {
-                double* wp = wpart + (st * kNsiWarps + warp) * 3;
-                wp[0] = su; wp[1] = sv; wp[2] = sc;
-                __threadfence_block();
-                if (atomicAdd(finished + st, 1u) == uint32_t(kNsiWarps - 1)) {
-                    // the tile's last warp: the partials in warp order, as nsi_partial adds them
-                    __threadfence_block();
-                    const volatile double* vp = wpart + st * kNsiWarps * 3;
-                    double t0 = vp[0], t1 = vp[1], t2 = vp[2];
-                    for (int w = 1; w < kNsiWarps; ++w) { t0 += vp[w * 3]; t1 += vp[w * 3 + 1]; t2 += vp[w * 3 + 2]; }
-                    g.part[b * 3 + 0] = t0;
-                    g.part[b * 3 + 1] = t1;
-                    g.part[b * 3 + 2] = t2;
-                    finished[st] = 0;
-                }
-                mbar_arrive(empty + st);
-            }
-        }
-        if (lane == 0 && k < mine) atomicMin(reinterpret_cast<unsigned long long*>(&s_consumed),
-                                             static_cast<unsigned long long>(k));
-    }
-    __syncthreads();
-    if (*reinterpret_cast<volatile int*>(&s_abort)) {
-        // a copy never completed: wait (briefly, bounded) for this CTA's copies still in flight, then leave
-        if (tid == 0)
-            for (int64_t q = s_consumed; q < s_issued; ++q)
-                nsi_mbar_wait(full + int(q % S), uint32_t(q / S) & 1u, 100000000ull);
-        __syncthreads();
-        return;
-    }
-    // the last CTA to finish sums the per-tile partials in tile order
-    __threadfence();
-    if (tid == 0) s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(gridDim.x - 1);
-    __syncthreads();
-    if (s_last) nsi_final(g, tiles);  // block-uniform; every thread reaches its barrier
-}
-
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kNsiThreads) k_ns_incomp(NsiK g) {
     nsi_block<T, VEC>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0);
 }
-// The tile path: one block per tile, 4 blocks per SM (64 registers a thread at most).
+// The tile path of one residual: launched with a block per tile, 4 blocks per SM (64 registers a thread at most).
+// Measured on B200 at 4096²: a persistent grid (4 blocks per SM taking tiles k, k + grid, ...) ran 0.0914 / 0.0663 ms
+// (f32 / bf16) against 0.0811 / 0.0616 ms for a block per tile, which the hardware hands out in tile order as blocks
+// finish. The two storage types end a block in the form that measured faster for each (the same sums either way):
+// f32 tiles as the task kernel's (0.0803 against 0.0810 ms), bf16 with one fence after the partial and no closing
+// barrier (0.0617 against 0.0638 ms); the bf16 form takes any grid, a block's tiles in order.
 template <typename T>
 __global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_tile(NsiK g) {
     extern __shared__ __align__(16) unsigned char nsi_raw[];
-    nsi_tile_block<T>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, reinterpret_cast<T*>(nsi_raw));
+    T* const buf = reinterpret_cast<T*>(nsi_raw);
+    if constexpr (sizeof(T) == 4) {
+        nsi_tile_block<T>(g, blockIdx.x, gridDim.x, g.ctrl + kDone0, buf);
+    } else {
+        __shared__ int s_last;
+        const int64_t tiles = nsi_tiles<T>(g.nx, g.ny);
+        for (int64_t b = blockIdx.x; b < tiles; b += gridDim.x) {
+            double su = 0.0, sv = 0.0, sc = 0.0;
+            nsi_tile<T>(g, b, buf, su, sv, sc);
+            nsi_partial<false>(g, b, su, sv, sc);
+        }
+        if (threadIdx.x < 3) __threadfence();  // the partials this thread stored, before the count
+        __syncthreads();
+        if (threadIdx.x == 0) s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(gridDim.x - 1);
+        __syncthreads();
+        if (s_last) nsi_final(g, tiles);  // block-uniform
+    }
 }
 
 // ---- many residuals in one persistent launch -----------------------------------------------------------------
@@ -761,7 +614,7 @@ __global__ void k_nsi_plan(NsiTasksK g) {
             const bool fast = nsi_fast(t, 4);
             int H, segs;
             int64_t items, blocks;
-            if (fast && nsi_tile_rows(g.bf16 != 0, t.nx)) blocks = nsi_tiles(t.nx, t.ny);  // the tile path
+            if (fast && nsi_tile_rows(g.bf16 != 0, t.nx)) blocks = nsi_tiles(g.bf16 != 0, t.nx, t.ny);  // tiles
             else nsi_shape(t.nx, t.ny, fast ? 4 : 1, H, segs, items, blocks);
             nb = uint64_t(blocks);
         } else {
@@ -812,7 +665,7 @@ __global__ void __launch_bounds__(kNsiThreads, MINB) k_nsi_tasks(NsiTasksK g) {
         NsiK k{};
         int64_t blocks;
         const bool tile = fast && nsi_tile_rows(sizeof(T) == 2, t.nx);
-        if (tile) blocks = nsi_tiles(t.nx, t.ny);
+        if (tile) blocks = nsi_tiles<T>(t.nx, t.ny);
         else nsi_shape(t.nx, t.ny, fast ? vfast : 1, k.H, k.segs, k.items, blocks);
         k.nx = t.nx;
         k.ny = t.ny;
@@ -865,25 +718,14 @@ NsiPlan nsi_plan(int nx, int ny, int vec) {
     return p;
 }
 
-// The persistent TMA kernel over `tiles` tiles of a residual whose fields are 16-byte aligned and whose rows are whole
-// 16-byte chunks. CSPB_ERR_UNSUPPORTED when the driver does not encode the tensor maps (the caller then launches the
-// cp.async tiles).
+// The tile kernel over the tiles of one residual (or slab), a block per tile.
 template <typename T>
-int launch_tma_t(const NsiK& g, int64_t tiles, cudaStream_t st) {
-    CUtensorMap m[3];
-    const void* f[3] = {g.u, g.v, g.p};
-    const bool bf16 = sizeof(T) == 2;
-    for (int i = 0; i < 3; ++i)
-        if (!cspb_host::encode_tensor_map_2d(&m[i], f[i], bf16, uint64_t(g.nx), uint64_t(g.ny), uint64_t(g.nx),
-                                             uint32_t(kNsiPitch<T>), uint32_t(kNsiTileRows + 2)))
-            return CSPB_ERR_UNSUPPORTED;
-    const cspb_host::DeviceInfo di = cspb_host::device_info();
-    if (di.device < 0) return CSPB_ERR_CUDA;
-    const void* kern = reinterpret_cast<const void*>(k_ns_incomp_tma<T>);
-    if (!tile_ready(kern, kNsiTmaSmem<T>)) return CSPB_ERR_LAUNCH;
-    int64_t grid = int64_t(di.sms) * kNsiTmaCtasPerSm;
-    if (grid > tiles) grid = tiles;
-    k_ns_incomp_tma<T><<<unsigned(grid), kNsiTmaThreads, kNsiTmaSmem<T>, st>>>(m[0], m[1], m[2], g, tiles);
+int launch_tiles(const NsiK& g, cudaStream_t st) {
+    const void* kern = reinterpret_cast<const void*>(k_ns_incomp_tile<T>);
+    const int64_t tiles = nsi_tiles<T>(g.nx, g.ny);
+    if (tiles > int64_t(0x7fffffff)) return CSPB_ERR_TOO_LARGE;  // the grid's x extent
+    if (!tile_ready(kern, kNsiTileBytes<T>)) return CSPB_ERR_LAUNCH;
+    k_ns_incomp_tile<T><<<unsigned(tiles), kNsiThreads, kNsiTileBytes<T>, st>>>(g);
     return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
@@ -892,7 +734,9 @@ struct NsiTasksLayout {
     uint64_t cap_blocks = 0;
 };
 
-// Σ blocks over tasks <= Σ (cells/1024 + (nx + ny)/32 + 2) <= max_cells/80 + 3·count (nx, ny >= 3)
+// Σ blocks over tasks <= max_cells/80 + 3·count. A task's blocks: register strips <= cells/1024 + (nx + ny)/32 + 2;
+// f32 tiles <= cells/4096 + nx/128 + ny/32 + 1; bf16 tiles <= cells/8192 + nx/512 + ny/16 + 1. Each is at most
+// cells/80 + 3 for nx, ny >= 3 (the tiles take nx >= 4, nx >= 8 in bf16).
 NsiTasksLayout nsi_tasks_layout(int64_t count, int64_t max_cells) {
     NsiTasksLayout L;
     L.cap_blocks = uint64_t(max_cells) / 80 + 3 * uint64_t(count);
@@ -917,8 +761,10 @@ extern "C" {
 
 size_t cspb_ns_incomp_workspace_bytes(int32_t nx, int32_t ny) {
     if (nx < 3 || ny < 3) return 0;
-    // the scalar plan (vec 1) or the f32 tiles: whichever has more blocks
-    const size_t tiles = align_up(kCtrlBytes + size_t(nsi_tiles(nx, ny)) * 3 * sizeof(double), 256);
+    // the scalar plan (vec 1) or the tiles of either storage type: whichever has the most partials
+    const int64_t nt = nsi_tiles<float>(nx, ny) > nsi_tiles<__nv_bfloat16>(nx, ny) ? nsi_tiles<float>(nx, ny)
+                                                                                  : nsi_tiles<__nv_bfloat16>(nx, ny);
+    const size_t tiles = align_up(kCtrlBytes + size_t(nt) * 3 * sizeof(double), 256);
     const size_t scalar = nsi_plan(nx, ny, 1).ws;
     return tiles > scalar ? tiles : scalar;
 }
@@ -938,7 +784,7 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     NsiPlan P = nsi_plan(d->nx, d->ny, fast ? vfast : 1);
     const bool tile = fast && nsi_tile_rows(bf16, d->nx);
     if (tile) {
-        P.blocks = nsi_tiles(d->nx, d->ny);
+        P.blocks = nsi_tiles(bf16, d->nx, d->ny);
         P.ws = align_up(kCtrlBytes + size_t(P.blocks) * 3 * sizeof(double), 256);
     }
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < P.ws) return CSPB_ERR_WORKSPACE;
@@ -958,25 +804,12 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     g.norms = d->norms;
     g.ctrl = static_cast<uint32_t*>(d->workspace);
     g.part = reinterpret_cast<double*>(static_cast<char*>(d->workspace) + kCtrlBytes);
+    // aligned fields with whole 16-byte rows: the tiles; otherwise the register path, a block per item
+    if (tile) return bf16 ? launch_tiles<__nv_bfloat16>(g, st) : launch_tiles<float>(g, st);
     const dim3 grid(unsigned(P.blocks)), block(kNsiThreads);
-    // bf16 fields take the TMA ring (4057 against 3926 GB/s at 4096² on B200); f32 fields the cp.async tiles at 4
-    // blocks per SM (4903 against 4128 GB/s for the ring: both hold about four tiles per SM in flight, and the ring's
-    // CTAs have fewer warps to compute and store with). Residuals and norms are bit-identical either way.
-    if (tile && bf16) {
-        const int rc = launch_tma_t<__nv_bfloat16>(g, P.blocks, st);
-        if (rc != CSPB_ERR_UNSUPPORTED) return rc;  // else the driver refused a tensor map: the cp.async tiles
-    }
-    if (tile && bf16) {
-        const size_t bytes = kNsiTileBytes<__nv_bfloat16>;
-        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<__nv_bfloat16>), bytes)) return CSPB_ERR_LAUNCH;
-        k_ns_incomp_tile<__nv_bfloat16><<<grid, block, bytes, st>>>(g);
-    } else if (bf16) {
+    if (bf16) {
         if (fast) k_ns_incomp<__nv_bfloat16, 4><<<grid, block, 0, st>>>(g);
         else k_ns_incomp<__nv_bfloat16, 1><<<grid, block, 0, st>>>(g);
-    } else if (tile) {
-        const size_t bytes = kNsiTileBytes<float>;
-        if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), bytes)) return CSPB_ERR_LAUNCH;
-        k_ns_incomp_tile<float><<<grid, block, bytes, st>>>(g);
     } else {
         k_ns_incomp<float, 1><<<grid, block, 0, st>>>(g);
     }
@@ -1033,7 +866,7 @@ int cspb_ns_incomp_tasks(const cspb_ns_incomp_task* tasks, int64_t count, int64_
 
 size_t cspb_ns_incomp_slab_workspace_bytes(int32_t nx, int32_t rows) {
     if (nx < 3 || rows < 1) return 0;
-    return align_up(kCtrlBytes + size_t(nsi_tiles(nx, rows)) * 3 * sizeof(double), 256);
+    return align_up(kCtrlBytes + size_t(nsi_tiles<float>(nx, rows)) * 3 * sizeof(double), 256);
 }
 
 int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
@@ -1069,9 +902,7 @@ int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
         g.dn[f] = d->dn[f];
     }
     g.slab = 1;
-    if (!tile_ready(reinterpret_cast<const void*>(k_ns_incomp_tile<float>), kNsiTileBytes<float>)) return CSPB_ERR_LAUNCH;
-    k_ns_incomp_tile<float><<<dim3(unsigned(nsi_tiles(d->nx, d->rows))), dim3(kNsiThreads), kNsiTileBytes<float>, st>>>(g);
-    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+    return launch_tiles<float>(g, st);
 }
 
 }  // extern "C"

@@ -40,7 +40,8 @@ enum {
     CSPB_ERR_UNSUPPORTED = 7, /* a dtype / option combination this build does not provide */
     CSPB_ERR_CUDA = 8,        /* another CUDA runtime error (cudaMemsetAsync, cudaMemcpyAsync, ...) */
     CSPB_ERR_CAPACITY = 9,    /* device status: device-computed totals do not fit the capacities the caller declared */
-    CSPB_ERR_TOO_LARGE = 10   /* the input is larger than the fixed scratch of cspb_build_column_static allows */
+    CSPB_ERR_TOO_LARGE = 10   /* the input is larger than the call allows (the fixed scratch of
+                                 cspb_build_column_static; an NS grid of more than 2^31 - 1 tiles) */
 };
 
 /* bits of the device status word (the first 4 bytes of every workspace) */
@@ -362,6 +363,8 @@ int cspb_ns_init_cons(float* U, int32_t nx, int32_t ny, float amp, void* stream)
  *   r_u = u·∂u/∂x + v·∂u/∂y + ∂p/∂x − ν∇²u,   r_v = u·∂v/∂x + v·∂v/∂y + ∂p/∂y − ν∇²v,   r_c = ∂u/∂x + ∂v/∂y
  * with 2nd-order central differences on spacing h). u, v, p are (ny, nx) in f32 or bf16 storage; r_u, r_v, r_c are
  * f32. norms (device, 3 doubles, may be NULL) receives ||r_u||₂, ||r_v||₂, ||r_c||₂ from f64 sums in a fixed order.
+ * CSPB_ERR_TOO_LARGE when the grid would need more than 2^31 − 1 tiles (blocks of 128 × 32 cells in f32 storage,
+ * 512 × 16 in bf16).
  * ================================================================================================================== */
 typedef struct cspb_ns_incomp_desc {
     int32_t nx, ny;      /* >= 3 each */
