@@ -561,12 +561,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
         __threadfence();
         const int64_t gsize = g.tiles - grp * kGroup < kGroup ? g.tiles - grp * kGroup : kGroup;
         s_last = atomicAdd(g.gdone + grp, 1u) == uint32_t(gsize - 1);
+        if (s_last) __threadfence();  // for the whole block: the barrier orders the others' loads after it
     }
     __syncthreads();
     if (!s_last) return;
 
-    // 5. the last tile of its group: the group's tile partials in tile order (thread t: tile grp·kGroup + t)
-    __threadfence();
+    // 5. the last tile of its group: the group's tile partials in tile order (thread t: tile grp·kGroup + t). One
+    // thread fences (above), not every thread: a warp's fence would first wait for its residual stores to drain.
     {
         const int64_t t = grp * kGroup + tid;
         float dm = 3.0e38f, wm = 0.0f;
@@ -585,13 +586,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_ns_comp(K g) {
             for (int v = 0; v < 4; ++v) g.gpart_sq[grp * 4 + v] = sd[v];
             __threadfence();
             s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(g.groups - 1);
+            if (s_last) __threadfence();
         }
         __syncthreads();
     }
     if (!s_last) return;
 
     // 6. the last group: the group partials in group order (thread t: groups t, t + 256, ...), and the error stage
-    __threadfence();
     float dm = 3.0e38f, wm = 0.0f;
     double sd[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t q = tid; q < g.groups; q += kThreads) {
