@@ -29,7 +29,9 @@ def test_ns_compressible_matches_reference_golden(cuda, golden, tag, walls, lim)
     assert dg[12] == 0.0 and dg[13] == 0.0
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 48), (96, 80), (250, 130), (512, 512)])
+# tiles of 32 x 15 cells, the deterministic diagnostics combined in groups of 256 tiles: 512 x 240 is exactly one group,
+# 32 x 3855 is 257 tiles (a last group of one), 512 x 512 is 560 tiles (a partial third group)
+@pytest.mark.parametrize("nx,ny", [(64, 48), (96, 80), (250, 130), (512, 512), (512, 240), (32, 3855)])
 @pytest.mark.parametrize("walls,lim", [(True, 0), (False, 1), (True, 1), (False, 0)])
 def test_ns_compressible_vs_oracle(cuda, nx, ny, walls, lim):
     import torch
@@ -116,6 +118,22 @@ def test_ns_incompressible_bf16_storage(cuda):
     for got, want in ((ru, o[0]), (rv, o[1]), (rc, o[2])):
         assert oracle.rel_l2(_np(got), want) < TOL_I
     # the storage error against the f32 fields is reported by the benchmark; the residual amplifies it (1/h)
+
+
+@pytest.mark.parametrize("nx,ny", [(8, 3), (8, 40), (520, 17), (1032, 33), (512, 16), (36, 20)])
+def test_ns_incompressible_bf16_shapes(cuda, nx, ny):
+    # bf16 fields take tiles of 512 x 16 cells when nx % 8 == 0: a grid one tile wide, a last tile column of 8 cells
+    # (520), three columns (1032), one exact tile (512 x 16), rows short of a tile; the halo cells come in as aligned
+    # pairs of cells. 36 % 8 != 0 takes the register path.
+    import torch
+    import cospanmdao_b200 as cb
+    g = torch.Generator(device="cpu").manual_seed(nx * 1000 + ny)
+    u, v, p = ((torch.rand((ny, nx), generator=g) + 0.5).to(torch.bfloat16).to(cuda) for _ in range(3))
+    ru, rv, rc, norms = cb.ns_incompressible(u, v, p, h=0.1, nu=1e-3)
+    o = oracle.ns_incomp_f64(_np(u), _np(v), _np(p), 0.1, 1e-3)
+    for got, want in ((ru, o[0]), (rv, o[1]), (rc, o[2])):
+        assert oracle.rel_l2(_np(got), want) < TOL_I
+    assert np.allclose(norms.cpu().numpy(), o[3], rtol=1e-5)
 
 
 def test_ns_incompressible_deterministic(cuda):
