@@ -47,7 +47,7 @@ def _raise(status: int, what: str) -> None:
         return
     msg = f"{what}: {lib().cspb_status_string(status).decode()}"
     if status in (_capi.ERR_ARGUMENT, _capi.ERR_UNSUPPORTED, _capi.ERR_WORKSPACE, _capi.ERR_NEGATIVE,
-                  _capi.ERR_EXCEEDS32, _capi.ERR_CAPACITY):
+                  _capi.ERR_EXCEEDS32, _capi.ERR_CAPACITY, _capi.ERR_TOO_LARGE):
         raise ValueError(msg)
     if status == _capi.ERR_TIMEOUT:
         raise DeviceTimeout(msg)
