@@ -151,7 +151,8 @@ inline bool whole_leaves(const PatternLeaves& L, std::size_t a, std::size_t k, s
 inline void fast_fail(int st, const std::string& what) {
     if (st == CSPB_OK) return;
     const std::string m = "naga::cospan: " + what + ": " + cspb_status_string(st);
-    if (st == CSPB_ERR_ARGUMENT || st == CSPB_ERR_UNSUPPORTED || st == CSPB_ERR_WORKSPACE) throw std::invalid_argument(m);
+    if (st == CSPB_ERR_ARGUMENT || st == CSPB_ERR_UNSUPPORTED || st == CSPB_ERR_WORKSPACE || st == CSPB_ERR_TOO_LARGE)
+        throw std::invalid_argument(m);
     throw std::runtime_error(m);
 }
 
