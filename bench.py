@@ -494,7 +494,7 @@ def bench_ragged(torch, cb, dist, args, peak):
     b.run(check=True)
     torch.cuda.synchronize()
     offsets_ok = b.offsets_match()
-    tuned = autotune(b, reps=2)
+    tuned = autotune(b, reps=4)  # the candidates differ by 1-2 %: four runs a trial keep the pick stable
     tune = tuned["tune"]
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
