@@ -27,6 +27,32 @@ DeviceInfo device_info() {
 
 int map_cuda_error(cudaError_t e) { return e == cudaSuccess ? CSPB_OK : CSPB_ERR_CUDA; }
 
+namespace {
+__global__ void k_clear_ctrl(uint32_t* ctrl) {
+    asm volatile("griddepcontrol.launch_dependents;");  // the dependent grid may be scheduled from now on
+    ctrl[threadIdx.x] = 0u;
+}
+}  // namespace
+
+int clear_ctrl(void* ws, cudaStream_t st) {
+    k_clear_ctrl<<<1, unsigned(cspb::kCtrlBytes / 4), 0, st>>>(static_cast<uint32_t*>(ws));
+    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
+int launch_dependent(const void* kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kern, args) == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+}
+
 }  // namespace cspb_host
 
 namespace {

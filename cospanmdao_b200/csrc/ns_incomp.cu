@@ -430,7 +430,10 @@ __device__ __forceinline__ void nsi_norms(const NsiK& g, int64_t b, int64_t nblo
                                           double sv, double sc) {
     __shared__ int s_last;
     nsi_partial(g, b, su, sv, sc);
-    if (threadIdx.x == 0) s_last = atomicAdd(done, 1u) == uint32_t(nblocks - 1);
+    if (threadIdx.x == 0) {
+        pdl_wait();  // the count lives in the control block a single call clears with a kernel ahead of this one
+        s_last = atomicAdd(done, 1u) == uint32_t(nblocks - 1);
+    }
     __syncthreads();
     if (s_last) nsi_final(g, nblocks);  // block-uniform
     __syncthreads();  // the shared memory of this block is reused by the next block of a persistent caller
@@ -561,7 +564,10 @@ __global__ void __launch_bounds__(kNsiThreads, 4) k_ns_incomp_tile(NsiK g) {
         }
         if (threadIdx.x < 3) __threadfence();  // the partials this thread stored, before the count
         __syncthreads();
-        if (threadIdx.x == 0) s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(gridDim.x - 1);
+        if (threadIdx.x == 0) {
+            pdl_wait();
+            s_last = atomicAdd(g.ctrl + kDone0, 1u) == uint32_t(gridDim.x - 1);
+        }
         __syncthreads();
         if (s_last) nsi_final(g, tiles);  // block-uniform
     }
@@ -718,15 +724,18 @@ NsiPlan nsi_plan(int nx, int ny, int vec) {
     return p;
 }
 
-// The tile kernel over the tiles of one residual (or slab), a block per tile.
+// The tile kernel over the tiles of one residual (or slab), a block per tile, after the kernel that clears the
+// workspace's control block: it may start before that kernel ends and waits for it only at its completion count.
 template <typename T>
-int launch_tiles(const NsiK& g, cudaStream_t st) {
+int launch_tiles(NsiK g, cudaStream_t st) {
     const void* kern = reinterpret_cast<const void*>(k_ns_incomp_tile<T>);
     const int64_t tiles = nsi_tiles<T>(g.nx, g.ny);
     if (tiles > int64_t(0x7fffffff)) return CSPB_ERR_TOO_LARGE;  // the grid's x extent
     if (!tile_ready(kern, kNsiTileBytes<T>)) return CSPB_ERR_LAUNCH;
-    k_ns_incomp_tile<T><<<unsigned(tiles), kNsiThreads, kNsiTileBytes<T>, st>>>(g);
-    return cudaGetLastError() == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+    const int rc = cspb_host::clear_ctrl(g.ctrl, st);
+    if (rc != CSPB_OK) return rc;
+    void* args[] = {&g};
+    return cspb_host::launch_dependent(kern, dim3(unsigned(tiles)), dim3(kNsiThreads), kNsiTileBytes<T>, st, args);
 }
 
 struct NsiTasksLayout {
@@ -789,7 +798,8 @@ int cspb_ns_incompressible(const cspb_ns_incomp_desc* d, void* stream) {
     }
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < P.ws) return CSPB_ERR_WORKSPACE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
+    // the tiles clear the control block themselves (launch_tiles); the register path after a memset
+    if (!tile && cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
     NsiK g{};
     g.nx = d->nx;
     g.ny = d->ny;
@@ -885,8 +895,7 @@ int cspb_ns_incomp_slab(const cspb_ns_incomp_slab_desc* d, void* stream) {
     const size_t need = cspb_ns_incomp_slab_workspace_bytes(d->nx, d->rows);
     if (!d->workspace || !aligned(d->workspace, 256) || d->workspace_bytes < need) return CSPB_ERR_WORKSPACE;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (cudaMemsetAsync(d->workspace, 0, kCtrlBytes, st) != cudaSuccess) return CSPB_ERR_CUDA;
-    NsiK g{};
+    NsiK g{};  // launch_tiles clears the control block
     g.nx = d->nx;
     g.ny = d->rows;
     g.inv2h = float(1.0 / (2.0 * d->h));
