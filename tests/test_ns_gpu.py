@@ -136,6 +136,27 @@ def test_ns_incompressible_bf16_shapes(cuda, nx, ny):
     assert np.allclose(norms.cpu().numpy(), o[3], rtol=1e-5)
 
 
+def test_ns_incompressible_after_other_calls_on_one_workspace(cuda):
+    # The tile path clears the workspace's control block with a kernel that lets the tiles start before it ends (they
+    # wait for it only at their completion count). Calls of other entry points in between leave that block dirty.
+    import torch
+    import cospanmdao_b200 as cb
+    from cospanmdao_b200 import workloads
+    ws = cb.Workspace(cuda)
+    u, v, p, h = workloads.ns_fields(512, seed=3, device=cuda)
+    ub, vb, pb = (t.to(torch.bfloat16) for t in (u, v, p))
+    first = [t.clone() for t in cb.ns_incompressible(u, v, p, h=h, nu=1e-3, workspace=ws)]
+    first16 = [t.clone() for t in cb.ns_incompressible(ub, vb, pb, h=h, nu=1e-3, workspace=ws)]
+    d = workloads.gemver_inputs(640, seed=1, device=cuda)
+    for _ in range(2):
+        cb.gemver(d["A"], d["u1"], d["v1"], d["u2"], d["v2"], d["y"], d["z"], alpha=1.5, beta=1.2, workspace=ws)
+        cb.exclusive_scan(torch.arange(5000, dtype=torch.int32, device=cuda), workspace=ws)
+        again = cb.ns_incompressible(u, v, p, h=h, nu=1e-3, workspace=ws)
+        again16 = cb.ns_incompressible(ub, vb, pb, h=h, nu=1e-3, workspace=ws)
+        assert all(torch.equal(x, y) for x, y in zip(first, again))
+        assert all(torch.equal(x, y) for x, y in zip(first16, again16))
+
+
 def test_ns_incompressible_deterministic(cuda):
     import torch
     import cospanmdao_b200 as cb
