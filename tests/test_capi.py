@@ -62,6 +62,19 @@ def test_workspace_sizes():
     assert lib.cspb_scan_workspace_bytes(0) >= 256
     assert lib.cspb_ns_incomp_workspace_bytes(2, 2) == 0
     assert lib.cspb_ns_incomp_workspace_bytes(4096, 4096) > 256
+    # one call's workspace serves either storage type: room for the control block and 3 f64 norm partials per tile
+    # of the f32 tiles (128 x 32 cells) and of the bf16 tiles (512 x 16), whichever there are more of (a grid 8 wide
+    # and 10000 tall has 313 f32 tiles and 625 bf16 ones)
+    import math
+    for nx, ny in ((8, 10000), (4096, 4096), (520, 17), (8, 3), (12000, 40)):
+        tiles = max(math.ceil(nx / 128) * math.ceil(ny / 32), math.ceil(nx / 512) * math.ceil(ny / 16))
+        assert lib.cspb_ns_incomp_workspace_bytes(nx, ny) >= 256 + 24 * tiles, (nx, ny)
+    # the compressible residual: the control block, one u32 count per group of 256 tiles of 32 x 15 cells, and the
+    # tile and group partials (4 B + 4 B + 32 B each)
+    for nx, ny in ((4096, 4096), (32, 3855), (64, 48)):
+        tiles = math.ceil(nx / 32) * math.ceil(ny / 15)
+        groups = math.ceil(tiles / 256)
+        assert lib.cspb_ns_comp_workspace_bytes(nx, ny) >= 256 + 4 * groups + 40 * tiles + 40 * groups, (nx, ny)
 
 
 def test_arguments_are_rejected_before_cuda():
