@@ -50,7 +50,10 @@ int launch_dependent(const void* kern, dim3 grid, dim3 block, size_t smem, cudaS
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, kern, args) == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
+    if (cudaLaunchKernelExC(&cfg, kern, args) == cudaSuccess) return CSPB_OK;
+    // a driver that refuses the attribute: a plain launch, ordered after the previous kernel as usual
+    (void)cudaGetLastError();
+    return cudaLaunchKernel(kern, grid, block, args, smem, st) == cudaSuccess ? CSPB_OK : CSPB_ERR_LAUNCH;
 }
 
 }  // namespace cspb_host

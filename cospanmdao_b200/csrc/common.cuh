@@ -234,7 +234,7 @@ int map_cuda_error(cudaError_t e);
 // 2 µs before every launch, 3 % of a 4096² incompressible residual.
 int clear_ctrl(void* ws, cudaStream_t st);
 // A kernel launch allowed to start before the previous kernel on the stream has finished (programmatic stream
-// serialization); ignored where the device or driver does not support it.
+// serialization); a plain launch where the driver refuses it.
 int launch_dependent(const void* kern, dim3 grid, dim3 block, size_t smem, cudaStream_t st, void** args);
 
 }  // namespace cspb_host
